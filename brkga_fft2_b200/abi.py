@@ -1,0 +1,129 @@
+"""ctypes mirror of ``include/brkga_b200.h`` (structs, status codes, loader).
+
+Only plain ctypes: the shared library ``libbrkga_b200.so`` is built in-tree
+by :mod:`brkga_fft2_b200.build` and loaded from the package directory.  The
+loader raises when the library is missing — there is no fallback path.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+ABI_VERSION = 1
+
+OK = 0
+ERR_INVALID_ARGUMENT = 1
+ERR_BAD_INSTANCE = 2
+ERR_CUDA = 3
+ERR_WORKSPACE = 4
+ERR_CAPACITY = 5
+ERR_NEW_BIN_UNFIT = 6
+ERR_NO_DEVICE = 7
+
+STATUS_NAMES = {
+    OK: "ok",
+    ERR_INVALID_ARGUMENT: "invalid argument",
+    ERR_BAD_INSTANCE: "bad instance",
+    ERR_CUDA: "CUDA error",
+    ERR_WORKSPACE: "workspace too small",
+    ERR_CAPACITY: "bin pool exhausted",
+    ERR_NEW_BIN_UNFIT: "new plate received a rotation that does not fit",
+    ERR_NO_DEVICE: "no CUDA device",
+}
+
+
+class BrkgaError(RuntimeError):
+    """A non-zero BrkgaStatus returned by the native library."""
+
+    def __init__(self, status: int, what: str = ""):
+        self.status = int(status)
+        msg = STATUS_NAMES.get(self.status, f"status {status}")
+        super().__init__(f"{what}: {msg}" if what else msg)
+
+
+class BrkgaProblemDesc(ctypes.Structure):
+    _fields_ = [
+        ("n_genes", ctypes.c_int32),
+        ("n_machines", ctypes.c_int32),
+        ("n_types", ctypes.c_int32),
+        ("threshold_mode", ctypes.c_int32),
+        ("gene_type", ctypes.POINTER(ctypes.c_int32)),
+        ("thresholds", ctypes.POINTER(ctypes.c_double)),
+        ("bin_length", ctypes.POINTER(ctypes.c_int32)),
+        ("bin_width", ctypes.POINTER(ctypes.c_int32)),
+        ("bin_area", ctypes.POINTER(ctypes.c_double)),
+        ("setup_time", ctypes.POINTER(ctypes.c_double)),
+        ("proc_time", ctypes.POINTER(ctypes.c_double)),
+        ("proc_time_height", ctypes.POINTER(ctypes.c_double)),
+        ("part_area", ctypes.POINTER(ctypes.c_double)),
+        ("part_nrot", ctypes.POINTER(ctypes.c_int32)),
+        ("part_best_rot", ctypes.POINTER(ctypes.c_int32)),
+        ("rot_h", ctypes.POINTER(ctypes.c_int32)),
+        ("rot_w", ctypes.POINTER(ctypes.c_int32)),
+        ("rot_mask_offset", ctypes.POINTER(ctypes.c_int64)),
+        ("masks", ctypes.POINTER(ctypes.c_uint8)),
+        ("masks_bytes", ctypes.c_int64),
+    ]
+
+
+class BrkgaPlacement(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int32) for n in ("gene", "bin", "x", "y", "rot")]
+
+
+PLACEMENT_DTYPE = np.dtype([("gene", "<i4"), ("bin", "<i4"), ("x", "<i4"), ("y", "<i4"), ("rot", "<i4")])
+
+
+def ptr(arr: np.ndarray, ctype):
+    if not arr.flags["C_CONTIGUOUS"]:
+        raise ValueError("array must be C-contiguous")
+    return arr.ctypes.data_as(ctypes.POINTER(ctype))
+
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_NAME = "libbrkga_b200.so"
+LIB_PATH = os.path.join(PKG_DIR, LIB_NAME)
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load ``libbrkga_b200.so`` and declare its entry points.
+
+    Raises ``RuntimeError`` when the library has not been built: the decoder
+    has no CPU fallback.
+    """
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(
+            f"{path} is missing: build the CUDA library first "
+            "(python -m brkga_fft2_b200.build); there is no CPU fallback")
+    lib = ctypes.CDLL(path)
+    c_int, c_i32, c_i64, c_sz, vp = ctypes.c_int, ctypes.c_int32, ctypes.c_int64, ctypes.c_size_t, ctypes.c_void_p
+    P = ctypes.POINTER
+    sig = {
+        "brkga_abi_version": (c_int, []),
+        "brkga_status_string": (ctypes.c_char_p, [c_int]),
+        "brkga_problem_create": (c_int, [P(BrkgaProblemDesc), P(vp)]),
+        "brkga_problem_destroy": (None, [vp]),
+        "brkga_workspace_bytes": (c_int, [vp, c_i32, c_i64, P(c_sz)]),
+        "brkga_decode": (c_int, [vp, vp, c_i32, vp, vp, vp, vp, c_sz, c_i64, vp]),
+        "brkga_evaluate_host": (c_int, [vp, P(ctypes.c_float), c_i32, P(ctypes.c_double), vp]),
+        "brkga_last_counters": (c_int, [vp, P(c_i64), P(c_i64), P(c_i64)]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if lib.brkga_abi_version() != ABI_VERSION:
+        raise RuntimeError("libbrkga_b200.so ABI version mismatch; rebuild it")
+    _lib = lib
+    return lib
+
+
+def check(status: int, what: str = "") -> None:
+    if status != OK:
+        raise BrkgaError(status, what)

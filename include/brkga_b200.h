@@ -1,0 +1,138 @@
+/*
+ * brkga_b200.h — C ABI of the B200 BRKGA chromosome decoder.
+ *
+ * The decoder maps a population of random-key chromosomes (float32, P rows of
+ * 2N keys: N sequencing keys then N machine keys) to one makespan per
+ * chromosome, with the placement rule of the reference's sequential decoder
+ * (placement.py:94-165, binClassNew.py:45-174).  Plain pointers and sizes
+ * only; no exception crosses this boundary; every entry point returns a
+ * BrkgaStatus code.
+ *
+ * Reference interfaces replaced (paths inside paulonasc7/BRKGA_FFT2):
+ *   brkga_problem_create   NativeFullDecoder::NativeFullDecoder  full_native_decoder.py:408-533
+ *                          + _pack_problem_data                  full_native_decoder.py:2788-2926
+ *   brkga_problem_destroy  NativeFullDecoder destructor (pybind11-owned object)
+ *   brkga_evaluate_host    NativeFullDecoder::evaluate_batch     full_native_decoder.py:563-641
+ *                          (host float32 [P,2N] in, host float64 [P] out)
+ *   brkga_decode           the device part of evaluate_batch: process_machine_batch
+ *                          full_native_decoder.py:1290-1431, stream-ordered, caller-owned buffers
+ *   brkga_workspace_bytes  workspace sizing (reference: grow_grid_storage :2102-2153)
+ */
+#ifndef BRKGA_B200_H
+#define BRKGA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BRKGA_ABI_VERSION 1
+
+/* Machine-assignment comparison: placement.py:122-127 compares float32 keys
+ * against Python-float thresholds, which NumPy >= 2 evaluates in float32;
+ * full_native_decoder.py:961-973 compares in float64.  The two differ only
+ * for thresholds that are not exactly representable in float32 (M = 3, 5, 6...). */
+#define BRKGA_THRESH_F32 0
+#define BRKGA_THRESH_F64 1
+
+typedef enum BrkgaStatus {
+  BRKGA_OK = 0,
+  BRKGA_ERR_INVALID_ARGUMENT = 1, /* null pointer, bad size, P < 0 ...            */
+  BRKGA_ERR_BAD_INSTANCE = 2,     /* inconsistent tables (e.g. mask larger than 1024) */
+  BRKGA_ERR_CUDA = 3,             /* a CUDA runtime call failed                      */
+  BRKGA_ERR_WORKSPACE = 4,        /* workspace too small for this P                  */
+  BRKGA_ERR_CAPACITY = 5,         /* device bin pool exhausted (retry with more)      */
+  BRKGA_ERR_NEW_BIN_UNFIT = 6,    /* a new plate got a best_rotation that does not fit;
+                                     the reference raises in numpy slicing here      */
+  BRKGA_ERR_NO_DEVICE = 7
+} BrkgaStatus;
+
+/* Host description of one instance.  All arrays are read during
+ * brkga_problem_create only (they are copied to the device). */
+typedef struct BrkgaProblemDesc {
+  int32_t n_genes;        /* N: parts in the instance; a chromosome has 2N keys */
+  int32_t n_machines;     /* M >= 1 */
+  int32_t n_types;        /* T: distinct part types */
+  int32_t threshold_mode; /* BRKGA_THRESH_F32 or BRKGA_THRESH_F64 */
+  const int32_t* gene_type;        /* [N]   type index 0..T-1 of gene j (instance_parts) */
+  const double* thresholds;        /* [M-1] machine-key thresholds, ascending */
+  const int32_t* bin_length;       /* [M]   plate rows L   (MachineData.bin_length) */
+  const int32_t* bin_width;        /* [M]   plate columns W (MachineData.bin_width) */
+  const double* bin_area;          /* [M]   MachineData.bin_area */
+  const double* setup_time;        /* [M]   MachineData.setup_time */
+  const double* proc_time;         /* [M*T] MachinePartData.proc_time */
+  const double* proc_time_height;  /* [M*T] MachinePartData.proc_time_height */
+  const double* part_area;         /* [T]   PartData.area (> 0) */
+  const int32_t* part_nrot;        /* [T]   2 or 4 */
+  const int32_t* part_best_rot;    /* [T]   index of the rotation used on a new plate */
+  const int32_t* rot_h;            /* [T*4] rows of np.rot90(mask, r) */
+  const int32_t* rot_w;            /* [T*4] columns of np.rot90(mask, r) */
+  const int64_t* rot_mask_offset;  /* [T*4] byte offset of rotation r's row-major 0/1 mask */
+  const uint8_t* masks;            /* concatenated masks */
+  int64_t masks_bytes;
+} BrkgaProblemDesc;
+
+/* One placement of the audit log: gene index, plate index within the
+ * machine, left column x, bottom row y and rotation — the fields of the
+ * reference's golden files (create_golden.py:194-210: part_id/bin_idx/col/row/rot). */
+typedef struct BrkgaPlacement {
+  int32_t gene;
+  int32_t bin;
+  int32_t x;
+  int32_t y;
+  int32_t rot;
+} BrkgaPlacement;
+
+typedef struct BrkgaProblem BrkgaProblem; /* opaque, device-resident tables */
+
+/* Library ABI version (BRKGA_ABI_VERSION). */
+int brkga_abi_version(void);
+
+/* Static text for a status code. */
+const char* brkga_status_string(int status);
+
+/* Validate the tables, derive bit-packed masks, row runs and densities, and
+ * copy everything to the current CUDA device.  (full_native_decoder.py:408-533) */
+int brkga_problem_create(const BrkgaProblemDesc* desc, BrkgaProblem** out);
+
+/* Free the device tables and the object.  Safe on NULL. */
+void brkga_problem_destroy(BrkgaProblem* problem);
+
+/* Device bytes a caller must provide to brkga_decode for P chromosomes with
+ * a bin pool of `pool_bins` plates (0 = the library's default for P). */
+int brkga_workspace_bytes(const BrkgaProblem* problem, int32_t P, int64_t pool_bins,
+                          size_t* bytes);
+
+/* Decode P chromosomes on `stream` (a cudaStream_t, NULL = legacy default).
+ *   d_chrom     device float32 [P, 2N], row-major
+ *   d_makespan  device float64 [P]; 1e16 for infeasible chromosomes
+ *               (placement.py:9,151-153); NaN where d_status reports an error
+ *   d_log       device BrkgaPlacement [P, M, N] or NULL; entries past a
+ *               machine's part count hold gene = -1
+ *   d_status    device int32 [1]: 0 or a BrkgaStatus raised inside the kernels
+ *   d_ws        device workspace of brkga_workspace_bytes(problem, P, pool_bins)
+ * Asynchronous: returns launch errors only; no allocation, no host sync. */
+int brkga_decode(const BrkgaProblem* problem, const float* d_chrom, int32_t P,
+                 double* d_makespan, BrkgaPlacement* d_log, int32_t* d_status,
+                 void* d_ws, size_t ws_bytes, int64_t pool_bins, void* stream);
+
+/* Host-to-host evaluation, the drop-in for NativeFullDecoder::evaluate_batch
+ * (full_native_decoder.py:563-641): copies h_chrom [P, 2N] float32 to the
+ * device, decodes, and writes h_makespan [P] float64.  Grows its internal
+ * workspace and retries on BRKGA_ERR_CAPACITY.  Synchronous.  h_log may be
+ * NULL (else host BrkgaPlacement [P, M, N]). */
+int brkga_evaluate_host(BrkgaProblem* problem, const float* h_chrom, int32_t P,
+                        double* h_makespan, BrkgaPlacement* h_log);
+
+/* Counters of the last brkga_evaluate_host call (placement tests issued to
+ * the collision search, candidate rows examined, plates opened). */
+int brkga_last_counters(const BrkgaProblem* problem, int64_t* tests, int64_t* rows,
+                        int64_t* bins);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BRKGA_B200_H */

@@ -1,0 +1,340 @@
+"""Generate the golden fixtures in tests/golden from the reference itself.
+
+Run in a container where the reference checkout is available (read-only):
+
+    python tests/golden/make_golden.py --reference /root/reference
+
+It imports the reference's sequential decoder (placement.py / binClassNew.py /
+numba_utils.py / collision_backend.py with the ``torch_cpu`` backend) and
+records, per chromosome, the makespan and every placement (part id, plate,
+column x, bottom row y, rotation).  Outputs:
+
+* ``real_<inst>.npz`` / ``fp_<inst>.npz`` — reference instances rebuilt from ``data/`` (masks from
+  ``data/partsMatrices``, part/machine specs and polygon areas parsed from the
+  xlsx files as raw XML, never from the pickle), with the reference's own
+  known answers:
+    - P75M2-0: ``results/golden/P75M2-0`` (chromosome 688, makespan and the 75
+      ordered placements);
+    - P50M2-0: chromosome 462 of ``np.random.seed(42)`` uniform (500, 100)
+      -> 448166.8336 (``verify_native_vs_pp.py:31-32``) and the final plate
+      grids ``results/inspection_output/pp_bin_m*_b*.txt`` (bit-packed here);
+    - the 8 instances of ``benchmarks/20260422_*.json``: the first five
+      feasible makespans of rep 4 (population ``default_rng(127)``) and the
+      feasible / infeasible counts of the whole population.
+* ``syn_<name>.npz`` — seeded synthetic instances (brkga_fft2_b200.instances)
+  with reference makespans and placement logs for a batch of chromosomes.
+
+Nothing under tests/ reads the reference at run time; only this script does.
+"""
+from __future__ import annotations
+
+import argparse
+import glob
+import json
+import os
+import sys
+import threading
+import time
+import xml.etree.ElementTree as ET
+import zipfile
+
+os.environ.setdefault("NUMBA_CACHE_DIR", "/tmp/brkga_numba_cache")
+sys.dont_write_bytecode = True
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, REPO)
+
+from brkga_fft2_b200 import instances as syn  # noqa: E402
+from brkga_fft2_b200.instance_io import save_instance  # noqa: E402
+from brkga_fft2_b200.problem import MachineData, MachinePartData, ProblemData, make_part_data  # noqa: E402
+
+NS = {"m": "http://schemas.openxmlformats.org/spreadsheetml/2006/main"}
+RID = "{http://schemas.openxmlformats.org/officeDocument/2006/relationships}id"
+
+
+def read_xlsx(path):
+    """Sheets of an xlsx file as lists of {column letter: value} rows (raw XML)."""
+    z = zipfile.ZipFile(path)
+    sst = []
+    if "xl/sharedStrings.xml" in z.namelist():
+        for si in ET.fromstring(z.read("xl/sharedStrings.xml")).findall("m:si", NS):
+            sst.append("".join(t.text or "" for t in si.iter("{%s}t" % NS["m"])))
+    wb = ET.fromstring(z.read("xl/workbook.xml"))
+    rels = {r.get("Id"): r.get("Target") for r in ET.fromstring(z.read("xl/_rels/workbook.xml.rels"))}
+    out = {}
+    for s in wb.find("m:sheets", NS):
+        root = ET.fromstring(z.read("xl/" + rels[s.get(RID)]))
+        rows = []
+        for r in root.find("m:sheetData", NS).findall("m:row", NS):
+            d = {}
+            for c in r.findall("m:c", NS):
+                v = c.find("m:v", NS)
+                if v is None:
+                    continue
+                col = "".join(ch for ch in c.get("r") if ch.isalpha())
+                d[col] = sst[int(v.text)] if c.get("t") == "s" else float(v.text)
+            rows.append(d)
+        out[s.get("name")] = rows
+    return out
+
+
+class Reference:
+    """The reference's CPU decoder, imported read-only, with a placement logger."""
+
+    def __init__(self, root):
+        self.root = root
+        sys.path.insert(0, root)
+        import torch
+        torch.set_num_threads(1)
+        import placement
+        import binClassNew
+        from collision_backend import create_collision_backend
+        import data_structures
+        self.placement = placement
+        self.binClassNew = binClassNew
+        self.ds = data_structures
+        self.backend = create_collision_backend("torch_cpu")
+        self._orig_insert = binClassNew.BuildingPlate.insert
+        self._orig_machine = placement._process_single_machine
+        self._tls = threading.local()
+        ref = self
+
+        def insert(plate, x, y, partMatrix, shapes, partArea, gpu_tensor=None):
+            st = getattr(ref._tls, "state", None)
+            if st is not None:
+                pid, rot = st["rot_of"][id(partMatrix)]
+                bins = st["bins"]
+                if id(plate) not in bins:
+                    bins[id(plate)] = len(bins)
+                st["log"][st["machine"]].append((pid, bins[id(plate)], int(x), int(y), rot))
+            return ref._orig_insert(plate, x, y, partMatrix, shapes, partArea, gpu_tensor=gpu_tensor)
+
+        def machine(args):
+            st = getattr(ref._tls, "state", None)
+            if st is not None:
+                st["machine"] = args[0]
+                st["bins"] = {}
+            return ref._orig_machine(args)
+
+        binClassNew.BuildingPlate.insert = insert
+        placement._process_single_machine = machine
+
+    def problem(self, ours: ProblemData, nb_machines):
+        """Reference ProblemData (with torch_cpu FFTs) from one of ours."""
+        ds = self.ds
+        parts = {}
+        for pid, p in ours.parts.items():
+            rd = ds.PartData(id=pid, area=p.area, nrot=p.nrot, rotations=[r.astype(np.int32) for r in p.rotations],
+                             shapes=list(p.shapes), densities=list(p.densities), best_rotation=p.best_rotation,
+                             rotations_gpu=None, rotations_uint8=[r.astype(np.uint8) for r in p.rotations])
+            rd.prepare_jit_data()
+            parts[pid] = rd
+        machines = []
+        for m in range(nb_machines):
+            md = ours.machines[m]
+            L, W = int(md.bin_length), int(md.bin_width)
+            mp = {}
+            for pid in ours.parts:
+                ffts = [self.backend.prepare_part_fft(parts[pid].rotations[r], L, W) for r in range(parts[pid].nrot)]
+                # numpy scalars, as BRKGA_alg3.py:411-417 gets them from pandas: CPython >= 3.12
+                # sums exact Python floats with compensation but numpy float64 items naively,
+                # which is what the reference's pipeline (and its C++ decoder) does.
+                mp[pid] = ds.MachinePartData(ffts=ffts, proc_time=np.float64(md.parts[pid].proc_time),
+                                             proc_time_height=np.float64(md.parts[pid].proc_time_height))
+            st = md.setup_time
+            st = np.int64(st) if float(st).is_integer() else np.float64(st)
+            machines.append(ds.MachineData(bin_length=L, bin_width=W, bin_area=md.bin_area,
+                                           setup_time=st, parts=mp))
+        return ds.ProblemData(parts=parts, machines=machines, instance_parts=ours.instance_parts,
+                              instance_parts_unique=ours.instance_parts_unique)
+
+    def decode(self, rpd, nb_parts, nb_machines, thresholds, chrom, inst_parts, stable=False):
+        rot_of = {}
+        for pid, p in rpd.parts.items():
+            for r, arr in enumerate(p.rotations_uint8):
+                rot_of[id(arr)] = (int(pid), r)
+        self._tls.state = {"rot_of": rot_of, "log": {m: [] for m in range(nb_machines)}, "machine": 0, "bins": {}}
+        orig_argsort = np.argsort
+        try:
+            if stable:
+                np.argsort = lambda a, *k, **kw: orig_argsort(a, kind="stable")
+            ms = self.placement.placementProcedure(rpd, nb_parts, nb_machines, list(thresholds),
+                                                   np.asarray(chrom, np.float32), np.asarray(inst_parts),
+                                                   self.backend, parallel=False)
+        finally:
+            np.argsort = orig_argsort
+            log = self._tls.state["log"]
+            self._tls.state = None
+        return float(ms), log
+
+
+def log_to_array(log, nb_machines, nb_parts):
+    """Per machine ordered placements -> int64 [M, N, 5] (part, bin, x, y, rot), -1 padded."""
+    out = -np.ones((nb_machines, nb_parts, 5), np.int64)
+    for m in range(nb_machines):
+        for k, rec in enumerate(log[m]):
+            out[m, k] = rec
+    return out
+
+
+def real_problem(root, nb_parts, nb_machines, inst):
+    spec = read_xlsx(os.path.join(root, "data/PartsMachines/part-machine-information.xlsx"))
+    areas = read_xlsx(os.path.join(root, "data/PartsMachines/polygon_areas.xlsx"))
+    part_rows = {int(r["A"]): r for r in spec["part"][1:]}
+    mach_rows = spec["machine"][1:]
+    area = {int(r["A"]): r["B"] for r in list(areas.values())[0][1:]}
+    with open(os.path.join(root, f"data/Instances/P{nb_parts}M{nb_machines}-{inst}.txt")) as f:
+        inst_parts = np.array([int(v) for v in f.read().split()], np.int64)
+    uniq = np.unique(inst_parts)
+    parts = {int(p): make_part_data(int(p), np.load(os.path.join(root, f"data/partsMatrices/matrix_{p}.npy")),
+                                    area[int(p)]) for p in uniq}
+    machines = []
+    for m in range(nb_machines):
+        mr = mach_rows[m]  # columns: B W(mm), C L(mm), E ST, F VT, G SPT, H HT (BRKGA_alg3.py:389-417)
+        L, W = int(mr["C"]), int(mr["B"])
+        mp = {int(p): MachinePartData(None,
+                                      part_rows[int(p)]["E"] * mr["F"] + part_rows[int(p)]["F"] * mr["G"],
+                                      part_rows[int(p)]["D"] * mr["H"]) for p in uniq}
+        machines.append(MachineData(L, W, float(L * W), float(int(mr["E"])), mp))
+    pd = ProblemData(parts, machines, inst_parts, uniq)
+    return pd, inst_parts, [t / nb_machines for t in range(1, nb_machines)]
+
+
+def read_plate(path):
+    rows = [list(map(int, line.split())) for line in open(path) if line.strip()]
+    return np.packbits(np.array(rows, np.uint8) != 0, axis=1), np.array(rows).shape
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--out", default=HERE)
+    ap.add_argument("--only", default="")
+    args = ap.parse_args()
+    root = args.reference
+    ref = Reference(root)
+    only = set(filter(None, args.only.split(",")))
+
+    def want(tag):
+        return not only or tag in only
+
+    t0 = time.time()
+    # --- reference golden P75M2-0 (results/golden/P75M2-0) -------------------
+    if want("real_P75M2-0"):
+        g = json.load(open(os.path.join(root, "results/golden/P75M2-0")))
+        pd, ip, thr = real_problem(root, 75, 2, 0)
+        rpd = ref.problem(pd, 2)
+        ms, log = ref.decode(rpd, 75, 2, thr, np.array(g["chromosome"], np.float32), ip)
+        gl = -np.ones((2, 75, 5), np.int64)
+        for m in range(2):
+            for k, p in enumerate(g["machines"][str(m)]["placements"]):
+                gl[m, k] = (p["part_id"], p["bin_idx"], p["col"], p["row"], p["rot"])
+        ours = log_to_array(log, 2, 75)
+        assert (ours == gl).all(), "reference run here differs from results/golden/P75M2-0"
+        save_instance(os.path.join(args.out, "real_P75M2-0.npz"), pd, 75, 2, thr, ip, extra={
+            "chromosomes": np.array([g["chromosome"]], np.float32),
+            "golden_makespan": np.array([g["makespan"]], np.float64),
+            "machine_makespan": np.array([g["machines"][str(m)]["makespan"] for m in range(2)], np.float64),
+            "makespans": np.array([ms], np.float64), "logs": gl[None]})
+        print(f"real_P75M2-0: {ms} (golden {g['makespan']})  [{time.time() - t0:.1f}s]")
+
+    # --- P50M2-0 chromosome 462 + plate dumps ----------------------------------
+    if want("real_P50M2-0"):
+        pd, ip, thr = real_problem(root, 50, 2, 0)
+        rpd = ref.problem(pd, 2)
+        np.random.seed(42)
+        pop = np.random.uniform(0.0, 1.0, size=(500, 100)).astype(np.float32)
+        ms, log = ref.decode(rpd, 50, 2, thr, pop[462], ip)
+        extra = {"chromosomes": pop[462:463], "golden_makespan": np.array([448166.8336]),
+                 "makespans": np.array([ms]), "logs": log_to_array(log, 2, 50)[None]}
+        for path in sorted(glob.glob(os.path.join(root, "results/inspection_output/pp_bin_m*_b*.txt"))):
+            tag = os.path.basename(path)[len("pp_bin_"):-4]
+            bits, shape = read_plate(path)
+            extra[f"plate_{tag}"] = bits
+            extra[f"plate_{tag}_shape"] = np.array(shape)
+        save_instance(os.path.join(args.out, "real_P50M2-0.npz"), pd, 50, 2, thr, ip, extra=extra)
+        print(f"real_P50M2-0 #462: {ms}  [{time.time() - t0:.1f}s]")
+
+    # --- benchmark fingerprints (benchmark_harness.py:171-195) -----------------
+    bench = json.load(open(sorted(glob.glob(os.path.join(root, "benchmarks/*.json")))[0]))
+    seen = set()
+    for res in bench["results"]:
+        name = res["instance"]
+        if name in seen or not want("fp_" + name):
+            continue
+        seen.add(name)
+        n, mm, k = res["nb_parts"], res["nb_machines"], res["inst_idx"]
+        pd, ip, thr = real_problem(root, n, mm, k)
+        pop = np.random.default_rng(bench["seed"] + bench["n_reps"] - 1).random(
+            (bench["mult"] * n, 2 * n), dtype=np.float64).astype(np.float32)
+        fp = np.array([float(v) for v in res["fingerprint"]], np.float64)
+        # reference pp run on the first chromosomes, until five feasible ones are decoded
+        rpd = ref.problem(pd, mm)
+        rows, mss, logs = [], [], []
+        for i in range(pop.shape[0]):
+            ms, log = ref.decode(rpd, n, mm, thr, pop[i], ip)
+            rows.append(i)
+            mss.append(ms)
+            logs.append(log_to_array(log, mm, n))
+            if sum(1 for v in mss if v < 1e15) == 5:
+                break
+        feas = np.array([v for v in mss if v < 1e15])
+        assert np.allclose(feas, fp, rtol=0, atol=5e-7), (name, feas, fp)
+        save_instance(os.path.join(args.out, f"fp_{name}.npz"), pd, n, mm, thr, ip, extra={
+            "pop_seed": np.int64(bench["seed"] + bench["n_reps"] - 1), "pop_mult": np.int64(bench["mult"]),
+            "fingerprint": fp, "n_feasible": np.int64(res["n_feasible"]),
+            "n_infeasible": np.int64(res["n_infeasible"]), "rows": np.array(rows),
+            "chromosomes": pop[rows], "makespans": np.array(mss), "logs": np.stack(logs)})
+        print(f"fp_{name}: fingerprint ok over {len(rows)} chromosomes  [{time.time() - t0:.1f}s]")
+
+    # --- synthetic instances ----------------------------------------------------
+    def syn_case(tag, inst, chrom, stable=False):
+        if not want(tag):
+            return
+        rpd = ref.problem(inst.problem_data, inst.nb_machines)
+        mss, logs = [], []
+        for c in chrom:
+            ms, log = ref.decode(rpd, inst.nb_parts, inst.nb_machines, inst.thresholds, c, inst.instance_parts,
+                                 stable=stable)
+            mss.append(ms)
+            logs.append(log_to_array(log, inst.nb_machines, inst.nb_parts))
+        save_instance(os.path.join(args.out, f"{tag}.npz"), inst.problem_data, inst.nb_parts, inst.nb_machines,
+                      inst.thresholds, inst.instance_parts,
+                      extra={"chromosomes": np.asarray(chrom, np.float32), "makespans": np.array(mss),
+                             "logs": np.stack(logs), "stable_ties": np.int64(stable)})
+        print(f"{tag}: {len(chrom)} chromosomes  [{time.time() - t0:.1f}s]")
+
+    i50 = syn.p50m2(0)
+    syn_case("syn_P50M2_s0", i50, syn.chromosomes(32, 50, 1))
+    i100 = syn.p100m4(0)
+    syn_case("syn_P100M4_s0", i100, syn.chromosomes(8, 100, 1))
+    small = syn.small(3, n_parts=14, plates=((64, 48), (40, 72)), bbox_max=30)
+    syn_case("syn_small_nonsquare", small, syn.chromosomes(48, 14, 2))
+    # infeasible parts: machine 1's plate is smaller than some masks (placement.py:47-53)
+    tight = syn.make_instance("tight", 10, [(90, 90), (26, 30)], 5, bbox_min=8, bbox_max=40, allow_unfit=True)
+    syn_case("syn_infeasible", tight, syn.chromosomes(40, 10, 3))
+    # three machines: thresholds 1/3, 2/3 are not float32-exact; keys placed on f32(t)
+    m3 = syn.make_instance("M3", 18, [(70, 70), (60, 80), (80, 60)], 7, bbox_min=6, bbox_max=32)
+    ch = syn.chromosomes(24, 18, 4)
+    f13, f23 = np.float32(1 / 3), np.float32(2 / 3)
+    for r in range(0, 24, 2):
+        ch[r, 18 + (r % 18)] = f13
+        ch[r, 18 + ((r + 5) % 18)] = f23
+        ch[r, 18 + ((r + 9) % 18)] = np.nextafter(f13, np.float32(1))
+    syn_case("syn_three_machines", m3, ch)
+    # equal sequencing keys: reference run with a stable argsort (ties keep gene order)
+    ties = syn.make_instance("ties", 16, [(64, 64), (56, 56)], 9, bbox_min=6, bbox_max=28)
+    ch = syn.chromosomes(24, 16, 6)
+    ch[:, :16] = np.floor(ch[:, :16] * 4) / 4
+    syn_case("syn_ties_stable", ties, ch, stable=True)
+    # full-row and single-cell masks, plates barely larger than the parts
+    edge = syn.make_instance("edge", 12, [(24, 24), (20, 31)], 11, bbox_min=1, bbox_max=18, fill=(0.3, 1.0))
+    syn_case("syn_edge", edge, syn.chromosomes(48, 12, 8))
+    print(f"done in {time.time() - t0:.1f}s")
+
+
+if __name__ == "__main__":
+    main()

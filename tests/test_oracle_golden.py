@@ -1,0 +1,89 @@
+"""Pin the CPU oracle to the reference's own known answers and to golden
+vectors produced by running the reference's decoder (tests/golden)."""
+import numpy as np
+import pytest
+
+from oracle import oracle_decode
+from tests import goldens
+
+
+def test_p75m2_0_reference_golden():
+    """results/golden/P75M2-0: makespan 358657.39113 and the 75 ordered placements."""
+    packed, _, z = goldens.load("real_P75M2-0")
+    ms, log = oracle_decode(packed, z["chromosomes"], with_log=True)
+    assert abs(ms[0] - float(z["golden_makespan"][0])) < 1e-6 * 358657  # verify_correctness.py:149 tolerance 1e-6 rel-ish
+    assert ms[0] == float(z["makespans"][0])  # bit-exact vs the reference run here
+    assert (goldens.part_ids_of_log(packed, log) == z["logs"]).all()
+
+
+def test_p50m2_0_chromosome_462_and_plate_dumps():
+    """verify_native_vs_pp.py:31-32 (448166.8336) and results/inspection_output/pp_bin_m*_b*.txt."""
+    packed, pdata, z = goldens.load("real_P50M2-0")
+    ms, log = oracle_decode(packed, z["chromosomes"], with_log=True)
+    assert round(ms[0], 4) == 448166.8336
+    assert ms[0] == float(z["makespans"][0])
+    assert (goldens.part_ids_of_log(packed, log) == z["logs"]).all()
+    # rebuild the final plates from the log and compare with the reference's dumps
+    plates = [k for k in z.files if k.startswith("plate_") and not k.endswith("_shape")]
+    assert plates
+    for key in plates:
+        m, b = (int(s[1:]) for s in key[len("plate_"):].split("_"))
+        shape = tuple(z[key + "_shape"])
+        grid = np.zeros(shape, np.uint8)
+        for rec in log[0, m]:
+            if rec["gene"] < 0 or rec["bin"] != b:
+                continue
+            pid = packed.type_ids[packed.arrays["gene_type"][rec["gene"]]]
+            mask = pdata.parts[int(pid)].rotations[rec["rot"]]
+            h, w = mask.shape
+            grid[rec["y"] - h + 1: rec["y"] + 1, rec["x"]: rec["x"] + w] += mask.astype(np.uint8)
+        ref = np.unpackbits(z[key], axis=1)[:, : shape[1]]
+        assert grid.max() <= 1
+        assert (grid == ref).all(), key
+
+
+@pytest.mark.parametrize("name", goldens.names("fp_"))
+def test_benchmark_fingerprints(name):
+    """benchmarks/20260422_*.json: first five feasible makespans (%.6f) of rep 4."""
+    packed, _, z = goldens.load(name)
+    ms, log = oracle_decode(packed, z["chromosomes"], n_threads=4, with_log=True)
+    feas = ms[ms < 1e15]
+    assert len(feas) == 5
+    assert [f"{v:.6f}" for v in feas] == [f"{v:.6f}" for v in z["fingerprint"]]
+    assert (ms == z["makespans"]).all()
+    ok = ms < 1e15
+    assert (goldens.part_ids_of_log(packed, log)[ok] == z["logs"][ok]).all()
+
+
+@pytest.mark.parametrize("name", goldens.names("fp_"))
+def test_benchmark_feasible_counts(name):
+    """n_feasible / n_infeasible of the whole rep-4 population (benchmark JSON)."""
+    packed, _, z = goldens.load(name)
+    n = packed.n_genes
+    pop = np.random.default_rng(int(z["pop_seed"])).random((int(z["pop_mult"]) * n, 2 * n)).astype(np.float32)
+    a = packed.arrays
+    M = packed.n_machines
+    thr = np.float32(a["thresholds"][: M - 1])
+    mv = pop[:, n:]
+    mach = np.zeros(mv.shape, np.int64)
+    for k in range(M - 1):
+        mach += mv > thr[k]
+    t = a["gene_type"]
+    h0 = a["rot_h"][t * 4]
+    w0 = a["rot_w"][t * 4]
+    L = a["bin_length"][mach]
+    W = a["bin_width"][mach]
+    unfit = ((h0 > L) | (w0 > W)) & ((w0 > L) | (h0 > W))
+    infeasible = unfit.any(axis=1)
+    assert int((~infeasible).sum()) == int(z["n_feasible"])
+    assert int(infeasible.sum()) == int(z["n_infeasible"])
+
+
+@pytest.mark.parametrize("name", goldens.names("syn_"))
+def test_synthetic_goldens(name):
+    """Seeded synthetic instances decoded by the reference (makespans + placements)."""
+    packed, _, z = goldens.load(name)
+    ms, log = oracle_decode(packed, z["chromosomes"], n_threads=4, with_log=True)
+    np.testing.assert_array_equal(ms, z["makespans"])
+    ok = ms < 1e15
+    assert (goldens.part_ids_of_log(packed, log)[ok] == z["logs"][ok]).all()
