@@ -111,8 +111,9 @@ def load_library(path: str = LIB_PATH):
         "brkga_problem_destroy": (None, [vp]),
         "brkga_workspace_bytes": (c_int, [vp, c_i32, c_i64, P(c_sz)]),
         "brkga_decode": (c_int, [vp, vp, c_i32, vp, vp, vp, vp, c_sz, c_i64, vp]),
+        "brkga_decode_stage": (c_int, [c_i32, vp, vp, c_i32, vp, vp, vp, vp, c_sz, c_i64, vp]),
         "brkga_evaluate_host": (c_int, [vp, P(ctypes.c_float), c_i32, P(ctypes.c_double), vp]),
-        "brkga_last_counters": (c_int, [vp, P(c_i64), P(c_i64), P(c_i64)]),
+        "brkga_last_counters": (c_int, [vp, P(c_i64), P(c_i64), P(c_i64), P(c_i64)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -1,0 +1,1043 @@
+// brkga_decoder.cu — B200 (sm_100a) BRKGA chromosome decoder behind the C ABI
+// of include/brkga_b200.h.
+//
+// Semantics: the reference's sequential decoder (paulonasc7/BRKGA_FFT2
+// placement.py:94-165, binClassNew.py:45-174, numba_utils.py:50-188,
+// collision_backend.py:109-213).  The reference finds collision-free
+// positions with a float FFT correlation; here the correlation is evaluated
+// exactly on bit-packed rows, which yields the same feasible set.
+//
+// Pipeline per population (three launches on one stream, no host sync):
+//   1. assign_sort_kernel  one CTA per chromosome: machine of every gene from
+//      the machine keys, then a bitonic sort of (machine, sequencing key,
+//      gene) 64-bit keys in shared memory -> per-(chromosome, machine) part
+//      order (placement.py:118-135).
+//   2. decode_kernel       persistent CTAs of 4 warps pulling (chromosome,
+//      machine) items from a device counter.  A plate is L rows of
+//      ceil(W/32)+2 32-bit words (bit x of a row = cell x); the first S plates
+//      of an item live in shared memory, further ones in a global pool.  For
+//      each part: first-fit over plates (area filter, then the collision
+//      search), else a new plate with the best rotation at (0, L-1).
+//      The collision search splits (rotation, 32 candidate rows) chunks over
+//      the warps; a lane tests one candidate top row: vacancy filter, then
+//      the exact run-dilation test word by word, giving the leftmost free x.
+//      Results are merged with a 64-bit lexicographic key
+//      (newLen, -y, x, rotation) by atomicMin in shared memory, which is the
+//      reference's rotation rule (binClassNew.py:101-117) — see key_of().
+//   3. reduce_kernel       max over machines, 1e16 for infeasible chromosomes.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "../../include/brkga_b200.h"
+
+namespace {
+
+constexpr int kMaxMachines = 255;
+constexpr int kMaxGenes = 8192;     // bitonic sort buffer: 8192 x 8 B = 64 KB shared memory
+constexpr int kMaxSide = 8191;      // 13-bit fields of the selection key
+constexpr int kDecodeThreads = 128; // 4 warps per item
+constexpr unsigned long long kKeyNone = ~0ull;
+constexpr unsigned kFull = 0xFFFFFFFFu;
+
+struct RotDev {
+  int h, w, mw;      // rows, columns, 32-bit words per mask row
+  int dens_row;      // first entry in dens[] (h entries)
+  int run_row;       // first entry in run_off[] (h + 1 entries, absolute indices into runs[])
+  int mask_base;     // first word in maskbits[] (h * mw words)
+  int imax, dmax;    // row with the longest run of ones and that length
+};
+
+struct MachDev {
+  int L, W, NW, RS;  // plate rows, columns, words per row, row stride (NW + 2 zero pad words)
+  double area;       // MachineData.bin_area
+  double setup;      // MachineData.setup_time
+};
+
+struct BinScal {     // per-plate scalars of binClassNew.BuildingPlate
+  double area, pt, pth;
+  int minrow, maxrow, enc, pool;
+};
+
+struct DecodeParams {
+  const int32_t* gene_type;
+  const MachDev* mach;
+  const double* pt;
+  const double* pth;
+  const double* part_area;
+  const int32_t* nrot;
+  const int32_t* best_rot;
+  const RotDev* rot;
+  const uint16_t* dens;
+  const int32_t* run_off;
+  const uint32_t* runs;
+  const uint32_t* maskbits;
+  const uint8_t* newbin_ok;
+  int N, M, T;
+  int P;
+  const uint16_t* seq;
+  const int32_t* cnt;
+  const int32_t* infeas;
+  double* mk;
+  BrkgaPlacement* log;
+  int32_t* status;
+  unsigned int* item_ctr;
+  unsigned int* pool_ctr;
+  unsigned long long* counters;
+  BinScal* binscal;
+  uint32_t* pool;
+  long long pool_bins;
+  int S;
+  int slot_words;
+  int slot_vac_off;
+};
+
+struct AssignParams {
+  const float* chrom;
+  const double* thr;
+  const int32_t* gene_type;
+  const uint8_t* fits;
+  int N, M, mode, S2;
+  uint16_t* seq;
+  int32_t* cnt;
+  int32_t* infeas;
+  int32_t* status;
+  unsigned int* item_ctr;
+  unsigned int* pool_ctr;
+  unsigned long long* counters;
+};
+
+// ---------------------------------------------------------------- device helpers
+
+__device__ __forceinline__ unsigned ordered_bits(float v) {
+  unsigned u = __float_as_uint(v);
+  if (v == 0.0f) u = 0u;               // -0 and +0 compare equal in the reference's sort
+  if (v != v) u = 0x7FC00000u;         // NaN sorts after every number (np.argsort)
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+// placement.py:122-127 for ascending thresholds: the first machine whose
+// upper threshold is >= the key, else the last; a NaN key matches no mask.
+__device__ __forceinline__ int machine_of(float mv, const double* thr, int M, int mode) {
+  if (M <= 1) return 0;
+  if (mv != mv) return M;
+  int m = 0;
+  if (mode == BRKGA_THRESH_F32) {
+    while (m < M - 1 && !(mv <= (float)thr[m])) ++m;
+  } else {
+    const double v = (double)mv;
+    while (m < M - 1 && !(v <= thr[m])) ++m;
+  }
+  return m;
+}
+
+// Selection key, smaller is better.  Within one plate the reference keeps the
+// rotation of largest packing density (area + a) / (newLen * W); numerator and
+// W are shared and newLen * W are distinct integers <= 2^26, so the float64
+// quotients are strictly ordered by newLen: max density == min newLen.  Ties
+// go to the larger bottom row y, then the smaller x, then the first rotation.
+__device__ __forceinline__ unsigned long long key_of(int newlen, int y, int x, int r) {
+  return ((unsigned long long)newlen << 28) | ((unsigned long long)(kMaxSide - y) << 15) |
+         ((unsigned long long)x << 2) | (unsigned long long)r;
+}
+
+// bits [p, p + 32) of a row (p >= 0; reads words p>>5 and p>>5 + 1)
+__device__ __forceinline__ uint32_t bits32(const uint32_t* row, int p) {
+  const int wi = p >> 5;
+  return __funnelshift_r(row[wi], row[wi + 1], p & 31);
+}
+
+__device__ __forceinline__ bool range_any(const uint32_t* row, int lo, int hi) {
+  const int wl = lo >> 5, wh = (hi - 1) >> 5;
+  const uint32_t ml = 0xFFFFFFFFu << (lo & 31);
+  const uint32_t mh = 0xFFFFFFFFu >> (31 - ((hi - 1) & 31));
+  if (wl == wh) return (row[wl] & ml & mh) != 0u;
+  if (row[wl] & ml) return true;
+  for (int w = wl + 1; w < wh; ++w)
+    if (row[w]) return true;
+  return (row[wh] & mh) != 0u;
+}
+
+// For the 32 placements x' = 0..31 (absolute x = p0 - a + x'), bit x' is set
+// when a run of d mask cells starting at plate column p0 + x' covers an
+// occupied cell: OR of row bits [p0 + x', p0 + x' + d).
+__device__ __forceinline__ uint32_t blocked(const uint32_t* row, int p0, int d) {
+  if (d <= 32) {
+    uint32_t lo = bits32(row, p0), hi = bits32(row, p0 + 32);
+    int s = 1;
+    while (2 * s <= d) {  // doubling: after a step lo bit j = OR of 2s bits from j
+      lo |= __funnelshift_r(lo, hi, s);
+      hi |= hi >> s;
+      s <<= 1;
+    }
+    if (d > s) lo |= __funnelshift_r(lo, hi, d - s);
+    return lo;
+  }
+  // d > 32: every window contains [p0 + 31, p0 + d)
+  if (range_any(row, p0 + 31, p0 + d)) return 0xFFFFFFFFu;
+  uint32_t res = 0u;
+  const uint32_t left = bits32(row, p0) & 0x7FFFFFFFu;       // cell p0+j blocks x' <= j
+  if (left) res |= (2u << (31 - __clz(left))) - 1u;
+  const uint32_t right = bits32(row, p0 + d) & 0x7FFFFFFFu;  // cell p0+d+j blocks x' > j
+  if (right) res |= ~((2u << (__ffs(right) - 1)) - 1u);
+  return res;
+}
+
+__device__ __forceinline__ bool vacancy_ok(const uint16_t* vac, int ty, const RotDev& rd,
+                                           const uint16_t* dens) {
+  if (vac[ty + rd.imax] < rd.dmax) return false;
+  const uint16_t* d = dens + rd.dens_row;
+  for (int i = 0; i < rd.h; ++i)
+    if (vac[ty + i] < __ldg(d + i)) return false;
+  return true;
+}
+
+// Leftmost x at which the rotation fits with its top row at ty, or -1.
+__device__ int first_free_x(const uint32_t* grid, int RS, int W, int ty, const RotDev& rd,
+                            const int32_t* run_off, const uint32_t* runs) {
+  const int nx = W - rd.w + 1;
+  const int nwo = (nx + 31) >> 5;
+  const int32_t* ro = run_off + rd.run_row;
+  for (int k = 0; k < nwo; ++k) {
+    uint32_t F = (k == nwo - 1 && (nx & 31)) ? ((1u << (nx & 31)) - 1u) : 0xFFFFFFFFu;
+    const int base = k << 5;
+    for (int i = 0; i < rd.h && F; ++i) {
+      const uint32_t* row = grid + (size_t)(ty + i) * RS;
+      const int q1 = __ldg(ro + i + 1);
+      for (int q = __ldg(ro + i); q < q1 && F; ++q) {
+        const uint32_t rr = __ldg(runs + q);
+        F &= ~blocked(row, base + (int)(rr & 0xFFFFu), (int)(rr >> 16));
+      }
+    }
+    if (F) return base + __ffs(F) - 1;
+  }
+  return -1;
+}
+
+// longest run of empty cells in a plate row (numba_utils.py:160-188)
+__device__ int max_zero_run(const uint32_t* row, int W, int NW) {
+  int run = 0, best = 0;
+  for (int w = 0; w < NW; ++w) {
+    uint32_t v = row[w];
+    const int valid = W - 32 * w;
+    if (valid < 32) v |= 0xFFFFFFFFu << valid;
+    if (v == 0u) {
+      run += 32;
+      continue;
+    }
+    const int tz = __ffs(v) - 1;
+    run += tz;
+    best = max(best, run);
+    const int hb = 31 - __clz(v);
+    if (hb > tz + 1) {
+      uint32_t zi = ~v & ((1u << hb) - 1u) & ~((2u << tz) - 1u);
+      int n = 0;
+      while (zi) {
+        zi &= zi >> 1;
+        ++n;
+      }
+      best = max(best, n);
+    }
+    run = __clz(v);
+  }
+  return max(best, run);
+}
+
+__device__ __forceinline__ void raise_status(int32_t* status, int code) {
+  atomicCAS(status, 0, code);
+}
+
+// ---------------------------------------------------------------- kernels
+
+__global__ void assign_sort_kernel(AssignParams p) {
+  extern __shared__ unsigned long long keys[];
+  __shared__ int s_cnt[kMaxMachines + 1];
+  __shared__ int s_start[kMaxMachines + 1];
+  __shared__ int s_inf;
+  const int c = blockIdx.x, tid = threadIdx.x, nt = blockDim.x;
+  const int N = p.N, M = p.M;
+  if (c == 0 && tid == 0) {
+    *p.item_ctr = 0u;
+    *p.pool_ctr = 0u;
+    p.counters[0] = p.counters[1] = p.counters[2] = p.counters[3] = 0ull;
+    *p.status = 0;
+  }
+  for (int i = tid; i <= M; i += nt) s_cnt[i] = 0;
+  if (tid == 0) s_inf = 0;
+  __syncthreads();
+  const float* ch = p.chrom + (size_t)c * 2 * N;
+  for (int i = tid; i < p.S2; i += nt) {
+    unsigned long long key = ~0ull;
+    if (i < N) {
+      const int m = machine_of(ch[N + i], p.thr, M, p.mode);
+      atomicAdd(&s_cnt[m], 1);
+      if (m < M && !p.fits[p.gene_type[i] * M + m]) s_inf = 1;  // placement.py:47-53
+      key = ((unsigned long long)m << 48) | ((unsigned long long)ordered_bits(ch[i]) << 16) |
+            (unsigned long long)i;
+    }
+    keys[i] = key;
+  }
+  __syncthreads();
+  for (int k = 2; k <= p.S2; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = tid; i < p.S2; i += nt) {
+        const int ixj = i ^ j;
+        if (ixj > i) {
+          const unsigned long long a = keys[i], b = keys[ixj];
+          const bool up = (i & k) == 0;
+          if ((a > b) == up) {
+            keys[i] = b;
+            keys[ixj] = a;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  if (tid == 0) {
+    int acc = 0;
+    for (int m = 0; m < M; ++m) {
+      s_start[m] = acc;
+      acc += s_cnt[m];
+    }
+  }
+  __syncthreads();
+  for (int i = tid; i < N; i += nt) {
+    const unsigned long long key = keys[i];
+    const int m = (int)(key >> 48);
+    if (m < M) p.seq[((size_t)c * M + m) * N + (i - s_start[m])] = (uint16_t)(key & 0xFFFFu);
+  }
+  for (int m = tid; m < M; m += nt) p.cnt[(size_t)c * M + m] = s_cnt[m];
+  if (tid == 0) p.infeas[c] = s_inf;
+}
+
+__global__ void __launch_bounds__(kDecodeThreads) decode_kernel(DecodeParams p) {
+  extern __shared__ __align__(16) uint32_t smem[];
+  __shared__ unsigned long long s_best;
+  __shared__ int s_item, s_chunk, s_total, s_nr, s_fail, s_pool;
+  __shared__ int s_rlist[4];
+  const int tid = threadIdx.x, lane = tid & 31;
+  BinScal* bs = p.binscal + (size_t)blockIdx.x * p.N;
+  unsigned long long c_tests = 0, c_chunks = 0, c_bins = 0, c_bytes = 0;
+  const int n_items = p.P * p.M;
+
+  for (;;) {
+    if (tid == 0) s_item = (int)atomicAdd(p.item_ctr, 1u);
+    __syncthreads();
+    const int item = s_item;
+    __syncthreads();
+    if (item >= n_items) break;
+
+    const int c = item / p.M, m = item - c * p.M;
+    const MachDev md = p.mach[m];
+    BrkgaPlacement* lg = p.log ? p.log + (size_t)item * p.N : nullptr;
+    const int n = p.cnt[item];
+    if (p.infeas[c]) {  // any part too large for its machine: the whole chromosome scores 1e16
+      if (lg)
+        for (int k = tid; k < p.N; k += kDecodeThreads) lg[k] = BrkgaPlacement{-1, -1, -1, -1, -1};
+      if (tid == 0) p.mk[item] = 0.0;
+      continue;
+    }
+    if (lg)
+      for (int k = n + tid; k < p.N; k += kDecodeThreads) lg[k] = BrkgaPlacement{-1, -1, -1, -1, -1};
+
+    int nb = 0;
+    bool failed = false;
+    for (int k = 0; k < n && !failed; ++k) {
+      const int gene = p.seq[(size_t)item * p.N + k];
+      const int t = p.gene_type[gene];
+      const double a = p.part_area[t];
+      int pb = -1;
+      unsigned long long key = kKeyNone;
+
+      // ---- first fit over the open plates (placement.py:56-64)
+      for (int b = 0; b < nb; ++b) {
+        if (bs[b].area + a > md.area) continue;  // placement.py:57-59
+        uint32_t* grid = b < p.S ? smem + (size_t)b * p.slot_words
+                                 : p.pool + (size_t)bs[b].pool * p.slot_words;
+        const uint16_t* vac = reinterpret_cast<const uint16_t*>(grid + p.slot_vac_off);
+        const int enc = bs[b].enc;
+        if (tid == 0) {
+          int nr = 0, hmin = kMaxSide + 1;
+          const int nrot = p.nrot[t];
+          for (int r = 0; r < nrot; ++r) {
+            const RotDev rd = p.rot[t * 4 + r];
+            if (rd.h <= md.L && rd.w <= md.W) {  // numba_utils.py:82-84
+              s_rlist[nr++] = r;
+              hmin = min(hmin, rd.h);
+              c_bytes += 4ull * ((unsigned long long)md.L * md.NW + (unsigned long long)rd.h * rd.mw);
+            }
+          }
+          s_nr = nr;
+          s_total = nr ? nr * ((md.L - hmin + 1 + 31) >> 5) : 0;
+          s_best = kKeyNone;
+          s_chunk = 0;
+          c_tests += nr;
+        }
+        __syncthreads();
+        const int nr = s_nr, total = s_total;
+        for (int guard = 0; guard < total; ++guard) {
+          int ci = 0;
+          if (lane == 0) ci = atomicAdd(&s_chunk, 1);
+          ci = __shfl_sync(kFull, ci, 0);
+          if (ci >= total) break;
+          const int r = s_rlist[ci % nr];
+          const int level = ci / nr;
+          const RotDev rd = p.rot[t * 4 + r];
+          const int ty_hi = md.L - rd.h - 32 * level;
+          if (ty_hi < 0) continue;
+          unsigned long long cur = 0;
+          if (lane == 0) cur = *(volatile unsigned long long*)&s_best;
+          cur = __shfl_sync(kFull, cur, 0);
+          if (key_of(max(enc, md.L - ty_hi), ty_hi + rd.h - 1, 0, r) >= cur) continue;
+          const int ty = ty_hi - lane;
+          int x = -1;
+          if (ty >= 0 && vacancy_ok(vac, ty, rd, p.dens))
+            x = first_free_x(grid, md.RS, md.W, ty, rd, p.run_off, p.runs);
+          const unsigned fm = __ballot_sync(kFull, x >= 0);
+          if (lane == 0) ++c_chunks;
+          if (fm) {
+            const int l = __ffs(fm) - 1;
+            const int xb = __shfl_sync(kFull, x, l);
+            if (lane == 0) {
+              const int tyb = ty_hi - l;
+              atomicMin(&s_best, key_of(max(enc, md.L - tyb), tyb + rd.h - 1, xb, r));
+            }
+          }
+        }
+        __syncthreads();
+        key = s_best;
+        __syncthreads();
+        if (key != kKeyNone) {
+          pb = b;
+          break;
+        }
+      }
+
+      int r, x, ty;
+      if (pb < 0) {
+        // ---- new plate, best rotation at column 0, bottom row L-1 (placement.py:66-83)
+        r = p.best_rot[t];
+        if (tid == 0) {
+          s_fail = 0;
+          s_pool = -1;
+          if (!p.newbin_ok[t * p.M + m]) {
+            s_fail = BRKGA_ERR_NEW_BIN_UNFIT;
+          } else if (nb >= p.S) {
+            const unsigned idx = atomicAdd(p.pool_ctr, 1u);
+            if ((long long)idx >= p.pool_bins) s_fail = BRKGA_ERR_CAPACITY;
+            else s_pool = (int)idx;
+          }
+        }
+        __syncthreads();
+        if (s_fail) {
+          if (tid == 0) {
+            raise_status(p.status, s_fail);
+            p.mk[item] = nan("");
+          }
+          failed = true;
+          break;
+        }
+        pb = nb++;
+        uint32_t* grid = pb < p.S ? smem + (size_t)pb * p.slot_words : p.pool + (size_t)s_pool * p.slot_words;
+        uint16_t* vac = reinterpret_cast<uint16_t*>(grid + p.slot_vac_off);
+        for (int i = tid; i < md.L * md.RS; i += kDecodeThreads) grid[i] = 0u;
+        for (int i = tid; i < md.L; i += kDecodeThreads) vac[i] = (uint16_t)md.W;  // binClassNew.py:20
+        if (tid == 0) {
+          BinScal z;
+          z.area = 0.0;
+          z.pt = 0.0;
+          z.pth = 0.0;
+          z.minrow = md.L;
+          z.maxrow = -1;
+          z.enc = 0;
+          z.pool = s_pool;
+          bs[pb] = z;
+          ++c_bins;
+        }
+        x = 0;
+        ty = md.L - p.rot[t * 4 + r].h;
+        __syncthreads();
+      } else {
+        r = (int)(key & 3ull);
+        x = (int)((key >> 2) & 0x1FFFull);
+        const int y = kMaxSide - (int)((key >> 15) & 0x1FFFull);
+        ty = y - p.rot[t * 4 + r].h + 1;
+      }
+
+      // ---- insert (binClassNew.py:155-174)
+      {
+        const RotDev rd = p.rot[t * 4 + r];
+        uint32_t* grid = pb < p.S ? smem + (size_t)pb * p.slot_words
+                                  : p.pool + (size_t)bs[pb].pool * p.slot_words;
+        uint16_t* vac = reinterpret_cast<uint16_t*>(grid + p.slot_vac_off);
+        const int sx = x & 31, wx = x >> 5, span = rd.mw + 1;
+        const uint32_t* mb = p.maskbits + rd.mask_base;
+        for (int idx = tid; idx < rd.h * span; idx += kDecodeThreads) {
+          const int i = idx / span, j = idx - i * span;
+          const uint32_t lo = j > 0 ? __ldg(mb + i * rd.mw + j - 1) : 0u;
+          const uint32_t hi = j < rd.mw ? __ldg(mb + i * rd.mw + j) : 0u;
+          const uint32_t v = __funnelshift_l(lo, hi, sx);
+          if (v) grid[(size_t)(ty + i) * md.RS + wx + j] |= v;
+        }
+        __syncthreads();
+        for (int i = tid; i < rd.h; i += kDecodeThreads)
+          vac[ty + i] = (uint16_t)max_zero_run(grid + (size_t)(ty + i) * md.RS, md.W, md.NW);
+        if (tid == 0) {
+          BinScal s = bs[pb];
+          s.area += a;
+          s.minrow = min(s.minrow, ty);
+          s.maxrow = max(s.maxrow, ty + rd.h - 1);
+          s.enc = (s.minrow > s.maxrow) ? 0 : md.L - s.minrow;  // binClassNew.py:147-152
+          s.pt += p.pt[(size_t)m * p.T + t];
+          const double ph = p.pth[(size_t)m * p.T + t];
+          if (ph > s.pth) s.pth = ph;
+          bs[pb] = s;
+          if (lg) lg[k] = BrkgaPlacement{gene, pb, x, ty + rd.h - 1, r};
+        }
+        __syncthreads();
+      }
+    }
+    if (!failed && tid == 0) {  // placement.py:86-89
+      double ms = 0.0;
+      for (int b = 0; b < nb; ++b) ms += (bs[b].pt + bs[b].pth) + md.setup;
+      p.mk[item] = ms;
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    atomicAdd(&p.counters[0], c_tests);
+    atomicAdd(&p.counters[2], c_bins);
+    atomicAdd(&p.counters[3], c_bytes);
+  }
+  if (lane == 0) atomicAdd(&p.counters[1], c_chunks);
+}
+
+__global__ void reduce_kernel(int P, int M, const int32_t* infeas, const double* mk, double* out) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= P) return;
+  if (infeas[c]) {
+    out[c] = 1e16;  // placement.py:9,151-153
+    return;
+  }
+  double worst = 0.0;
+  bool bad = false;
+  for (int m = 0; m < M; ++m) {
+    const double v = mk[(size_t)c * M + m];
+    if (v != v) bad = true;
+    else if (v > worst) worst = v;  // placement.py:154-156
+  }
+  out[c] = bad ? nan("") : worst;
+}
+
+// ---------------------------------------------------------------- host side
+
+size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+struct Layout {
+  size_t off_ctr, off_seq, off_cnt, off_inf, off_mk, off_bins, off_pool, total;
+};
+
+}  // namespace
+
+struct BrkgaProblem {
+  int device = 0;
+  int N = 0, M = 0, T = 0, mode = 0;
+  int sm_count = 0;
+  int S = 0, slot_words = 0, slot_vac_off = 0;
+  int n_slots = 0;
+  size_t decode_smem = 0;
+  std::vector<MachDev> mach;
+  std::vector<void*> allocations;
+  int32_t* d_gene_type = nullptr;
+  double* d_thr = nullptr;
+  MachDev* d_mach = nullptr;
+  double* d_pt = nullptr;
+  double* d_pth = nullptr;
+  double* d_area = nullptr;
+  int32_t* d_nrot = nullptr;
+  int32_t* d_best = nullptr;
+  RotDev* d_rot = nullptr;
+  uint16_t* d_dens = nullptr;
+  int32_t* d_run_off = nullptr;
+  uint32_t* d_runs = nullptr;
+  uint32_t* d_maskbits = nullptr;
+  uint8_t* d_fits = nullptr;
+  uint8_t* d_newbin_ok = nullptr;
+  // brkga_evaluate_host state
+  std::mutex mu;
+  cudaStream_t stream = nullptr;
+  float* e_chrom = nullptr;
+  double* e_out = nullptr;
+  int32_t* e_status = nullptr;
+  BrkgaPlacement* e_log = nullptr;
+  void* e_ws = nullptr;
+  size_t e_ws_bytes = 0;
+  int e_cap_P = 0;
+  bool e_cap_log = false;
+  int64_t e_pool_bins = 0;
+  int64_t last_counters[4] = {0, 0, 0, 0};
+};
+
+namespace {
+
+Layout layout_of(const BrkgaProblem* pb, int32_t P, int64_t pool_bins) {
+  Layout l;
+  size_t o = 0;
+  l.off_ctr = o;
+  o += 64;
+  l.off_seq = o = align_up(o, 256);
+  o += (size_t)P * pb->M * pb->N * sizeof(uint16_t);
+  l.off_cnt = o = align_up(o, 256);
+  o += (size_t)P * pb->M * sizeof(int32_t);
+  l.off_inf = o = align_up(o, 256);
+  o += (size_t)P * sizeof(int32_t);
+  l.off_mk = o = align_up(o, 256);
+  o += (size_t)P * pb->M * sizeof(double);
+  l.off_bins = o = align_up(o, 256);
+  o += (size_t)pb->n_slots * std::max(pb->N, 1) * sizeof(BinScal);
+  l.off_pool = o = align_up(o, 256);
+  o += (size_t)pool_bins * pb->slot_words * sizeof(uint32_t);
+  l.total = align_up(o, 256);
+  return l;
+}
+
+int64_t default_pool_bins(const BrkgaProblem* pb, int32_t P) {
+  const int64_t items = (int64_t)P * pb->M;
+  return std::max<int64_t>(256, items * (pb->S > 0 ? 2 : 4));
+}
+
+template <typename T>
+int upload(BrkgaProblem* pb, T** dst, const std::vector<T>& src) {
+  const size_t bytes = std::max<size_t>(1, src.size()) * sizeof(T);
+  void* p = nullptr;
+  if (cudaMalloc(&p, bytes) != cudaSuccess) return BRKGA_ERR_CUDA;
+  pb->allocations.push_back(p);
+  if (!src.empty() && cudaMemcpy(p, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess)
+    return BRKGA_ERR_CUDA;
+  *dst = static_cast<T*>(p);
+  return BRKGA_OK;
+}
+
+class DeviceGuard {
+ public:
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev_);
+    if (prev_ != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() { cudaSetDevice(prev_); }
+
+ private:
+  int prev_ = 0;
+};
+
+int configure(BrkgaProblem* pb) {
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, pb->device) != cudaSuccess) return BRKGA_ERR_CUDA;
+  pb->sm_count = prop.multiProcessorCount;
+  int Lmax = 0, RSmax = 0;
+  for (const MachDev& m : pb->mach) {
+    Lmax = std::max(Lmax, m.L);
+    RSmax = std::max(RSmax, m.RS);
+  }
+  pb->slot_vac_off = Lmax * RSmax;
+  pb->slot_words = (int)align_up((size_t)pb->slot_vac_off + (size_t)(Lmax + 1) / 2, 4);
+  const size_t slot_bytes = (size_t)pb->slot_words * 4;
+  const size_t per_sm = prop.sharedMemPerMultiprocessor;
+  const size_t per_block_max = prop.sharedMemPerBlockOptin;
+  const size_t reserve = 1024 + 256;  // per-block system reservation + static shared variables
+  // Aim at 8 resident items per SM (32 warps); fewer when one plate does not fit that share.
+  int S = 0, ctas = 8;
+  for (; ctas >= 1; --ctas) {
+    const size_t share = per_sm / ctas;
+    if (share <= reserve) continue;
+    S = (int)std::min<size_t>((share - reserve) / slot_bytes, (per_block_max - 256) / slot_bytes);
+    if (S >= 1) break;
+  }
+  if (S < 1) {  // plates larger than shared memory: all of them in the global pool
+    S = 0;
+    ctas = 8;
+  }
+  S = std::min(S, 4);
+  pb->S = S;
+  pb->decode_smem = (size_t)S * slot_bytes;
+  if (cudaFuncSetAttribute(decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)std::max<size_t>(pb->decode_smem, 1)) != cudaSuccess)
+    return BRKGA_ERR_CUDA;
+  if (cudaFuncSetAttribute(assign_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           kMaxGenes * 8) != cudaSuccess)
+    return BRKGA_ERR_CUDA;
+  int occ = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, decode_kernel, kDecodeThreads, pb->decode_smem) !=
+      cudaSuccess)
+    return BRKGA_ERR_CUDA;
+  occ = std::max(1, std::min(occ, ctas));
+  pb->n_slots = pb->sm_count * occ;
+  return BRKGA_OK;
+}
+
+int validate(const BrkgaProblemDesc* d) {
+  if (!d) return BRKGA_ERR_INVALID_ARGUMENT;
+  if (d->n_genes < 1 || d->n_genes > kMaxGenes || d->n_machines < 1 || d->n_machines > kMaxMachines ||
+      d->n_types < 1 || (d->threshold_mode != BRKGA_THRESH_F32 && d->threshold_mode != BRKGA_THRESH_F64))
+    return BRKGA_ERR_INVALID_ARGUMENT;
+  if (!d->gene_type || (!d->thresholds && d->n_machines > 1) || !d->bin_length || !d->bin_width ||
+      !d->bin_area || !d->setup_time || !d->proc_time || !d->proc_time_height || !d->part_area ||
+      !d->part_nrot || !d->part_best_rot || !d->rot_h || !d->rot_w || !d->rot_mask_offset || !d->masks)
+    return BRKGA_ERR_INVALID_ARGUMENT;
+  for (int j = 0; j < d->n_genes; ++j)
+    if (d->gene_type[j] < 0 || d->gene_type[j] >= d->n_types) return BRKGA_ERR_BAD_INSTANCE;
+  for (int m = 0; m + 1 < d->n_machines; ++m) {
+    if (!std::isfinite(d->thresholds[m])) return BRKGA_ERR_BAD_INSTANCE;
+    if (m > 0 && d->thresholds[m] < d->thresholds[m - 1]) return BRKGA_ERR_BAD_INSTANCE;
+  }
+  for (int m = 0; m < d->n_machines; ++m) {
+    if (d->bin_length[m] < 1 || d->bin_length[m] > kMaxSide || d->bin_width[m] < 1 ||
+        d->bin_width[m] > kMaxSide || !std::isfinite(d->bin_area[m]) || !std::isfinite(d->setup_time[m]))
+      return BRKGA_ERR_BAD_INSTANCE;
+  }
+  for (int t = 0; t < d->n_types; ++t) {
+    if (!(d->part_area[t] > 0.0) || !std::isfinite(d->part_area[t])) return BRKGA_ERR_BAD_INSTANCE;
+    const int nrot = d->part_nrot[t];
+    if (nrot != 2 && nrot != 4) return BRKGA_ERR_BAD_INSTANCE;
+    if (d->part_best_rot[t] < 0 || d->part_best_rot[t] >= nrot) return BRKGA_ERR_BAD_INSTANCE;
+    for (int r = 0; r < nrot; ++r) {
+      const int k = t * 4 + r;
+      const int h = d->rot_h[k], w = d->rot_w[k];
+      if (h < 1 || w < 1 || h > kMaxSide || w > kMaxSide) return BRKGA_ERR_BAD_INSTANCE;
+      const int64_t off = d->rot_mask_offset[k];
+      if (off < 0 || off + (int64_t)h * w > d->masks_bytes) return BRKGA_ERR_BAD_INSTANCE;
+      for (int64_t i = 0; i < (int64_t)h * w; ++i)
+        if (d->masks[off + i] > 1) return BRKGA_ERR_BAD_INSTANCE;
+    }
+    for (int m = 0; m < d->n_machines; ++m) {
+      const size_t i = (size_t)m * d->n_types + t;
+      if (!std::isfinite(d->proc_time[i]) || !std::isfinite(d->proc_time_height[i])) return BRKGA_ERR_BAD_INSTANCE;
+    }
+  }
+  return BRKGA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int brkga_abi_version(void) { return BRKGA_ABI_VERSION; }
+
+const char* brkga_status_string(int status) {
+  switch (status) {
+    case BRKGA_OK: return "ok";
+    case BRKGA_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case BRKGA_ERR_BAD_INSTANCE: return "bad instance";
+    case BRKGA_ERR_CUDA: return "CUDA error";
+    case BRKGA_ERR_WORKSPACE: return "workspace too small";
+    case BRKGA_ERR_CAPACITY: return "bin pool exhausted";
+    case BRKGA_ERR_NEW_BIN_UNFIT: return "new plate received a rotation that does not fit";
+    case BRKGA_ERR_NO_DEVICE: return "no CUDA device";
+    default: return "unknown status";
+  }
+}
+
+void brkga_problem_destroy(BrkgaProblem* pb) {
+  if (!pb) return;
+  {
+    DeviceGuard g(pb->device);
+    for (void* p : pb->allocations) cudaFree(p);
+    if (pb->e_chrom) cudaFree(pb->e_chrom);
+    if (pb->e_out) cudaFree(pb->e_out);
+    if (pb->e_status) cudaFree(pb->e_status);
+    if (pb->e_log) cudaFree(pb->e_log);
+    if (pb->e_ws) cudaFree(pb->e_ws);
+    if (pb->stream) cudaStreamDestroy(pb->stream);
+  }
+  delete pb;
+}
+
+int brkga_problem_create(const BrkgaProblemDesc* d, BrkgaProblem** out) {
+  if (!out) return BRKGA_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  int st = validate(d);
+  if (st) return st;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
+    cudaGetLastError();
+    return BRKGA_ERR_NO_DEVICE;
+  }
+  BrkgaProblem* pb = new BrkgaProblem();
+  cudaGetDevice(&pb->device);
+  pb->N = d->n_genes;
+  pb->M = d->n_machines;
+  pb->T = d->n_types;
+  pb->mode = d->threshold_mode;
+  const int N = pb->N, M = pb->M, T = pb->T;
+
+  // derived part tables: densities, runs of ones, bit-packed rows
+  std::vector<RotDev> rot((size_t)T * 4);
+  std::vector<uint16_t> dens;
+  std::vector<int32_t> run_off;
+  std::vector<uint32_t> runs, maskbits;
+  for (int t = 0; t < T; ++t) {
+    for (int r = 0; r < 4; ++r) {
+      RotDev rd{};
+      if (r < d->part_nrot[t]) {
+        const int k = t * 4 + r, h = d->rot_h[k], w = d->rot_w[k];
+        const uint8_t* mk = d->masks + d->rot_mask_offset[k];
+        rd.h = h;
+        rd.w = w;
+        rd.mw = (w + 31) / 32;
+        rd.dens_row = (int)dens.size();
+        rd.run_row = (int)run_off.size();
+        rd.mask_base = (int)maskbits.size();
+        rd.imax = 0;
+        rd.dmax = 0;
+        for (int i = 0; i < h; ++i) {
+          run_off.push_back((int32_t)runs.size());
+          int best = 0, j = 0;
+          while (j < w) {
+            if (mk[(size_t)i * w + j]) {
+              const int s = j;
+              while (j < w && mk[(size_t)i * w + j]) ++j;
+              runs.push_back((uint32_t)s | ((uint32_t)(j - s) << 16));
+              best = std::max(best, j - s);
+            } else {
+              ++j;
+            }
+          }
+          dens.push_back((uint16_t)best);
+          if (best > rd.dmax) {
+            rd.dmax = best;
+            rd.imax = i;
+          }
+          for (int wd = 0; wd < rd.mw; ++wd) {
+            uint32_t v = 0;
+            for (int bit = 0; bit < 32 && wd * 32 + bit < w; ++bit)
+              if (mk[(size_t)i * w + wd * 32 + bit]) v |= 1u << bit;
+            maskbits.push_back(v);
+          }
+        }
+        run_off.push_back((int32_t)runs.size());
+      }
+      rot[(size_t)t * 4 + r] = rd;
+    }
+  }
+  pb->mach.resize(M);
+  std::vector<uint8_t> fits((size_t)T * M), newbin_ok((size_t)T * M);
+  for (int m = 0; m < M; ++m) {
+    MachDev& md = pb->mach[m];
+    md.L = d->bin_length[m];
+    md.W = d->bin_width[m];
+    md.NW = (md.W + 31) / 32;
+    md.RS = md.NW + 2;
+    md.area = d->bin_area[m];
+    md.setup = d->setup_time[m];
+    for (int t = 0; t < T; ++t) {
+      const int h0 = d->rot_h[t * 4], w0 = d->rot_w[t * 4];
+      fits[(size_t)t * M + m] = !((h0 > md.L || w0 > md.W) && (w0 > md.L || h0 > md.W));
+      const int rb = d->part_best_rot[t];
+      newbin_ok[(size_t)t * M + m] = d->rot_h[t * 4 + rb] <= md.L && d->rot_w[t * 4 + rb] <= md.W;
+    }
+  }
+  std::vector<double> thr(std::max(1, M - 1), 0.0);
+  for (int m = 0; m + 1 < M; ++m)
+    thr[m] = d->threshold_mode == BRKGA_THRESH_F32 ? (double)(float)d->thresholds[m] : d->thresholds[m];
+  std::vector<int32_t> gene_type(d->gene_type, d->gene_type + N);
+  std::vector<double> pt(d->proc_time, d->proc_time + (size_t)M * T);
+  std::vector<double> pth(d->proc_time_height, d->proc_time_height + (size_t)M * T);
+  std::vector<double> area(d->part_area, d->part_area + T);
+  std::vector<int32_t> nrot(d->part_nrot, d->part_nrot + T), best(d->part_best_rot, d->part_best_rot + T);
+
+  if ((st = upload(pb, &pb->d_gene_type, gene_type)) || (st = upload(pb, &pb->d_thr, thr)) ||
+      (st = upload(pb, &pb->d_mach, pb->mach)) || (st = upload(pb, &pb->d_pt, pt)) ||
+      (st = upload(pb, &pb->d_pth, pth)) || (st = upload(pb, &pb->d_area, area)) ||
+      (st = upload(pb, &pb->d_nrot, nrot)) || (st = upload(pb, &pb->d_best, best)) ||
+      (st = upload(pb, &pb->d_rot, rot)) || (st = upload(pb, &pb->d_dens, dens)) ||
+      (st = upload(pb, &pb->d_run_off, run_off)) || (st = upload(pb, &pb->d_runs, runs)) ||
+      (st = upload(pb, &pb->d_maskbits, maskbits)) || (st = upload(pb, &pb->d_fits, fits)) ||
+      (st = upload(pb, &pb->d_newbin_ok, newbin_ok)) || (st = configure(pb))) {
+    brkga_problem_destroy(pb);
+    return st;
+  }
+  *out = pb;
+  return BRKGA_OK;
+}
+
+int brkga_workspace_bytes(const BrkgaProblem* pb, int32_t P, int64_t pool_bins, size_t* bytes) {
+  if (!pb || !bytes || P < 0 || pool_bins < 0) return BRKGA_ERR_INVALID_ARGUMENT;
+  if (pool_bins == 0) pool_bins = default_pool_bins(pb, P);
+  *bytes = layout_of(pb, P, pool_bins).total;
+  return BRKGA_OK;
+}
+
+int brkga_decode_stage(int32_t stage, const BrkgaProblem* pb, const float* d_chrom, int32_t P,
+                       double* d_makespan, BrkgaPlacement* d_log, int32_t* d_status, void* d_ws,
+                       size_t ws_bytes, int64_t pool_bins, void* stream) {
+  if (!pb || P < 0 || pool_bins < 0 || stage < 0 || stage > 3) return BRKGA_ERR_INVALID_ARGUMENT;
+  if (P == 0) return BRKGA_OK;
+  if (!d_chrom || !d_makespan || !d_status || !d_ws) return BRKGA_ERR_INVALID_ARGUMENT;
+  if ((int64_t)P * pb->M >= (int64_t)1 << 31) return BRKGA_ERR_INVALID_ARGUMENT;
+  if (pool_bins == 0) pool_bins = default_pool_bins(pb, P);
+  const Layout l = layout_of(pb, P, pool_bins);
+  if (ws_bytes < l.total) return BRKGA_ERR_WORKSPACE;
+  DeviceGuard g(pb->device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  char* ws = static_cast<char*>(d_ws);
+  unsigned int* ctr = reinterpret_cast<unsigned int*>(ws + l.off_ctr);
+  unsigned long long* counters = reinterpret_cast<unsigned long long*>(ws + l.off_ctr + 8);
+
+  AssignParams ap;
+  ap.chrom = d_chrom;
+  ap.thr = pb->d_thr;
+  ap.gene_type = pb->d_gene_type;
+  ap.fits = pb->d_fits;
+  ap.N = pb->N;
+  ap.M = pb->M;
+  ap.mode = pb->mode;
+  int S2 = 1;
+  while (S2 < pb->N) S2 <<= 1;
+  ap.S2 = S2;
+  ap.seq = reinterpret_cast<uint16_t*>(ws + l.off_seq);
+  ap.cnt = reinterpret_cast<int32_t*>(ws + l.off_cnt);
+  ap.infeas = reinterpret_cast<int32_t*>(ws + l.off_inf);
+  ap.status = d_status;
+  ap.item_ctr = ctr;
+  ap.pool_ctr = ctr + 1;
+  ap.counters = counters;
+  const int at = std::min(1024, std::max(64, S2 / 2));
+  if (stage == 0 || stage == 1) assign_sort_kernel<<<P, at, (size_t)S2 * 8, s>>>(ap);
+
+  DecodeParams dp;
+  dp.gene_type = pb->d_gene_type;
+  dp.mach = pb->d_mach;
+  dp.pt = pb->d_pt;
+  dp.pth = pb->d_pth;
+  dp.part_area = pb->d_area;
+  dp.nrot = pb->d_nrot;
+  dp.best_rot = pb->d_best;
+  dp.rot = pb->d_rot;
+  dp.dens = pb->d_dens;
+  dp.run_off = pb->d_run_off;
+  dp.runs = pb->d_runs;
+  dp.maskbits = pb->d_maskbits;
+  dp.newbin_ok = pb->d_newbin_ok;
+  dp.N = pb->N;
+  dp.M = pb->M;
+  dp.T = pb->T;
+  dp.P = P;
+  dp.seq = ap.seq;
+  dp.cnt = ap.cnt;
+  dp.infeas = ap.infeas;
+  dp.mk = reinterpret_cast<double*>(ws + l.off_mk);
+  dp.log = d_log;
+  dp.status = d_status;
+  dp.item_ctr = ctr;
+  dp.pool_ctr = ctr + 1;
+  dp.counters = counters;
+  dp.binscal = reinterpret_cast<BinScal*>(ws + l.off_bins);
+  dp.pool = reinterpret_cast<uint32_t*>(ws + l.off_pool);
+  dp.pool_bins = pool_bins;
+  dp.S = pb->S;
+  dp.slot_words = pb->slot_words;
+  dp.slot_vac_off = pb->slot_vac_off;
+  const int grid = (int)std::min<int64_t>(pb->n_slots, (int64_t)P * pb->M);
+  if (stage == 0 || stage == 2) decode_kernel<<<grid, kDecodeThreads, pb->decode_smem, s>>>(dp);
+  if (stage == 0 || stage == 3) reduce_kernel<<<(P + 255) / 256, 256, 0, s>>>(P, pb->M, ap.infeas, dp.mk, d_makespan);
+  return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
+}
+
+int brkga_decode(const BrkgaProblem* pb, const float* d_chrom, int32_t P, double* d_makespan,
+                 BrkgaPlacement* d_log, int32_t* d_status, void* d_ws, size_t ws_bytes, int64_t pool_bins,
+                 void* stream) {
+  return brkga_decode_stage(0, pb, d_chrom, P, d_makespan, d_log, d_status, d_ws, ws_bytes, pool_bins, stream);
+}
+
+int brkga_evaluate_host(BrkgaProblem* pb, const float* h_chrom, int32_t P, double* h_makespan,
+                        BrkgaPlacement* h_log) {
+  if (!pb || P < 0 || (P > 0 && (!h_chrom || !h_makespan))) return BRKGA_ERR_INVALID_ARGUMENT;
+  if (P == 0) return BRKGA_OK;
+  std::lock_guard<std::mutex> lock(pb->mu);
+  DeviceGuard g(pb->device);
+  if (!pb->stream && cudaStreamCreateWithFlags(&pb->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return BRKGA_ERR_CUDA;
+  const bool want_log = h_log != nullptr;
+  if (P > pb->e_cap_P || (want_log && !pb->e_cap_log)) {
+    const int cap = std::max(P, pb->e_cap_P);
+    cudaFree(pb->e_chrom);
+    cudaFree(pb->e_out);
+    cudaFree(pb->e_status);
+    cudaFree(pb->e_log);
+    pb->e_chrom = nullptr;
+    pb->e_out = nullptr;
+    pb->e_status = nullptr;
+    pb->e_log = nullptr;
+    pb->e_cap_P = 0;
+    if (cudaMalloc(&pb->e_chrom, (size_t)cap * 2 * pb->N * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&pb->e_out, (size_t)cap * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&pb->e_status, sizeof(int32_t)) != cudaSuccess)
+      return BRKGA_ERR_CUDA;
+    if ((want_log || pb->e_cap_log) &&
+        cudaMalloc(&pb->e_log, (size_t)cap * pb->M * pb->N * sizeof(BrkgaPlacement)) != cudaSuccess)
+      return BRKGA_ERR_CUDA;
+    pb->e_cap_log = want_log || pb->e_cap_log;
+    pb->e_cap_P = cap;
+  }
+  if (pb->e_pool_bins < default_pool_bins(pb, P)) pb->e_pool_bins = default_pool_bins(pb, P);
+  if (cudaMemcpyAsync(pb->e_chrom, h_chrom, (size_t)P * 2 * pb->N * sizeof(float), cudaMemcpyHostToDevice,
+                      pb->stream) != cudaSuccess)
+    return BRKGA_ERR_CUDA;
+  for (int attempt = 0; attempt < 12; ++attempt) {
+    const size_t need = layout_of(pb, P, pb->e_pool_bins).total;
+    if (need > pb->e_ws_bytes) {
+      if (cudaStreamSynchronize(pb->stream) != cudaSuccess) return BRKGA_ERR_CUDA;
+      cudaFree(pb->e_ws);
+      pb->e_ws = nullptr;
+      pb->e_ws_bytes = 0;
+      if (cudaMalloc(&pb->e_ws, need) != cudaSuccess) return BRKGA_ERR_CUDA;
+      pb->e_ws_bytes = need;
+    }
+    int st = brkga_decode(pb, pb->e_chrom, P, pb->e_out, want_log ? pb->e_log : nullptr, pb->e_status, pb->e_ws,
+                          pb->e_ws_bytes, pb->e_pool_bins, pb->stream);
+    if (st) return st;
+    int32_t status = 0;
+    if (cudaMemcpyAsync(&status, pb->e_status, sizeof(int32_t), cudaMemcpyDeviceToHost, pb->stream) !=
+            cudaSuccess ||
+        cudaMemcpyAsync(h_makespan, pb->e_out, (size_t)P * sizeof(double), cudaMemcpyDeviceToHost,
+                        pb->stream) != cudaSuccess)
+      return BRKGA_ERR_CUDA;
+    unsigned long long counters[4] = {0, 0, 0, 0};
+    const Layout l = layout_of(pb, P, pb->e_pool_bins);
+    if (cudaMemcpyAsync(counters, static_cast<char*>(pb->e_ws) + l.off_ctr + 8, sizeof(counters),
+                        cudaMemcpyDeviceToHost, pb->stream) != cudaSuccess)
+      return BRKGA_ERR_CUDA;
+    if (cudaStreamSynchronize(pb->stream) != cudaSuccess) return BRKGA_ERR_CUDA;
+    for (int i = 0; i < 4; ++i) pb->last_counters[i] = (int64_t)counters[i];
+    if (status == BRKGA_ERR_CAPACITY) {
+      pb->e_pool_bins *= 2;
+      continue;
+    }
+    if (status) return status;
+    if (want_log &&
+        cudaMemcpy(h_log, pb->e_log, (size_t)P * pb->M * pb->N * sizeof(BrkgaPlacement), cudaMemcpyDeviceToHost) !=
+            cudaSuccess)
+      return BRKGA_ERR_CUDA;
+    return BRKGA_OK;
+  }
+  return BRKGA_ERR_CAPACITY;
+}
+
+int brkga_last_counters(const BrkgaProblem* pb, int64_t* tests, int64_t* chunks, int64_t* bins,
+                        int64_t* scan_bytes) {
+  if (!pb) return BRKGA_ERR_INVALID_ARGUMENT;
+  if (tests) *tests = pb->last_counters[0];
+  if (chunks) *chunks = pb->last_counters[1];
+  if (bins) *bins = pb->last_counters[2];
+  if (scan_bytes) *scan_bytes = pb->last_counters[3];
+  return BRKGA_OK;
+}
+
+}  // extern "C"

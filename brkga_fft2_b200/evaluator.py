@@ -1,0 +1,199 @@
+"""Population evaluators over the CUDA decoder.
+
+``B200DecoderEvaluator`` is the drop-in for the reference's
+``FullNativeDecoderEvaluator`` (``full_native_decoder.py:2937-2981``) and
+``WaveBatchEvaluator`` (``wave_batch_evaluator.py:109-191``): same constructor
+arguments, ``evaluate_batch(np.ndarray [P, 2N]) -> list[float]`` with 1e16 for
+infeasible chromosomes, ``RuntimeError`` on bad input.  It goes through the
+host-to-host entry point ``brkga_evaluate_host`` of the C ABI.
+
+``DeviceDecoder`` decodes populations that are already on the GPU (torch
+tensors), stream-ordered and without host synchronisation, through
+``brkga_decode`` with a preallocated workspace — the form the GA loop and the
+throughput benchmark use.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Optional
+
+import numpy as np
+
+from . import abi
+from .problem import THRESH_F32, PackedProblem, pack_problem
+
+
+class _NativeProblem:
+    """Owns one ``BrkgaProblem*`` (device-resident tables)."""
+
+    def __init__(self, packed: PackedProblem):
+        self.lib = abi.load_library()
+        self.packed = packed
+        handle = ctypes.c_void_p()
+        st = self.lib.brkga_problem_create(ctypes.byref(packed.desc), ctypes.byref(handle))
+        abi.check(st, "brkga_problem_create")
+        self.handle = handle
+
+    def close(self):
+        if getattr(self, "handle", None) is not None and self.handle.value:
+            self.lib.brkga_problem_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class B200DecoderEvaluator:
+    """Drop-in evaluator: ``evaluate_batch(population) -> list of makespans``.
+
+    Arguments follow ``FullNativeDecoderEvaluator.__init__``
+    (``full_native_decoder.py:2940-2963``); ``collision_backend`` is accepted
+    and ignored, as there.  ``threshold_mode`` picks how machine keys are
+    compared with the thresholds: ``THRESH_F32`` is ``placement.py``'s
+    behaviour (float32 under NumPy >= 2), ``THRESH_F64`` the C++ decoder's.
+    """
+
+    def __init__(self, problem_data, nb_parts: int, nb_machines: int, thresholds, instance_parts,
+                 collision_backend=None, device: str = "cuda", threshold_mode: int = THRESH_F32):
+        del collision_backend
+        self._set_device(device)
+        self.nb_parts = int(nb_parts)
+        self.nb_machines = int(nb_machines)
+        self.packed = pack_problem(problem_data, nb_parts, nb_machines, thresholds, instance_parts,
+                                   threshold_mode)
+        self._native = _NativeProblem(self.packed)
+        self._lib = self._native.lib
+        self._counters = (0, 0, 0, 0)
+        self._totals = [0, 0, 0, 0]
+
+    @staticmethod
+    def _set_device(device: str):
+        if device is None or not str(device).startswith("cuda"):
+            raise RuntimeError("B200DecoderEvaluator needs a CUDA device (no CPU path)")
+        import torch
+        if not torch.cuda.is_available():
+            raise RuntimeError("CUDA is not available")
+        dev = torch.device(device)
+        torch.cuda.set_device(dev.index if dev.index is not None else 0)
+        torch.cuda.init()
+
+    def _check_input(self, chromosomes) -> np.ndarray:
+        chrom = np.ascontiguousarray(chromosomes, dtype=np.float32)
+        if chrom.ndim != 2:
+            raise RuntimeError("chromosomes must be a 2D float32 array")  # full_native_decoder.py:567-569
+        if chrom.shape[1] != 2 * self.nb_parts:
+            raise RuntimeError("chromosomes second dimension must be 2 * nb_parts")  # :571-573
+        return chrom
+
+    def evaluate_batch(self, chromosomes: np.ndarray, return_log: bool = False):
+        """Makespans of a population (list of float; 1e16 = infeasible)."""
+        chrom = self._check_input(chromosomes)
+        P = chrom.shape[0]
+        out = np.zeros(P, np.float64)
+        log = np.zeros((P, self.nb_machines, self.nb_parts), abi.PLACEMENT_DTYPE) if return_log else None
+        st = self._lib.brkga_evaluate_host(self._native.handle, abi.ptr(chrom, ctypes.c_float), P,
+                                           abi.ptr(out, ctypes.c_double),
+                                           log.ctypes.data_as(ctypes.c_void_p) if return_log else None)
+        if st != abi.OK:
+            raise RuntimeError(f"brkga_evaluate_host failed: {abi.STATUS_NAMES.get(st, st)}")
+        t, r, b, sb = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        self._lib.brkga_last_counters(self._native.handle, ctypes.byref(t), ctypes.byref(r), ctypes.byref(b),
+                                      ctypes.byref(sb))
+        self._counters = (t.value, r.value, b.value, sb.value)
+        self._totals[0] += P
+        self._totals[1] += t.value
+        self._totals[2] += r.value
+        self._totals[3] += b.value
+        return (out.tolist(), log) if return_log else out.tolist()
+
+    @property
+    def last_counters(self):
+        """(placement tests, 32-row chunks searched, plates opened, scan bytes) of the last call."""
+        return self._counters
+
+    def get_profile_summary(self) -> str:
+        """Counterpart of ``FullNativeDecoderEvaluator.get_profile_summary`` (:2970-2975)."""
+        d, t, r, b = self._totals
+        return (f"decodes={d} placement_tests={t} row_chunks={r} plates={b} "
+                f"tests_per_decode={t / max(d, 1):.1f}")
+
+    def reset_profile(self) -> None:
+        self._totals = [0, 0, 0, 0]
+
+    def close(self):
+        self._native.close()
+
+
+class DeviceDecoder:
+    """Stream-ordered decoding of device-resident populations (torch tensors).
+
+    Holds a workspace sized for up to ``max_pop`` chromosomes; ``decode`` is
+    asynchronous (no host synchronisation, no allocation) and therefore safe
+    to capture in a CUDA graph.  Check ``status`` (a device int32) for
+    BRKGA_ERR_CAPACITY after a run when plates may overflow the pool.
+    """
+
+    def __init__(self, packed: PackedProblem, max_pop: int, pool_bins: int = 0, device=None):
+        import torch
+        self.torch = torch
+        self.packed = packed
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        with torch.cuda.device(self.device):
+            torch.cuda.init()
+            self.native = _NativeProblem(packed)
+            self.lib = self.native.lib
+            self.max_pop = int(max_pop)
+            self.pool_bins = int(pool_bins)
+            nbytes = ctypes.c_size_t()
+            abi.check(self.lib.brkga_workspace_bytes(self.native.handle, self.max_pop, self.pool_bins,
+                                                     ctypes.byref(nbytes)), "brkga_workspace_bytes")
+            self.ws_bytes = nbytes.value
+            self.workspace = torch.empty(self.ws_bytes, dtype=torch.uint8, device=self.device)
+            self.status = torch.zeros(1, dtype=torch.int32, device=self.device)
+
+    def workspace_bytes(self, P: int) -> int:
+        nbytes = ctypes.c_size_t()
+        abi.check(self.lib.brkga_workspace_bytes(self.native.handle, int(P), self.pool_bins, ctypes.byref(nbytes)))
+        return nbytes.value
+
+    def decode(self, chrom, out=None, log=None, stream=None, kernel_events=None):
+        """Decode ``chrom`` (cuda float32 [P, 2N]) into ``out`` (cuda float64 [P]).
+
+        ``kernel_events`` = (start, end) torch.cuda.Event pair recorded on the
+        launch stream right around the decode kernel (stage 2).
+        """
+        torch = self.torch
+        if chrom.dtype != torch.float32 or chrom.dim() != 2 or chrom.shape[1] != 2 * self.packed.n_genes:
+            raise RuntimeError("chromosomes must be a float32 [P, 2N] CUDA tensor")
+        if not chrom.is_cuda or not chrom.is_contiguous():
+            raise RuntimeError("chromosomes must be a contiguous CUDA tensor")
+        P = chrom.shape[0]
+        if P > self.max_pop:
+            raise RuntimeError(f"population {P} exceeds the workspace capacity {self.max_pop}")
+        if out is None:
+            out = torch.empty(P, dtype=torch.float64, device=chrom.device)
+        if log is not None and (log.dtype != torch.int32 or tuple(log.shape) != (P, self.packed.n_machines,
+                                                                                  self.packed.n_genes, 5)):
+            raise RuntimeError("log must be int32 [P, M, N, 5]")
+        s = stream if stream is not None else torch.cuda.current_stream(chrom.device)
+        args = (self.native.handle, ctypes.c_void_p(chrom.data_ptr()), P, ctypes.c_void_p(out.data_ptr()),
+                ctypes.c_void_p(log.data_ptr()) if log is not None else None,
+                ctypes.c_void_p(self.status.data_ptr()), ctypes.c_void_p(self.workspace.data_ptr()),
+                self.ws_bytes, self.pool_bins, ctypes.c_void_p(s.cuda_stream))
+        if kernel_events is None:
+            abi.check(self.lib.brkga_decode(*args), "brkga_decode")
+        else:
+            abi.check(self.lib.brkga_decode_stage(1, *args), "brkga_decode_stage")
+            kernel_events[0].record(s)
+            abi.check(self.lib.brkga_decode_stage(2, *args), "brkga_decode_stage")
+            kernel_events[1].record(s)
+            abi.check(self.lib.brkga_decode_stage(3, *args), "brkga_decode_stage")
+        return out
+
+    def counters(self):
+        """(placement tests, row chunks, plates, scan bytes) of the last decode (synchronises)."""
+        c = self.workspace[8:8 + 32].view(self.torch.int64).cpu().tolist()
+        return tuple(int(v) for v in c)

@@ -118,6 +118,16 @@ int brkga_decode(const BrkgaProblem* problem, const float* d_chrom, int32_t P,
                  double* d_makespan, BrkgaPlacement* d_log, int32_t* d_status,
                  void* d_ws, size_t ws_bytes, int64_t pool_bins, void* stream);
 
+/* One stage of brkga_decode with the same arguments: 1 = machine assignment
+ * and key sort, 2 = the decode kernel, 3 = the max-over-machines reduction;
+ * 0 = all three (what brkga_decode does).  Running 1, 2, 3 in order on one
+ * stream equals brkga_decode; lets a caller put its own CUDA events around
+ * the decode kernel.  (No reference counterpart: the reference's phases are
+ * host-driven, full_native_decoder.py:1481-2097.) */
+int brkga_decode_stage(int32_t stage, const BrkgaProblem* problem, const float* d_chrom, int32_t P,
+                       double* d_makespan, BrkgaPlacement* d_log, int32_t* d_status, void* d_ws,
+                       size_t ws_bytes, int64_t pool_bins, void* stream);
+
 /* Host-to-host evaluation, the drop-in for NativeFullDecoder::evaluate_batch
  * (full_native_decoder.py:563-641): copies h_chrom [P, 2N] float32 to the
  * device, decodes, and writes h_makespan [P] float64.  Grows its internal
@@ -126,10 +136,14 @@ int brkga_decode(const BrkgaProblem* problem, const float* d_chrom, int32_t P,
 int brkga_evaluate_host(BrkgaProblem* problem, const float* h_chrom, int32_t P,
                         double* h_makespan, BrkgaPlacement* h_log);
 
-/* Counters of the last brkga_evaluate_host call (placement tests issued to
- * the collision search, candidate rows examined, plates opened). */
-int brkga_last_counters(const BrkgaProblem* problem, int64_t* tests, int64_t* rows,
-                        int64_t* bins);
+/* Counters of the last brkga_evaluate_host call: placement tests (plate x
+ * rotation pairs that passed the size and area filters and went to the
+ * collision search), 32-row candidate chunks searched, plates opened, and
+ * the algorithmic scan bytes sum over tests of 4*(L*ceil(W/32) + h*ceil(w/32))
+ * (one read of the bit-packed plate and rotated mask).  The same four int64
+ * values sit at byte offset 8 of a brkga_decode workspace after the run. */
+int brkga_last_counters(const BrkgaProblem* problem, int64_t* tests, int64_t* chunks, int64_t* bins,
+                        int64_t* scan_bytes);
 
 #ifdef __cplusplus
 }

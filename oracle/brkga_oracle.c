@@ -263,8 +263,12 @@ typedef struct {
 static int cmp_keygene(const void* a, const void* b) {
   const KeyGene* x = (const KeyGene*)a;
   const KeyGene* y = (const KeyGene*)b;
-  if (x->key < y->key) return -1;
-  if (x->key > y->key) return 1;
+  const int xn = x->key != x->key, yn = y->key != y->key; /* NaN sorts last, as in np.argsort */
+  if (xn != yn) return xn - yn;
+  if (!xn) {
+    if (x->key < y->key) return -1;
+    if (x->key > y->key) return 1;
+  }
   return (x->gene > y->gene) - (x->gene < y->gene); /* stable: gene order on ties */
 }
 

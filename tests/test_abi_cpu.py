@@ -1,0 +1,86 @@
+"""CPU-side checks of the C ABI: the library loads, exports every entry point
+declared in include/brkga_b200.h, and validates descriptors before touching a
+device.  No decode runs here (no GPU)."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from brkga_fft2_b200 import abi, build, instances, pack_problem
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    build.build()
+    return abi.load_library()
+
+
+def declared_functions():
+    text = open(os.path.join(REPO, "include", "brkga_b200.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(brkga_[a-z_0-9]+)\s*\(", text)))
+
+
+def test_exports_every_declared_symbol(lib):
+    names = declared_functions()
+    assert "brkga_decode" in names and "brkga_evaluate_host" in names
+    for n in names:
+        assert hasattr(lib, n), n
+
+
+def test_version_and_status_strings(lib):
+    assert lib.brkga_abi_version() == abi.ABI_VERSION
+    for code, name in abi.STATUS_NAMES.items():
+        assert lib.brkga_status_string(code).decode() == name
+
+
+def _packed():
+    inst = instances.small(1, n_parts=6)
+    return pack_problem(inst.problem_data, inst.nb_parts, inst.nb_machines, inst.thresholds,
+                        inst.instance_parts)
+
+
+def _create(lib, packed):
+    h = ctypes.c_void_p()
+    st = lib.brkga_problem_create(ctypes.byref(packed.desc), ctypes.byref(h))
+    if st == abi.OK:
+        lib.brkga_problem_destroy(h)
+    return st
+
+
+def test_create_rejects_bad_descriptors(lib):
+    pk = _packed()
+    assert lib.brkga_problem_create(None, ctypes.byref(ctypes.c_void_p())) == abi.ERR_INVALID_ARGUMENT
+    pk.arrays["gene_type"][0] = 99
+    assert _create(lib, pk) == abi.ERR_BAD_INSTANCE
+    pk = _packed()
+    pk.arrays["part_area"][0] = 0.0
+    assert _create(lib, pk) == abi.ERR_BAD_INSTANCE
+    pk = _packed()
+    pk.arrays["masks"][0] = 2
+    assert _create(lib, pk) == abi.ERR_BAD_INSTANCE
+    pk = _packed()
+    pk.arrays["part_best_rot"][0] = 4
+    assert _create(lib, pk) == abi.ERR_BAD_INSTANCE
+    pk = _packed()
+    pk.desc.threshold_mode = 7
+    assert _create(lib, pk) == abi.ERR_INVALID_ARGUMENT
+
+
+def test_create_without_gpu_reports_no_device(lib):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    assert _create(lib, _packed()) == abi.ERR_NO_DEVICE
+
+
+def test_null_problem_arguments(lib):
+    n = ctypes.c_size_t()
+    assert lib.brkga_workspace_bytes(None, 10, 0, ctypes.byref(n)) == abi.ERR_INVALID_ARGUMENT
+    assert lib.brkga_decode(None, None, 1, None, None, None, None, 0, 0, None) == abi.ERR_INVALID_ARGUMENT
+    assert lib.brkga_evaluate_host(None, None, 1, None, None) == abi.ERR_INVALID_ARGUMENT
+    lib.brkga_problem_destroy(None)
