@@ -12,6 +12,7 @@ import os
 import numpy as np
 
 ABI_VERSION = 1
+NOALLOC_SCRATCH_BYTES = 64 << 20  # BRKGA_NOALLOC_SCRATCH_BYTES
 
 OK = 0
 ERR_INVALID_ARGUMENT = 1
@@ -112,6 +113,7 @@ def load_library(path: str = LIB_PATH):
         "brkga_workspace_bytes": (c_int, [vp, c_i32, c_i64, P(c_sz)]),
         "brkga_decode": (c_int, [vp, vp, c_i32, vp, vp, vp, vp, c_sz, c_i64, vp]),
         "brkga_decode_stage": (c_int, [c_i32, vp, vp, c_i32, vp, vp, vp, vp, c_sz, c_i64, vp]),
+        "brkga_decode_noalloc": (c_int, [vp, vp, c_i32, vp, vp, vp, vp]),
         "brkga_evaluate_host": (c_int, [vp, P(ctypes.c_float), c_i32, P(ctypes.c_double), vp]),
         "brkga_last_counters": (c_int, [vp, P(c_i64), P(c_i64), P(c_i64), P(c_i64)]),
     }

@@ -546,8 +546,14 @@ struct Layout {
 
 }  // namespace
 
+// Fixed device scratch for brkga_decode_noalloc: every GPU that loads this
+// library reserves it until the process exits.  Host code must not use the
+// symbol as an address; brkga_problem_create looks up its device address.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[BRKGA_NOALLOC_SCRATCH_BYTES];
+
 struct BrkgaProblem {
   int device = 0;
+  void* noalloc_scratch = nullptr;  // device address of g_noalloc_scratch on `device`
   int N = 0, M = 0, T = 0, mode = 0;
   int sm_count = 0;
   int S = 0, slot_words = 0, slot_vac_off = 0;
@@ -863,6 +869,10 @@ int brkga_problem_create(const BrkgaProblemDesc* d, BrkgaProblem** out) {
     brkga_problem_destroy(pb);
     return st;
   }
+  if (cudaGetSymbolAddress(&pb->noalloc_scratch, g_noalloc_scratch) != cudaSuccess) {
+    brkga_problem_destroy(pb);
+    return BRKGA_ERR_CUDA;
+  }
   *out = pb;
   return BRKGA_OK;
 }
@@ -954,6 +964,24 @@ int brkga_decode(const BrkgaProblem* pb, const float* d_chrom, int32_t P, double
                  BrkgaPlacement* d_log, int32_t* d_status, void* d_ws, size_t ws_bytes, int64_t pool_bins,
                  void* stream) {
   return brkga_decode_stage(0, pb, d_chrom, P, d_makespan, d_log, d_status, d_ws, ws_bytes, pool_bins, stream);
+}
+
+// Decode without allocating: the workspace is the library's fixed device
+// array (address resolved when the problem was created), the bin pool takes
+// whatever that array has left after the per-population tables.
+int brkga_decode_noalloc(const BrkgaProblem* pb, const float* d_chrom, int32_t P, double* d_makespan,
+                         BrkgaPlacement* d_log, int32_t* d_status, void* stream) {
+  if (!pb || P < 0) return BRKGA_ERR_INVALID_ARGUMENT;
+  if (P == 0) return BRKGA_OK;
+  if (!pb->noalloc_scratch) return BRKGA_ERR_INVALID_ARGUMENT;
+  const size_t cap = (size_t)BRKGA_NOALLOC_SCRATCH_BYTES;
+  const Layout fixed = layout_of(pb, P, 0);  // offsets up to the pool do not depend on the pool size
+  if (fixed.off_pool >= cap) return BRKGA_ERR_WORKSPACE;
+  int64_t pool_bins = (int64_t)((cap - fixed.off_pool) / ((size_t)pb->slot_words * sizeof(uint32_t)));
+  while (pool_bins > 0 && layout_of(pb, P, pool_bins).total > cap) --pool_bins;  // 256-byte rounding
+  if (pool_bins < 1) return BRKGA_ERR_WORKSPACE;
+  return brkga_decode_stage(0, pb, d_chrom, P, d_makespan, d_log, d_status, pb->noalloc_scratch, cap,
+                            pool_bins, stream);
 }
 
 int brkga_evaluate_host(BrkgaProblem* pb, const float* h_chrom, int32_t P, double* h_makespan,

@@ -128,6 +128,28 @@ int brkga_decode_stage(int32_t stage, const BrkgaProblem* problem, const float* 
                        double* d_makespan, BrkgaPlacement* d_log, int32_t* d_status, void* d_ws,
                        size_t ws_bytes, int64_t pool_bins, void* stream);
 
+/* Size of the library's fixed device scratch used by brkga_decode_noalloc:
+ * 64 MiB, reserved on every GPU that loads the library until the process exits. */
+#define BRKGA_NOALLOC_SCRATCH_BYTES (64u << 20)
+
+/* brkga_decode for callers that must not allocate device memory — code that
+ * runs under a memory manager owning every device byte (a plugin host, an
+ * embedded scheduler), or a loop that must never hit cudaMalloc/cudaFree
+ * because those can synchronise the device.  No reference counterpart: the
+ * reference grows its workspaces as it goes.
+ * Same inputs and outputs as brkga_decode, but the workspace is a fixed
+ * 64 MiB array inside the library, so nothing is allocated or freed here.
+ * Its device address is looked up by brkga_problem_create (set-up, with the
+ * problem's device current).  The per-population tables must fit in it
+ * (else BRKGA_ERR_WORKSPACE, before any launch); the plate pool gets the rest,
+ * and running out of it sets *d_status = BRKGA_ERR_CAPACITY (decode a smaller
+ * batch then).  All calls share the one array: calls that overlap on the GPU
+ * (other streams, other problems, other threads) race and must be ordered by
+ * the caller.  Nothing needs clearing between calls — each decode resets the
+ * counters it uses. */
+int brkga_decode_noalloc(const BrkgaProblem* problem, const float* d_chrom, int32_t P,
+                         double* d_makespan, BrkgaPlacement* d_log, int32_t* d_status, void* stream);
+
 /* Host-to-host evaluation, the drop-in for NativeFullDecoder::evaluate_batch
  * (full_native_decoder.py:563-641): copies h_chrom [P, 2N] float32 to the
  * device, decodes, and writes h_makespan [P] float64.  Grows its internal
