@@ -84,6 +84,7 @@ struct DecodeParams {
   const uint16_t* seq;
   const int32_t* cnt;
   const int32_t* infeas;
+  const int32_t* order;
   double* mk;
   BrkgaPlacement* log;
   int32_t* status;
@@ -191,14 +192,17 @@ __device__ __forceinline__ uint32_t blocked(const uint32_t* row, int p0, int d) 
 
 __device__ __forceinline__ bool vacancy_ok(const uint16_t* vac, int ty, const RotDev& rd,
                                            const uint16_t* dens) {
-  if (vac[ty + rd.imax] < rd.dmax) return false;
+  if (vac[ty + rd.imax] < rd.dmax) return false;  // widest row first, then bottom to top
   const uint16_t* d = dens + rd.dens_row;
-  for (int i = 0; i < rd.h; ++i)
+  for (int i = rd.h - 1; i >= 0; --i)
     if (vac[ty + i] < __ldg(d + i)) return false;
   return true;
 }
 
 // Leftmost x at which the rotation fits with its top row at ty, or -1.
+// Output words (32 candidate x each) are tried left to right; inside a word
+// the mask rows go widest row first, then bottom to top: plates fill from
+// the bottom, so those rows reject a blocked candidate soonest.
 __device__ int first_free_x(const uint32_t* grid, int RS, int W, int ty, const RotDev& rd,
                             const int32_t* run_off, const uint32_t* runs) {
   const int nx = W - rd.w + 1;
@@ -207,7 +211,9 @@ __device__ int first_free_x(const uint32_t* grid, int RS, int W, int ty, const R
   for (int k = 0; k < nwo; ++k) {
     uint32_t F = (k == nwo - 1 && (nx & 31)) ? ((1u << (nx & 31)) - 1u) : 0xFFFFFFFFu;
     const int base = k << 5;
-    for (int i = 0; i < rd.h && F; ++i) {
+    for (int ii = -1; ii < rd.h && F; ++ii) {
+      const int i = ii < 0 ? rd.imax : rd.h - 1 - ii;
+      if (ii >= 0 && i == rd.imax) continue;
       const uint32_t* row = grid + (size_t)(ty + i) * RS;
       const int q1 = __ldg(ro + i + 1);
       for (int q = __ldg(ro + i); q < q1 && F; ++q) {
@@ -317,6 +323,28 @@ __global__ void assign_sort_kernel(AssignParams p) {
   if (tid == 0) p.infeas[c] = s_inf;
 }
 
+// Items in decreasing part count (infeasible chromosomes last): the persistent
+// CTAs pull them in this order, so the longest decodes start first.
+__global__ void order_items_kernel(int n_items, int M, int N, const int32_t* cnt, const int32_t* infeas,
+                                   int32_t* order) {
+  extern __shared__ int start[];  // N + 1 weights
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int i = tid; i <= N; i += nt) start[i] = 0;
+  __syncthreads();
+  for (int i = tid; i < n_items; i += nt) atomicAdd(&start[infeas[i / M] ? 0 : cnt[i]], 1);
+  __syncthreads();
+  if (tid == 0) {
+    int acc = 0;
+    for (int w = N; w >= 0; --w) {
+      const int h = start[w];
+      start[w] = acc;
+      acc += h;
+    }
+  }
+  __syncthreads();
+  for (int i = tid; i < n_items; i += nt) order[atomicAdd(&start[infeas[i / M] ? 0 : cnt[i]], 1)] = i;
+}
+
 __global__ void __launch_bounds__(kDecodeThreads) decode_kernel(DecodeParams p) {
   extern __shared__ __align__(16) uint32_t smem[];
   __shared__ unsigned long long s_best;
@@ -328,7 +356,10 @@ __global__ void __launch_bounds__(kDecodeThreads) decode_kernel(DecodeParams p) 
   const int n_items = p.P * p.M;
 
   for (;;) {
-    if (tid == 0) s_item = (int)atomicAdd(p.item_ctr, 1u);
+    if (tid == 0) {
+      const int q = (int)atomicAdd(p.item_ctr, 1u);
+      s_item = q < n_items ? p.order[q] : n_items;
+    }
     __syncthreads();
     const int item = s_item;
     __syncthreads();
@@ -541,7 +572,7 @@ __global__ void reduce_kernel(int P, int M, const int32_t* infeas, const double*
 size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 struct Layout {
-  size_t off_ctr, off_seq, off_cnt, off_inf, off_mk, off_bins, off_pool, total;
+  size_t off_ctr, off_seq, off_cnt, off_inf, off_ord, off_mk, off_bins, off_pool, total;
 };
 
 }  // namespace
@@ -604,6 +635,8 @@ Layout layout_of(const BrkgaProblem* pb, int32_t P, int64_t pool_bins) {
   o += (size_t)P * pb->M * sizeof(int32_t);
   l.off_inf = o = align_up(o, 256);
   o += (size_t)P * sizeof(int32_t);
+  l.off_ord = o = align_up(o, 256);
+  o += (size_t)P * pb->M * sizeof(int32_t);
   l.off_mk = o = align_up(o, 256);
   o += (size_t)P * pb->M * sizeof(double);
   l.off_bins = o = align_up(o, 256);
@@ -678,6 +711,9 @@ int configure(BrkgaProblem* pb) {
     return BRKGA_ERR_CUDA;
   if (cudaFuncSetAttribute(assign_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            kMaxGenes * 8) != cudaSuccess)
+    return BRKGA_ERR_CUDA;
+  if (cudaFuncSetAttribute(order_items_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (kMaxGenes + 1) * (int)sizeof(int)) != cudaSuccess)
     return BRKGA_ERR_CUDA;
   int occ = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, decode_kernel, kDecodeThreads, pb->decode_smem) !=
@@ -919,7 +955,12 @@ int brkga_decode_stage(int32_t stage, const BrkgaProblem* pb, const float* d_chr
   ap.pool_ctr = ctr + 1;
   ap.counters = counters;
   const int at = std::min(1024, std::max(64, S2 / 2));
-  if (stage == 0 || stage == 1) assign_sort_kernel<<<P, at, (size_t)S2 * 8, s>>>(ap);
+  int32_t* order = reinterpret_cast<int32_t*>(ws + l.off_ord);
+  if (stage == 0 || stage == 1) {
+    assign_sort_kernel<<<P, at, (size_t)S2 * 8, s>>>(ap);
+    order_items_kernel<<<1, 1024, (size_t)(pb->N + 1) * sizeof(int), s>>>(P * pb->M, pb->M, pb->N, ap.cnt,
+                                                                          ap.infeas, order);
+  }
 
   DecodeParams dp;
   dp.gene_type = pb->d_gene_type;
@@ -942,6 +983,7 @@ int brkga_decode_stage(int32_t stage, const BrkgaProblem* pb, const float* d_chr
   dp.seq = ap.seq;
   dp.cnt = ap.cnt;
   dp.infeas = ap.infeas;
+  dp.order = order;
   dp.mk = reinterpret_cast<double*>(ws + l.off_mk);
   dp.log = d_log;
   dp.status = d_status;
