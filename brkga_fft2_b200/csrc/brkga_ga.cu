@@ -1,0 +1,253 @@
+// brkga_ga.cu — the BRKGA generation step on the GPU (C ABI in include/brkga_b200.h).
+//
+// One generation of the reference's GA loop (BRKGA_alg3.py:229-265):
+//   rank      sort the population by fitness (partition, :178-186): elites are
+//             the n_elites best, in ascending fitness; ties keep the lower index
+//   breed     new population = [elites | mutants | offspring] (:246-250):
+//             mutants are uniform [0,1) keys (:207-208); each offspring takes
+//             one random elite and one random non-elite parent and copies each
+//             key from the elite with probability rho (:188-205)
+//   decode    (brkga_decode on rows n_elites..P-1; elites keep their fitness)
+//   track     per-generation min and mean fitness (:255-262), best-so-far
+//             chromosome, generation counter
+// Randomness is counter-based Philox4x32-10 (Salmon, Moraes, Dror, Shaw,
+// "Parallel random numbers: as easy as 1, 2, 3", SC'11), keyed by the run
+// seed and indexed by (gene block, row, generation, stream tag), so every
+// kernel is deterministic and replayable inside a CUDA graph: the generation
+// number is read from device memory, not baked into the launch.
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "../../include/brkga_b200.h"
+
+namespace {
+
+constexpr int kMaxRank = 8192;  // single-CTA bitonic sort: 8192 x 12 B in shared memory
+
+enum Tag : uint32_t { kTagInit = 0, kTagMutant = 1, kTagMask = 2, kTagParents = 3 };
+
+struct U4 {
+  uint32_t x, y, z, w;
+};
+
+__host__ __device__ inline uint32_t mulhi32(uint32_t a, uint32_t b) {
+  return (uint32_t)(((uint64_t)a * b) >> 32);
+}
+
+// Philox4x32 with 10 rounds: round(c, k) = (hi(M1*c2) ^ c1 ^ k0, lo(M1*c2),
+// hi(M0*c0) ^ c3 ^ k1, lo(M0*c0)); the key is bumped by the Weyl constants
+// between rounds.
+__host__ __device__ inline U4 philox(U4 c, uint32_t k0, uint32_t k1) {
+  for (int r = 0; r < 10; ++r) {
+    if (r) {
+      k0 += 0x9E3779B9u;
+      k1 += 0xBB67AE85u;
+    }
+    const uint32_t lo0 = 0xD2511F53u * c.x, hi0 = mulhi32(0xD2511F53u, c.x);
+    const uint32_t lo1 = 0xCD9E8D57u * c.z, hi1 = mulhi32(0xCD9E8D57u, c.z);
+    c = U4{hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0};
+  }
+  return c;
+}
+
+// 24 random bits -> float in [0, 1), exactly representable
+__device__ inline float unit_float(uint32_t v) { return (float)(v >> 8) * (1.0f / 16777216.0f); }
+
+__device__ inline unsigned long long ordered_f64(double v) {
+  unsigned long long u = (unsigned long long)__double_as_longlong(v);
+  if (v == 0.0) u = 0ull;
+  if (v != v) u = 0x7FF8000000000000ull;  // NaN (a failed decode) ranks last
+  return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
+}
+
+__global__ void init_population_kernel(float* pop, int P, int K, uint32_t k0, uint32_t k1, int skip_rows) {
+  const int blocks = (K + 3) >> 2;
+  const long long n = (long long)P * blocks;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int row = (int)(i / blocks), b = (int)(i - (long long)row * blocks);
+    if (row < skip_rows) continue;
+    const U4 r = philox(U4{(uint32_t)b, (uint32_t)row, 0u, kTagInit}, k0, k1);
+    const uint32_t v[4] = {r.x, r.y, r.z, r.w};
+    for (int q = 0; q < 4 && 4 * b + q < K; ++q) pop[(size_t)row * K + 4 * b + q] = unit_float(v[q]);
+  }
+}
+
+__global__ void rank_kernel(const double* fit, int P, int S2, int32_t* order) {
+  extern __shared__ unsigned long long sm[];
+  unsigned long long* key = sm;
+  int* idx = reinterpret_cast<int*>(sm + S2);
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int i = tid; i < S2; i += nt) {
+    key[i] = i < P ? ordered_f64(fit[i]) : ~0ull;
+    idx[i] = i < P ? i : 0x7FFFFFFF;
+  }
+  __syncthreads();
+  for (int k = 2; k <= S2; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = tid; i < S2; i += nt) {
+        const int ixj = i ^ j;
+        if (ixj > i) {
+          const unsigned long long a = key[i], b = key[ixj];
+          const int ia = idx[i], ib = idx[ixj];
+          const bool gt = a > b || (a == b && ia > ib);
+          if (gt == ((i & k) == 0)) {
+            key[i] = b;
+            key[ixj] = a;
+            idx[i] = ib;
+            idx[ixj] = ia;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  for (int i = tid; i < P; i += nt) order[i] = idx[i];
+}
+
+// One thread per (row, 4-key block) of the new population.
+__global__ void breed_kernel(const float* pop, const double* fit, const int32_t* order, int P, int K, int ne,
+                             int nm, float rho, uint32_t k0, uint32_t k1, const long long* generation, float* next,
+                             double* next_fit) {
+  const uint32_t gen = (uint32_t)(*generation);
+  const int blocks = (K + 3) >> 2;
+  const long long n = (long long)P * blocks;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int row = (int)(i / blocks), b = (int)(i - (long long)row * blocks);
+    float* dst = next + (size_t)row * K + 4 * b;
+    const int nk = min(4, K - 4 * b);
+    if (row < ne) {  // elites, best first
+      const float* src = pop + (size_t)order[row] * K + 4 * b;
+      for (int q = 0; q < nk; ++q) dst[q] = src[q];
+      if (b == 0) next_fit[row] = fit[order[row]];
+    } else if (row < ne + nm) {  // mutants
+      const U4 r = philox(U4{(uint32_t)b, (uint32_t)row, gen, kTagMutant}, k0, k1);
+      const uint32_t v[4] = {r.x, r.y, r.z, r.w};
+      for (int q = 0; q < nk; ++q) dst[q] = unit_float(v[q]);
+    } else {  // offspring of one elite and one non-elite parent
+      const U4 pr = philox(U4{0u, (uint32_t)row, gen, kTagParents}, k0, k1);
+      const int e = order[(int)mulhi32(pr.x, (uint32_t)ne)];
+      const int o = order[ne + (int)mulhi32(pr.y, (uint32_t)(P - ne))];
+      const U4 r = philox(U4{(uint32_t)b, (uint32_t)row, gen, kTagMask}, k0, k1);
+      const uint32_t v[4] = {r.x, r.y, r.z, r.w};
+      for (int q = 0; q < nk; ++q) {
+        const int g = 4 * b + q;
+        dst[q] = unit_float(v[q]) < rho ? pop[(size_t)e * K + g] : pop[(size_t)o * K + g];
+      }
+    }
+  }
+}
+
+// Min and mean of the fitness (history), best-so-far chromosome, generation++.
+__global__ void track_kernel(const double* fit, const float* pop, int P, int K, long long* generation,
+                             double* history, int history_len, double* best_fit, float* best_sol) {
+  __shared__ double s_min[1024], s_sum[1024];
+  __shared__ int s_arg[1024];
+  const int tid = threadIdx.x, nt = blockDim.x;
+  double mn = INFINITY, sum = 0.0;
+  int arg = 0x7FFFFFFF;
+  // fixed per-thread order, then a fixed tree: the mean does not depend on scheduling
+  for (int i = tid; i < P; i += nt) {
+    const double v = fit[i];
+    sum += v;
+    if (v < mn || (v == mn && i < arg)) {
+      mn = v;
+      arg = i;
+    }
+  }
+  s_min[tid] = mn;
+  s_sum[tid] = sum;
+  s_arg[tid] = arg;
+  __syncthreads();
+  for (int h = nt >> 1; h > 0; h >>= 1) {
+    if (tid < h) {
+      s_sum[tid] += s_sum[tid + h];
+      const double a = s_min[tid], b = s_min[tid + h];
+      if (b < a || (b == a && s_arg[tid + h] < s_arg[tid])) {
+        s_min[tid] = b;
+        s_arg[tid] = s_arg[tid + h];
+      }
+    }
+    __syncthreads();
+  }
+  const long long g = *generation;
+  const bool better = s_arg[0] < P && s_min[0] < *best_fit;
+  __syncthreads();
+  if (better)
+    for (int k = tid; k < K; k += nt) best_sol[k] = pop[(size_t)s_arg[0] * K + k];
+  if (tid == 0) {
+    if (g >= 0 && g < history_len) {
+      history[2 * g] = s_min[0];
+      history[2 * g + 1] = s_sum[0] / (double)P;
+    }
+    if (better) *best_fit = s_min[0];
+    *generation = g + 1;
+  }
+}
+
+int grid_for(long long n) {
+  long long g = (n + 255) / 256;
+  if (g > 148 * 16) g = 148 * 16;
+  return (int)(g < 1 ? 1 : g);
+}
+
+}  // namespace
+
+extern "C" {
+
+int brkga_ga_init_population(float* d_pop, int32_t P, int32_t n_keys, uint64_t seed, int32_t skip_rows,
+                             void* stream) {
+  if (P < 0 || n_keys < 1 || skip_rows < 0 || (P > 0 && !d_pop)) return BRKGA_ERR_INVALID_ARGUMENT;
+  if (P == 0) return BRKGA_OK;
+  init_population_kernel<<<grid_for((long long)P * ((n_keys + 3) / 4)), 256, 0, (cudaStream_t)stream>>>(
+      d_pop, P, n_keys, (uint32_t)seed, (uint32_t)(seed >> 32), skip_rows);
+  return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
+}
+
+int brkga_ga_rank(const double* d_fitness, int32_t P, int32_t* d_order, void* stream) {
+  if (P < 0 || P > kMaxRank || (P > 0 && (!d_fitness || !d_order))) return BRKGA_ERR_INVALID_ARGUMENT;
+  if (P == 0) return BRKGA_OK;
+  int S2 = 1;
+  while (S2 < P) S2 <<= 1;
+  const size_t smem = (size_t)S2 * (sizeof(unsigned long long) + sizeof(int));
+  if (smem > 48 * 1024) {  // above the default limit: opt in once per device (first call outside capture)
+    static int opted[64] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return BRKGA_ERR_CUDA;
+    if (!opted[dev]) {
+      if (cudaFuncSetAttribute(rank_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               kMaxRank * (int)(sizeof(unsigned long long) + sizeof(int))) != cudaSuccess)
+        return BRKGA_ERR_CUDA;
+      opted[dev] = 1;
+    }
+  }
+  rank_kernel<<<1, 1024, smem, (cudaStream_t)stream>>>(d_fitness, P, S2, d_order);
+  return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
+}
+
+int brkga_ga_breed(const float* d_pop, const double* d_fitness, const int32_t* d_order, int32_t P, int32_t n_keys,
+                   int32_t n_elites, int32_t n_mutants, float rho, uint64_t seed, const int64_t* d_generation,
+                   float* d_next_pop, double* d_next_fitness, void* stream) {
+  if (P < 1 || n_keys < 1 || n_elites < 1 || n_mutants < 0 || n_elites + n_mutants > P || !d_pop || !d_fitness ||
+      !d_order || !d_generation || !d_next_pop || !d_next_fitness || d_pop == d_next_pop)
+    return BRKGA_ERR_INVALID_ARGUMENT;
+  breed_kernel<<<grid_for((long long)P * ((n_keys + 3) / 4)), 256, 0, (cudaStream_t)stream>>>(
+      d_pop, d_fitness, d_order, P, n_keys, n_elites, n_mutants, rho, (uint32_t)seed, (uint32_t)(seed >> 32),
+      reinterpret_cast<const long long*>(d_generation), d_next_pop, d_next_fitness);
+  return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
+}
+
+int brkga_ga_track(const double* d_fitness, const float* d_pop, int32_t P, int32_t n_keys, int64_t* d_generation,
+                   double* d_history, int32_t history_len, double* d_best_fitness, float* d_best_solution,
+                   void* stream) {
+  if (P < 1 || n_keys < 1 || !d_fitness || !d_pop || !d_generation || (history_len > 0 && !d_history) ||
+      !d_best_fitness || !d_best_solution)
+    return BRKGA_ERR_INVALID_ARGUMENT;
+  track_kernel<<<1, 1024, 0, (cudaStream_t)stream>>>(d_fitness, d_pop, P, n_keys,
+                                                     reinterpret_cast<long long*>(d_generation), d_history,
+                                                     history_len, d_best_fitness, d_best_solution);
+  return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
+}
+
+}  // extern "C"

@@ -167,6 +167,38 @@ int brkga_evaluate_host(BrkgaProblem* problem, const float* h_chrom, int32_t P,
 int brkga_last_counters(const BrkgaProblem* problem, int64_t* tests, int64_t* chunks, int64_t* bins,
                         int64_t* scan_bytes);
 
+/* ---- GA generation step (device-resident population; BRKGA_alg3.py:210-265) ----
+ * Randomness: Philox4x32-10 keyed by `seed`, counters (key block, row,
+ * generation, stream), so results are deterministic and independent of the
+ * launch configuration.  The reference draws from NumPy's global MT19937, so
+ * GA trajectories are not comparable draw for draw; the operators are. */
+
+/* Uniform [0,1) float32 keys for rows skip_rows..P-1 of d_pop [P, n_keys]
+ * (initial population, BRKGA_alg3.py:213). */
+int brkga_ga_init_population(float* d_pop, int32_t P, int32_t n_keys, uint64_t seed, int32_t skip_rows,
+                             void* stream);
+
+/* d_order[P] = indices sorting d_fitness ascending, ties by index; NaN last.
+ * P <= 8192.  Replaces partition (BRKGA_alg3.py:178-186).  For P > 4096 the
+ * first call on a device sets a kernel attribute, so make it outside graph capture. */
+int brkga_ga_rank(const double* d_fitness, int32_t P, int32_t* d_order, void* stream);
+
+/* Next population [elites | mutants | offspring] (BRKGA_alg3.py:188-208,246-250):
+ * rows 0..n_elites-1 copy the best rows (and their fitness into d_next_fitness),
+ * the next n_mutants rows are uniform keys, the rest are offspring of a uniform
+ * elite and a uniform non-elite parent, each key taken from the elite with
+ * probability rho.  The generation number is read from *d_generation. */
+int brkga_ga_breed(const float* d_pop, const double* d_fitness, const int32_t* d_order, int32_t P,
+                   int32_t n_keys, int32_t n_elites, int32_t n_mutants, float rho, uint64_t seed,
+                   const int64_t* d_generation, float* d_next_pop, double* d_next_fitness, void* stream);
+
+/* After a population is scored: history[2g] = min, history[2g+1] = mean of
+ * d_fitness for g = *d_generation (BRKGA_alg3.py:224-227,255-262); copies the
+ * best row into d_best_solution when it beats *d_best_fitness; then ++*d_generation. */
+int brkga_ga_track(const double* d_fitness, const float* d_pop, int32_t P, int32_t n_keys,
+                   int64_t* d_generation, double* d_history, int32_t history_len, double* d_best_fitness,
+                   float* d_best_solution, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

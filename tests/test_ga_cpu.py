@@ -1,0 +1,49 @@
+"""GA oracle checks on the CPU: Philox4x32-10 known answers and the
+operators of BRKGA_alg3.py:178-265 as restated for the device GA."""
+import numpy as np
+
+from brkga_fft2_b200 import instances, pack_problem
+from oracle import ga_oracle as go
+
+
+def test_philox_known_answers():
+    """Known-answer vectors of Philox4x32-10 (Random123 distribution, kat_vectors)."""
+    kat = [((0, 0, 0, 0), (0, 0), (0x6627e8d5, 0xe169c58d, 0xbc57ac4c, 0x9b00dbd8)),
+           ((0xffffffff,) * 4, (0xffffffff, 0xffffffff), (0x408f276d, 0x41c83b0e, 0xa20bc7c6, 0x6d5451fd)),
+           ((0x243f6a88, 0x85a308d3, 0x13198a2e, 0x03707344), (0xa4093822, 0x299f31d0),
+            (0xd16cfe09, 0x94fdcceb, 0x5001e420, 0x24126ea1))]
+    for c, k, want in kat:
+        got = tuple(int(v) for v in go.philox(*c, seed=k[0] | (k[1] << 32)))
+        assert got == want
+
+
+def test_breed_structure():
+    rng = np.random.default_rng(0)
+    P, K, ne, nm = 40, 18, 6, 8
+    pop = rng.random((P, K)).astype(np.float32)
+    fit = rng.random(P) * 100
+    order = go.rank(fit)
+    assert (np.diff(fit[order]) >= 0).all()
+    nxt, nfit = go.breed(pop, fit, order, ne, nm, 0.7, seed=5, gen=3)
+    np.testing.assert_array_equal(nxt[:ne], pop[order[:ne]])       # elites, best first
+    np.testing.assert_array_equal(nfit[:ne], fit[order[:ne]])
+    assert ((nxt[ne:ne + nm] >= 0) & (nxt[ne:ne + nm] < 1)).all()    # mutants
+    elites, others = set(order[:ne]), set(order[ne:])
+    frac = []
+    for r in range(ne + nm, P):                                    # each offspring key from its two parents
+        child = nxt[r]
+        from_e = [e for e in elites if np.isin(child, pop[e]).sum() > 0]
+        assert from_e
+        frac.append(np.mean([np.any(pop[list(elites)][:, g] == child[g]) for g in range(K)]))
+    assert 0.5 < np.mean(frac) <= 1.0
+
+
+def test_small_run_history():
+    inst = instances.small(2, n_parts=10)
+    pk = pack_problem(inst.problem_data, inst.nb_parts, inst.nb_machines, inst.thresholds, inst.instance_parts)
+    pop, fit, hist, best, sol = go.run(pk, P=24, ne=4, nm=5, rho=0.7, seed=3, generations=4)
+    assert hist.shape == (5, 2)
+    assert (np.diff(hist[:, 0]) <= 0).all()       # elites survive: the minimum never increases
+    assert best == hist[-1, 0] == fit.min()
+    from oracle import oracle_decode
+    assert oracle_decode(pk, sol[None])[0] == best

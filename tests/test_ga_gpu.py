@@ -1,0 +1,82 @@
+"""Device GA step vs the NumPy oracle of the same operators: bit-exact
+populations, fitness, history and best solution; CUDA-graph replay equals
+eager execution."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from brkga_fft2_b200 import abi, instances, pack_problem
+from oracle import ga_oracle as go
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.fail("CUDA device required")
+    from brkga_fft2_b200 import build
+    build.build()
+    return torch
+
+
+def _p(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def test_kernels_match_oracle(torch):
+    lib = abi.load_library()
+    P, K, ne, nm, seed = 300, 42, 30, 45, 0x1234_5678_9ABC
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    pop = torch.zeros(P, K, dtype=torch.float32, device="cuda")
+    assert lib.brkga_ga_init_population(_p(pop), P, K, ctypes.c_uint64(seed), 0, s) == 0
+    np.testing.assert_array_equal(pop.cpu().numpy(), go.init_population(P, K, seed))
+    rng = np.random.default_rng(1)
+    fit_h = np.round(rng.random(P) * 50)            # many ties
+    fit_h[7] = np.nan
+    fit = torch.from_numpy(fit_h).cuda()
+    order = torch.zeros(P, dtype=torch.int32, device="cuda")
+    assert lib.brkga_ga_rank(_p(fit), P, _p(order), s) == 0
+    np.testing.assert_array_equal(order.cpu().numpy(), go.rank(fit_h))
+    gen = torch.full((1,), 17, dtype=torch.int64, device="cuda")
+    nxt = torch.zeros_like(pop)
+    nfit = torch.zeros_like(fit)
+    assert lib.brkga_ga_breed(_p(pop), _p(fit), _p(order), P, K, ne, nm, ctypes.c_float(0.7), ctypes.c_uint64(seed),
+                              _p(gen), _p(nxt), _p(nfit), s) == 0
+    ref, rfit = go.breed(go.init_population(P, K, seed), fit_h, go.rank(fit_h), ne, nm, 0.7, seed, 17)
+    np.testing.assert_array_equal(nxt.cpu().numpy(), ref)
+    np.testing.assert_array_equal(nfit.cpu().numpy()[:ne], rfit[:ne])
+
+
+@pytest.mark.parametrize("use_graph", [False, True])
+def test_ga_run_matches_oracle(torch, use_graph):
+    from brkga_fft2_b200.ga import DeviceBRKGA
+    inst = instances.small(5, n_parts=14, plates=((64, 64), (56, 72)), bbox_max=28)
+    pk = pack_problem(inst.problem_data, inst.nb_parts, inst.nb_machines, inst.thresholds, inst.instance_parts)
+    P, ne, nm, G, seed = 64, 8, 10, 6, 99
+    ga = DeviceBRKGA(None, inst.nb_parts, inst.nb_machines, inst.thresholds, inst.instance_parts,
+                     num_generations=G, num_individuals=P, num_elites=ne, num_mutants=nm, eliteCProb=0.7,
+                     seed=seed, use_graph=use_graph, packed=pk)
+    assert ga.fit() == "feasible"
+    pop, fit, hist, best, sol = go.run(pk, P, ne, nm, 0.7, seed, G)
+    np.testing.assert_array_equal(np.array([ga.history["min"], ga.history["mean"]]).T, hist)
+    np.testing.assert_array_equal(ga.population, pop)
+    np.testing.assert_array_equal(ga.fitness, fit)
+    assert ga.best_fitness == best
+    np.testing.assert_array_equal(ga.solution, sol)
+    assert len(ga.history["time"]) == G + 1 and all(np.diff(ga.history["time"]) >= 0)
+
+
+def test_ga_initial_solution_kept(torch):
+    from brkga_fft2_b200.ga import DeviceBRKGA
+    inst = instances.small(6, n_parts=12)
+    pk = pack_problem(inst.problem_data, inst.nb_parts, inst.nb_machines, inst.thresholds, inst.instance_parts)
+    init = instances.chromosomes(1, 12, 3)[0]
+    ga = DeviceBRKGA(None, 12, inst.nb_machines, inst.thresholds, inst.instance_parts, initialSol=init,
+                     num_generations=3, num_individuals=30, num_elites=4, num_mutants=5, packed=pk, seed=1)
+    ga.fit()
+    pop, fit, hist, best, sol = go.run(pk, 30, 4, 5, 0.7, 1, 3, initial=init)
+    np.testing.assert_array_equal(np.array(ga.history["min"]), hist[:, 0])
+    assert ga.best_fitness == best
