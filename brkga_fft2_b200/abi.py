@@ -119,6 +119,19 @@ def load_library(path: str = LIB_PATH):
         "brkga_ga_breed": (c_int, [vp, vp, vp, c_i32, c_i32, c_i32, c_i32, ctypes.c_float, ctypes.c_uint64, vp, vp,
                                    vp, vp]),
         "brkga_ga_track": (c_int, [vp, vp, c_i32, c_i32, vp, vp, c_i32, vp, vp, vp]),
+        "brkga_gemm_bf16": (c_int, [vp, c_i32, vp, c_i32, vp, c_i32, c_i32, c_i32, c_i32, vp, vp]),
+        "brkga_surrogate_create": (c_int, [vp, c_i32, c_i32, ctypes.c_uint64, P(vp)]),
+        "brkga_surrogate_destroy": (None, [vp]),
+        "brkga_surrogate_dims": (c_int, [vp, P(c_i32), P(c_i32), P(c_i64)]),
+        "brkga_surrogate_predict": (c_int, [vp, vp, c_i32, vp, vp]),
+        "brkga_surrogate_observe": (c_int, [vp, vp, vp, c_i32, vp]),
+        "brkga_surrogate_train": (c_int, [vp, c_i32, c_i32, ctypes.c_float, vp]),
+        "brkga_surrogate_features": (c_int, [vp, vp, c_i32, vp]),
+        "brkga_surrogate_load_batch": (c_int, [vp, vp, vp, c_i32, c_i32, vp]),
+        "brkga_surrogate_gradients": (c_int, [vp, c_i32, vp]),
+        "brkga_surrogate_adam": (c_int, [vp, ctypes.c_float, vp]),
+        "brkga_surrogate_buffers": (c_int, [vp, vp, vp, vp, vp, vp, vp, vp]),
+        "brkga_surrogate_io": (c_int, [vp, c_i32, vp, c_i64, c_i32]),
         "brkga_evaluate_host": (c_int, [vp, P(ctypes.c_float), c_i32, P(ctypes.c_double), vp]),
         "brkga_last_counters": (c_int, [vp, P(c_i64), P(c_i64), P(c_i64), P(c_i64)]),
     }

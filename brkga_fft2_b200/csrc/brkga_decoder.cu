@@ -607,6 +607,7 @@ struct BrkgaProblem {
   uint32_t* d_maskbits = nullptr;
   uint8_t* d_fits = nullptr;
   uint8_t* d_newbin_ok = nullptr;
+  double* d_bin_area = nullptr;
   // brkga_evaluate_host state
   std::mutex mu;
   cudaStream_t stream = nullptr;
@@ -772,6 +773,24 @@ extern "C" {
 
 int brkga_abi_version(void) { return BRKGA_ABI_VERSION; }
 
+// Device tables for the surrogate (same library, not part of the public ABI).
+__attribute__((visibility("hidden"))) int brkga_internal_problem_tables(
+    const BrkgaProblem* pb, int* N, int* M, int* T, int* mode, const double** thr, const int32_t** gene_type,
+    const double** part_area, const double** pt, const double** pth, const double** bin_area) {
+  if (!pb) return BRKGA_ERR_INVALID_ARGUMENT;
+  *N = pb->N;
+  *M = pb->M;
+  *T = pb->T;
+  *mode = pb->mode;
+  *thr = pb->d_thr;
+  *gene_type = pb->d_gene_type;
+  *part_area = pb->d_area;
+  *pt = pb->d_pt;
+  *pth = pb->d_pth;
+  *bin_area = pb->d_bin_area;
+  return BRKGA_OK;
+}
+
 const char* brkga_status_string(int status) {
   switch (status) {
     case BRKGA_OK: return "ok";
@@ -901,7 +920,9 @@ int brkga_problem_create(const BrkgaProblemDesc* d, BrkgaProblem** out) {
       (st = upload(pb, &pb->d_rot, rot)) || (st = upload(pb, &pb->d_dens, dens)) ||
       (st = upload(pb, &pb->d_run_off, run_off)) || (st = upload(pb, &pb->d_runs, runs)) ||
       (st = upload(pb, &pb->d_maskbits, maskbits)) || (st = upload(pb, &pb->d_fits, fits)) ||
-      (st = upload(pb, &pb->d_newbin_ok, newbin_ok)) || (st = configure(pb))) {
+      (st = upload(pb, &pb->d_newbin_ok, newbin_ok)) ||
+      (st = upload(pb, &pb->d_bin_area, std::vector<double>(d->bin_area, d->bin_area + M))) ||
+      (st = configure(pb))) {
     brkga_problem_destroy(pb);
     return st;
   }

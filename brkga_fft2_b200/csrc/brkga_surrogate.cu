@@ -1,0 +1,782 @@
+// brkga_surrogate.cu — online-trained MLP that ranks chromosomes by predicted
+// makespan (C ABI in include/brkga_b200.h).  No counterpart in the reference:
+// its GA decodes every offspring exactly (BRKGA_alg3.py:119-123).
+//
+// Network: features (3 per part in decode order + 2 per machine, padded to a
+// multiple of 64) -> 512 -> 256 -> 1, ReLU; bf16 weights and activations on
+// the tensor cores (umma_gemm.cuh, tcgen05) with fp32 accumulation, fp32
+// master weights and Adam state.  Every matrix product of the forward and
+// backward pass is one tcgen05 GEMM:
+//   Z1  = X   W1^T      dW2 = dZ2^T H1      dH1 = dZ2 W2      dW1 = dZ1^T X
+//   Z2  = H1  W2^T
+// (transposed bf16 copies of X, H1, dZ2, dZ1 and W2 are written by the
+// elementwise kernels so that every operand is K-major).  The last layer,
+// biases, the loss and Adam run on the CUDA cores.
+//
+// Features of a chromosome: parts sorted as the decoder visits them (by
+// machine, then sequencing key, placement.py:118-135); for part slot p:
+// machine / (M-1), proc_time / max proc_time, proc_time_height / max
+// proc_time_height; then per machine: assigned area / plate area and
+// assigned proc_time / max.  Targets: makespan standardised with the mean and
+// standard deviation of the first observed batch; infeasible chromosomes
+// (1e16) are not learned from.
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "../../include/brkga_b200.h"
+#include "umma_gemm.cuh"
+
+// access to the decoder's device tables (brkga_decoder.cu)
+extern "C" int brkga_internal_problem_tables(const BrkgaProblem* pb, int* N, int* M, int* T, int* mode,
+                                             const double** thr, const int32_t** gene_type, const double** part_area,
+                                             const double** pt, const double** pth, const double** bin_area);
+
+namespace {
+
+constexpr int kH1 = 512;
+constexpr int kH2 = 256;
+constexpr int kMaxGenes = 8192;
+
+struct U4 {
+  uint32_t x, y, z, w;
+};
+
+__device__ inline uint32_t mulhi32(uint32_t a, uint32_t b) { return (uint32_t)(((uint64_t)a * b) >> 32); }
+
+// Philox4x32-10 (Salmon et al., SC'11), as in brkga_ga.cu
+__device__ inline U4 philox(U4 c, uint32_t k0, uint32_t k1) {
+  for (int r = 0; r < 10; ++r) {
+    if (r) {
+      k0 += 0x9E3779B9u;
+      k1 += 0xBB67AE85u;
+    }
+    const uint32_t lo0 = 0xD2511F53u * c.x, hi0 = mulhi32(0xD2511F53u, c.x);
+    const uint32_t lo1 = 0xCD9E8D57u * c.z, hi1 = mulhi32(0xCD9E8D57u, c.z);
+    c = U4{hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0};
+  }
+  return c;
+}
+
+__device__ inline float unit_float(uint32_t v) { return (float)(v >> 8) * (1.0f / 16777216.0f); }
+
+__device__ inline unsigned ordered_bits(float v) {
+  unsigned u = __float_as_uint(v);
+  if (v == 0.0f) u = 0u;
+  if (v != v) u = 0x7FC00000u;
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+__device__ inline int machine_of(float mv, const double* thr, int M, int mode) {
+  if (M <= 1) return 0;
+  if (mv != mv) return M;
+  int m = 0;
+  if (mode == BRKGA_THRESH_F32) {
+    while (m < M - 1 && !(mv <= (float)thr[m])) ++m;
+  } else {
+    while (m < M - 1 && !((double)mv <= thr[m])) ++m;
+  }
+  return m;
+}
+
+struct FeatParams {
+  const float* chrom;
+  int P, N, M, T, mode, in_pad;
+  const double* thr;
+  const int32_t* gene_type;
+  const double* part_area;
+  const double* pt;
+  const double* pth;
+  const double* bin_area;
+  float inv_pt, inv_pth;  // 1 / max proc time, 1 / max height time
+  __nv_bfloat16* X;       // [rows, in_pad]
+  int row_offset;
+};
+
+// One CTA per chromosome: sort (machine, key, gene) like the decoder, write the
+// feature row.  Per-machine sums run in decode order, so features are deterministic.
+__global__ void features_kernel(FeatParams p) {
+  extern __shared__ unsigned long long keys[];
+  __shared__ float s_area[256], s_pt[256];
+  __shared__ int s_cnt[257], s_start[257];
+  const int c = blockIdx.x, tid = threadIdx.x, nt = blockDim.x;
+  int S2 = 1;
+  while (S2 < p.N) S2 <<= 1;
+  const float* ch = p.chrom + (size_t)c * 2 * p.N;
+  for (int m = tid; m <= p.M; m += nt) s_cnt[m] = 0;
+  __syncthreads();
+  for (int i = tid; i < S2; i += nt) {
+    unsigned long long key = ~0ull;
+    if (i < p.N) {
+      const int m = machine_of(ch[p.N + i], p.thr, p.M, p.mode);
+      key = ((unsigned long long)m << 48) | ((unsigned long long)ordered_bits(ch[i]) << 16) | (unsigned long long)i;
+      atomicAdd(&s_cnt[m], 1);
+    }
+    keys[i] = key;
+  }
+  __syncthreads();
+  for (int k = 2; k <= S2; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = tid; i < S2; i += nt) {
+        const int ixj = i ^ j;
+        if (ixj > i) {
+          const unsigned long long a = keys[i], b = keys[ixj];
+          if ((a > b) == ((i & k) == 0)) {
+            keys[i] = b;
+            keys[ixj] = a;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  if (tid == 0) {
+    int acc = 0;
+    for (int m = 0; m < p.M; ++m) {
+      s_start[m] = acc;
+      acc += s_cnt[m];
+    }
+  }
+  __syncthreads();
+  for (int m = tid; m < p.M; m += nt) {
+    float area = 0.f, load = 0.f;
+    for (int q = s_start[m]; q < s_start[m] + s_cnt[m]; ++q) {
+      const int t = p.gene_type[(int)(keys[q] & 0xFFFFu)];
+      area += (float)(p.part_area[t] / p.bin_area[m]);
+      load += (float)p.pt[(size_t)m * p.T + t] * p.inv_pt;
+    }
+    s_area[m] = area;
+    s_pt[m] = load;
+  }
+  __syncthreads();
+  __nv_bfloat16* row = p.X + (size_t)(p.row_offset + c) * p.in_pad;
+  const float mscale = p.M > 1 ? 1.f / (float)(p.M - 1) : 0.f;
+  for (int i = tid; i < p.in_pad; i += nt) {
+    float v = 0.f;
+    if (i < 3 * p.N) {
+      const unsigned long long key = keys[i / 3];
+      const int m = (int)(key >> 48);
+      if (m < p.M) {
+        const int t = p.gene_type[(int)(key & 0xFFFFu)];
+        const int f = i % 3;
+        v = f == 0 ? (float)m * mscale
+                   : f == 1 ? (float)p.pt[(size_t)m * p.T + t] * p.inv_pt : (float)p.pth[(size_t)m * p.T + t] * p.inv_pth;
+      }
+    } else if (i < 3 * p.N + 2 * p.M) {
+      const int q = i - 3 * p.N;
+      v = (q & 1) ? s_pt[q >> 1] : s_area[q >> 1];
+    }
+    row[i] = __float2bfloat16(v);
+  }
+}
+
+// Z <- max(Z + b, 0) in place; optional bf16 copies row-major and transposed
+__global__ void bias_relu_kernel(float* Z, const float* bias, int B, int H, __nv_bfloat16* out,
+                                 __nv_bfloat16* outT) {
+  const long long n = (long long)B * H;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int b = (int)(i / H), h = (int)(i - (long long)b * H);
+    const float v = fmaxf(Z[i] + bias[h], 0.f);
+    Z[i] = v;
+    const __nv_bfloat16 q = __float2bfloat16(v);
+    if (out) out[i] = q;
+    if (outT) outT[(size_t)h * B + b] = q;
+  }
+}
+
+// y[b] = sum_k A[b, k] w[k] + b0 (one warp per row)
+__global__ void out_layer_kernel(const float* A, const float* w, const float* b0, int B, int H, float* y) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (warp >= B) return;
+  float s = 0.f;
+  for (int k = lane; k < H; k += 32) s += A[(size_t)warp * H + k] * w[k];
+  for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xFFFFFFFFu, s, o);
+  if (lane == 0) y[warp] = s + b0[0];
+}
+
+// dZ2 = dy (x) w3, masked by ReLU'; bf16 row-major and transposed
+__global__ void out_backward_kernel(const float* Z2, const float* dy, const float* w3, int B, int H,
+                                    __nv_bfloat16* dZ, __nv_bfloat16* dZT) {
+  const long long n = (long long)B * H;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int b = (int)(i / H), h = (int)(i - (long long)b * H);
+    const float g = Z2[i] > 0.f ? dy[b] * w3[h] : 0.f;
+    const __nv_bfloat16 q = __float2bfloat16(g);
+    dZ[i] = q;
+    dZT[(size_t)h * B + b] = q;
+  }
+}
+
+// dZ1 = dH1 masked by ReLU' (in place) and its bf16 transpose
+__global__ void relu_backward_kernel(float* dH, const float* Z, int B, int H, __nv_bfloat16* dZT) {
+  const long long n = (long long)B * H;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int b = (int)(i / H), h = (int)(i - (long long)b * H);
+    const float g = Z[i] > 0.f ? dH[i] : 0.f;
+    dH[i] = g;
+    dZT[(size_t)h * B + b] = __float2bfloat16(g);
+  }
+}
+
+// out[h] = sum_b A[b, h] * (scale ? scale[b] : 1) * (mask ? (mask[b, h] > 0) : 1) * (colscale ? colscale[h] : 1)
+__global__ void col_reduce_kernel(const float* A, const float* scale, const float* mask, const float* colscale,
+                                  int B, int H, float* out) {
+  const int h = blockIdx.x * blockDim.x + threadIdx.x;
+  if (h >= H) return;
+  float s = 0.f;
+  for (int b = 0; b < B; ++b) {
+    const size_t i = (size_t)b * H + h;
+    float v = A ? A[i] : 1.f;
+    if (scale) v *= scale[b];
+    if (mask && !(mask[i] > 0.f)) v = 0.f;
+    s += v;
+  }
+  out[h] = colscale ? s * colscale[h] : s;
+}
+
+// Adam (Kingma & Ba); the step count t is read from device memory so graph replays stay correct
+__global__ void adam_kernel(float* w, const float* g, float* m, float* v, int n, float lr, float b1, float b2,
+                            float eps, const long long* t_ptr) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float t = (float)(*t_ptr);
+  const float bc1 = 1.f - powf(b1, t), bc2 = 1.f - powf(b2, t);
+  const float gi = g[i];
+  const float mi = b1 * m[i] + (1.f - b1) * gi;
+  const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  w[i] -= lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+}
+
+__global__ void cast_kernel(const float* W, int rows, int cols, __nv_bfloat16* out, __nv_bfloat16* outT) {
+  const long long n = (long long)rows * cols;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(i / cols), c = (int)(i - (long long)r * cols);
+    const __nv_bfloat16 q = __float2bfloat16(W[i]);
+    if (out) out[i] = q;
+    if (outT) outT[(size_t)c * rows + r] = q;
+  }
+}
+
+// uniform(-a, a) with a = sqrt(6 / fan_in) (He-uniform), Philox stream `tag`
+__global__ void init_weights_kernel(float* W, int n, int fan_in, int valid_cols, int cols, uint32_t k0, uint32_t k1,
+                                    uint32_t tag) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const U4 r = philox(U4{(uint32_t)i, 0u, 0u, 0x5300u + tag}, k0, k1);
+  const float a = sqrtf(6.f / (float)fan_in);
+  W[i] = (cols > 0 && (i % cols) >= valid_cols) ? 0.f : (2.f * unit_float(r.x) - 1.f) * a;
+}
+
+struct ObsParams {
+  const double* makespan;
+  int P;
+  const __nv_bfloat16* Xsrc;  // [P, in_pad] features of the observed rows
+  int in_pad;
+  __nv_bfloat16* bufX;        // [cap, in_pad]
+  float* bufY;                // [cap]
+  int cap;
+  double* norm;               // [mu, sigma, set]
+};
+
+// Standardisation from the first observed batch (feasible rows only).
+__global__ void set_norm_kernel(const double* ms, int P, double* norm) {
+  if (norm[2] != 0.0) return;
+  __shared__ double s1[256], s2[256], sn[256];
+  const int tid = threadIdx.x;
+  double a = 0, b = 0, n = 0;
+  for (int i = tid; i < P; i += blockDim.x) {
+    const double v = ms[i];
+    if (v < 1e15 && v == v) {
+      a += v;
+      b += v * v;
+      n += 1;
+    }
+  }
+  s1[tid] = a;
+  s2[tid] = b;
+  sn[tid] = n;
+  __syncthreads();
+  for (int h = blockDim.x >> 1; h; h >>= 1) {
+    if (tid < h) {
+      s1[tid] += s1[tid + h];
+      s2[tid] += s2[tid + h];
+      sn[tid] += sn[tid + h];
+    }
+    __syncthreads();
+  }
+  if (tid == 0 && sn[0] >= 2) {
+    const double mu = s1[0] / sn[0];
+    const double var = fmax(s2[0] / sn[0] - mu * mu, 1e-12 * mu * mu + 1e-12);
+    norm[0] = mu;
+    norm[1] = sqrt(var);
+    norm[2] = 1.0;
+  }
+}
+
+// Ring-buffer slots of the feasible rows, in row order (one CTA; deterministic).
+__global__ void observe_slots_kernel(const double* ms, int P, const double* norm, long long* count, int cap,
+                                     int* slot) {
+  if (threadIdx.x != 0) return;
+  long long c = *count;
+  const bool ready = norm[2] != 0.0;
+  for (int r = 0; r < P; ++r) {
+    const double v = ms[r];
+    if (ready && v < 1e15 && v == v) {
+      slot[r] = (int)(c % cap);
+      ++c;
+    } else {
+      slot[r] = -1;
+    }
+  }
+  *count = c;
+}
+
+// Append feasible rows (features + standardised target) to their slots.
+__global__ void observe_kernel(ObsParams p, const int* slot) {
+  const int r = blockIdx.x;
+  if (r >= p.P) return;
+  const int sl = slot[r];
+  if (sl < 0) return;
+  for (int i = threadIdx.x; i < p.in_pad; i += blockDim.x)
+    p.bufX[(size_t)sl * p.in_pad + i] = p.Xsrc[(size_t)r * p.in_pad + i];
+  if (threadIdx.x == 0) p.bufY[sl] = (float)((p.makespan[r] - p.norm[0]) / p.norm[1]);
+}
+
+// Minibatch: uniform rows of the filled part of the ring buffer.
+__global__ void gather_kernel(const __nv_bfloat16* bufX, const float* bufY, const long long* count, int cap, int B,
+                              int n_valid_max, int in_pad, uint32_t k0, uint32_t k1, const long long* step,
+                              __nv_bfloat16* X, __nv_bfloat16* XT, float* y, int* n_valid) {
+  const int b = blockIdx.x;
+  const long long filled = min((long long)cap, *count);
+  const int nv = (int)min((long long)n_valid_max, filled);
+  if (b == 0 && threadIdx.x == 0) *n_valid = nv;
+  const bool real = b < nv && filled > 0;
+  int src = 0;
+  if (real) {
+    const U4 r = philox(U4{(uint32_t)b, (uint32_t)(*step), 0x6A7u, 0u}, k0, k1);
+    src = (int)mulhi32(r.x, (uint32_t)filled);
+  }
+  for (int i = threadIdx.x; i < in_pad; i += blockDim.x) {
+    const __nv_bfloat16 q = real ? bufX[(size_t)src * in_pad + i] : __float2bfloat16(0.f);
+    X[(size_t)b * in_pad + i] = q;
+    XT[(size_t)i * B + b] = q;
+  }
+  if (threadIdx.x == 0) y[b] = real ? bufY[src] : 0.f;
+}
+
+__global__ void bump_kernel(long long* step) { *step += 1; }
+
+__global__ void set_int_kernel(int* p, int v) { *p = v; }
+
+__global__ void transpose_bf16_kernel(const __nv_bfloat16* X, int B, int I, __nv_bfloat16* XT) {
+  const long long n = (long long)B * I;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int b = (int)(i / I), c = (int)(i - (long long)b * I);
+    XT[(size_t)c * B + b] = X[i];
+  }
+}
+
+__global__ void loss_grad_dev_kernel(const float* y, const float* t, const int* n_valid, int B, float* dy,
+                                     float* loss) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B) return;
+  const int n = *n_valid;
+  float g = 0.f;
+  if (b < n) {
+    const float e = y[b] - t[b];
+    g = 2.f * e / (float)n;
+    atomicAdd(loss, e * e / (float)n);
+  }
+  dy[b] = g;
+}
+
+__global__ void denorm_kernel(const float* y, int P, const double* norm, double* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < P) out[i] = norm[2] != 0.0 ? (double)y[i] * norm[1] + norm[0] : (double)y[i];
+}
+
+int grid_for(long long n, int block = 256) {
+  long long g = (n + block - 1) / block;
+  return (int)std::max(1LL, std::min(g, 148LL * 32));
+}
+
+int round_up(int v, int a) { return (v + a - 1) / a * a; }
+
+}  // namespace
+
+struct BrkgaSurrogate {
+  const BrkgaProblem* problem = nullptr;
+  int N = 0, M = 0, T = 0, mode = 0;
+  int in = 0, in_pad = 0, max_batch = 0, cap = 0;
+  uint64_t seed = 0;
+  float inv_pt = 1.f, inv_pth = 1.f;
+  const double* thr = nullptr;
+  const int32_t* gene_type = nullptr;
+  const double* part_area = nullptr;
+  const double* pt = nullptr;
+  const double* pth = nullptr;
+  const double* bin_area = nullptr;
+  std::vector<void*> allocs;
+  // parameters (fp32 master), gradients, Adam moments: one flat block each
+  float *W1, *b1, *W2, *b2, *w3, *b3;
+  float *gW1, *gb1, *gW2, *gb2, *gw3, *gb3;
+  float *mom, *vel, *params, *grads;
+  long long n_params = 0;
+  __nv_bfloat16 *W1b, *W2b, *W2Tb;
+  // activations for up to max_batch rows
+  __nv_bfloat16 *X, *XT, *H1b, *H1Tb, *dZ2b, *dZ2Tb, *dZ1Tb;
+  float *Z1, *Z2, *y, *t, *dy, *dH1, *loss;
+  int* n_valid;
+  int* slot;
+  int* err;
+  long long *count, *step, *adam_t;
+  double* norm;
+  __nv_bfloat16* bufX;
+  float* bufY;
+};
+
+namespace {
+
+template <typename T>
+int dalloc(BrkgaSurrogate* s, T** p, size_t n) {
+  void* q = nullptr;
+  if (cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) return BRKGA_ERR_CUDA;
+  s->allocs.push_back(q);
+  if (cudaMemset(q, 0, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) return BRKGA_ERR_CUDA;
+  *p = static_cast<T*>(q);
+  return BRKGA_OK;
+}
+
+int gemm(const __nv_bfloat16* A, int lda, const __nv_bfloat16* B, int ldb, float* C, int ldc, int M, int N, int K,
+         int* err, cudaStream_t st) {
+  if (M % 128 || K % 64 || N % 64) return BRKGA_ERR_INVALID_ARGUMENT;
+  if (N % 128 == 0) {
+    umma::gemm_bf16_kernel<128><<<dim3(M / 128, N / 128), 128, 0, st>>>(A, lda, B, ldb, C, ldc, K, err);
+  } else {
+    umma::gemm_bf16_kernel<64><<<dim3(M / 128, N / 64), 128, 0, st>>>(A, lda, B, ldb, C, ldc, K, err);
+  }
+  return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
+}
+
+int features(BrkgaSurrogate* s, const float* d_chrom, int P, __nv_bfloat16* X, cudaStream_t st) {
+  FeatParams fp;
+  fp.chrom = d_chrom;
+  fp.P = P;
+  fp.N = s->N;
+  fp.M = s->M;
+  fp.T = s->T;
+  fp.mode = s->mode;
+  fp.in_pad = s->in_pad;
+  fp.thr = s->thr;
+  fp.gene_type = s->gene_type;
+  fp.part_area = s->part_area;
+  fp.pt = s->pt;
+  fp.pth = s->pth;
+  fp.bin_area = s->bin_area;
+  fp.inv_pt = s->inv_pt;
+  fp.inv_pth = s->inv_pth;
+  fp.X = X;
+  fp.row_offset = 0;
+  int S2 = 1;
+  while (S2 < s->N) S2 <<= 1;
+  features_kernel<<<P, std::min(1024, std::max(64, S2 / 2)), (size_t)S2 * 8, st>>>(fp);
+  return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
+}
+
+// forward on s->X [B, in_pad] (B % 128 == 0) -> s->y; keeps activations for backward
+int forward(BrkgaSurrogate* s, int B, bool keep_transposes, cudaStream_t st) {
+  int r;
+  if ((r = gemm(s->X, s->in_pad, s->W1b, s->in_pad, s->Z1, kH1, B, kH1, s->in_pad, s->err, st))) return r;
+  bias_relu_kernel<<<grid_for((long long)B * kH1), 256, 0, st>>>(s->Z1, s->b1, B, kH1, s->H1b,
+                                                                 keep_transposes ? s->H1Tb : nullptr);
+  if ((r = gemm(s->H1b, kH1, s->W2b, kH1, s->Z2, kH2, B, kH2, kH1, s->err, st))) return r;
+  bias_relu_kernel<<<grid_for((long long)B * kH2), 256, 0, st>>>(s->Z2, s->b2, B, kH2, nullptr, nullptr);
+  out_layer_kernel<<<(B * 32 + 255) / 256, 256, 0, st>>>(s->Z2, s->w3, s->b3, B, kH2, s->y);
+  return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
+}
+
+int cast_weights(BrkgaSurrogate* s, cudaStream_t st) {
+  cast_kernel<<<grid_for((long long)kH1 * s->in_pad), 256, 0, st>>>(s->W1, kH1, s->in_pad, s->W1b, nullptr);
+  cast_kernel<<<grid_for((long long)kH2 * kH1), 256, 0, st>>>(s->W2, kH2, kH1, s->W2b, s->W2Tb);
+  return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
+}
+
+}  // namespace
+
+extern "C" {
+
+int brkga_gemm_bf16(const void* d_A, int32_t lda, const void* d_B, int32_t ldb, float* d_C, int32_t ldc, int32_t M,
+                    int32_t N, int32_t K, int32_t* d_err, void* stream) {
+  if (!d_A || !d_B || !d_C || !d_err || M < 0 || N < 0 || K < 0 || lda < K || ldb < K || ldc < N || lda % 8 ||
+      ldb % 8 || ldc % 4)
+    return BRKGA_ERR_INVALID_ARGUMENT;
+  if (M == 0 || N == 0 || K == 0) return BRKGA_OK;
+  return gemm(static_cast<const __nv_bfloat16*>(d_A), lda, static_cast<const __nv_bfloat16*>(d_B), ldb, d_C, ldc, M,
+              N, K, d_err, static_cast<cudaStream_t>(stream));
+}
+
+void brkga_surrogate_destroy(BrkgaSurrogate* s) {
+  if (!s) return;
+  for (void* p : s->allocs) cudaFree(p);
+  delete s;
+}
+
+int brkga_surrogate_create(const BrkgaProblem* problem, int32_t max_batch, int32_t buffer_capacity, uint64_t seed,
+                           BrkgaSurrogate** out) {
+  if (!problem || !out || max_batch < 128 || max_batch % 128 || buffer_capacity < 1) return BRKGA_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  BrkgaSurrogate* s = new BrkgaSurrogate();
+  s->problem = problem;
+  const double* bin_area = nullptr;
+  if (brkga_internal_problem_tables(problem, &s->N, &s->M, &s->T, &s->mode, &s->thr, &s->gene_type, &s->part_area,
+                                    &s->pt, &s->pth, &bin_area) != BRKGA_OK || s->N > kMaxGenes || s->M > 256) {
+    delete s;
+    return BRKGA_ERR_INVALID_ARGUMENT;
+  }
+  s->bin_area = bin_area;
+  s->in = 3 * s->N + 2 * s->M;
+  s->in_pad = round_up(s->in, 64);
+  s->max_batch = max_batch;
+  s->cap = buffer_capacity;
+  s->seed = seed;
+  // feature scales from the host copies of the time tables
+  {
+    std::vector<double> pt((size_t)s->M * s->T), pth((size_t)s->M * s->T);
+    if (cudaMemcpy(pt.data(), s->pt, pt.size() * 8, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(pth.data(), s->pth, pth.size() * 8, cudaMemcpyDeviceToHost) != cudaSuccess) {
+      delete s;
+      return BRKGA_ERR_CUDA;
+    }
+    const double mp = *std::max_element(pt.begin(), pt.end()), mh = *std::max_element(pth.begin(), pth.end());
+    s->inv_pt = mp > 0 ? (float)(1.0 / mp) : 1.f;
+    s->inv_pth = mh > 0 ? (float)(1.0 / mh) : 1.f;
+  }
+  if (cudaFuncSetAttribute(features_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxGenes * 8) !=
+      cudaSuccess) {
+    delete s;
+    return BRKGA_ERR_CUDA;
+  }
+  const int B = max_batch, I = s->in_pad;
+  const long long nW1 = (long long)kH1 * I, nW2 = (long long)kH2 * kH1;
+  s->n_params = nW1 + kH1 + nW2 + kH2 + kH2 + 1;
+  int st = BRKGA_OK;
+  if ((st = dalloc(s, &s->params, s->n_params)) || (st = dalloc(s, &s->grads, s->n_params)) ||
+      (st = dalloc(s, &s->mom, s->n_params)) || (st = dalloc(s, &s->vel, s->n_params)) ||
+      (st = dalloc(s, &s->W1b, nW1)) || (st = dalloc(s, &s->W2b, nW2)) || (st = dalloc(s, &s->W2Tb, nW2)) ||
+      (st = dalloc(s, &s->X, (size_t)B * I)) || (st = dalloc(s, &s->XT, (size_t)B * I)) ||
+      (st = dalloc(s, &s->H1b, (size_t)B * kH1)) || (st = dalloc(s, &s->H1Tb, (size_t)B * kH1)) ||
+      (st = dalloc(s, &s->dZ2b, (size_t)B * kH2)) || (st = dalloc(s, &s->dZ2Tb, (size_t)B * kH2)) ||
+      (st = dalloc(s, &s->dZ1Tb, (size_t)B * kH1)) || (st = dalloc(s, &s->Z1, (size_t)B * kH1)) ||
+      (st = dalloc(s, &s->Z2, (size_t)B * kH2)) || (st = dalloc(s, &s->y, B)) || (st = dalloc(s, &s->t, B)) ||
+      (st = dalloc(s, &s->dy, B)) || (st = dalloc(s, &s->dH1, (size_t)B * kH1)) || (st = dalloc(s, &s->loss, 1)) ||
+      (st = dalloc(s, &s->n_valid, 1)) || (st = dalloc(s, &s->slot, B)) || (st = dalloc(s, &s->err, 1)) || (st = dalloc(s, &s->count, 1)) ||
+      (st = dalloc(s, &s->step, 1)) || (st = dalloc(s, &s->adam_t, 1)) || (st = dalloc(s, &s->norm, 3)) ||
+      (st = dalloc(s, &s->bufX, (size_t)s->cap * I)) || (st = dalloc(s, &s->bufY, s->cap))) {
+    brkga_surrogate_destroy(s);
+    return st;
+  }
+  float* q = s->params;
+  s->W1 = q; q += nW1; s->b1 = q; q += kH1; s->W2 = q; q += nW2; s->b2 = q; q += kH2; s->w3 = q; q += kH2; s->b3 = q;
+  q = s->grads;
+  s->gW1 = q; q += nW1; s->gb1 = q; q += kH1; s->gW2 = q; q += nW2; s->gb2 = q; q += kH2; s->gw3 = q; q += kH2;
+  s->gb3 = q;
+  const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+  init_weights_kernel<<<grid_for(nW1), 256>>>(s->W1, (int)nW1, s->in, s->in, I, k0, k1, 1);
+  init_weights_kernel<<<grid_for(nW2), 256>>>(s->W2, (int)nW2, kH1, kH1, kH1, k0, k1, 2);
+  init_weights_kernel<<<1, 256>>>(s->w3, kH2, kH2, kH2, kH2, k0, k1, 3);
+  if ((st = cast_weights(s, nullptr)) || cudaDeviceSynchronize() != cudaSuccess) {
+    brkga_surrogate_destroy(s);
+    return st ? st : BRKGA_ERR_CUDA;
+  }
+  *out = s;
+  return BRKGA_OK;
+}
+
+int brkga_surrogate_dims(const BrkgaSurrogate* s, int32_t* in_features, int32_t* in_padded, int64_t* n_params) {
+  if (!s) return BRKGA_ERR_INVALID_ARGUMENT;
+  if (in_features) *in_features = s->in;
+  if (in_padded) *in_padded = s->in_pad;
+  if (n_params) *n_params = s->n_params;
+  return BRKGA_OK;
+}
+
+int brkga_surrogate_buffers(const BrkgaSurrogate* s, float** params, float** grads, void** X, float** y,
+                            int32_t** err, int64_t** count, double** norm) {
+  if (!s) return BRKGA_ERR_INVALID_ARGUMENT;
+  if (params) *params = s->params;
+  if (grads) *grads = s->grads;
+  if (X) *X = s->X;
+  if (y) *y = s->y;
+  if (err) *err = s->err;
+  if (count) *count = reinterpret_cast<int64_t*>(s->count);
+  if (norm) *norm = s->norm;
+  return BRKGA_OK;
+}
+
+int brkga_surrogate_predict(BrkgaSurrogate* s, const float* d_chrom, int32_t P, double* d_pred, void* stream) {
+  if (!s || P < 0 || (P > 0 && (!d_chrom || !d_pred))) return BRKGA_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  int r;
+  for (int off = 0; off < P; off += s->max_batch) {
+    const int n = std::min(s->max_batch, P - off);
+    const int B = round_up(n, 128);
+    if (B > n && cudaMemsetAsync(s->X + (size_t)n * s->in_pad, 0, (size_t)(B - n) * s->in_pad * 2, st) != cudaSuccess)
+      return BRKGA_ERR_CUDA;
+    if ((r = features(s, d_chrom + (size_t)off * 2 * s->N, n, s->X, st))) return r;
+    if ((r = forward(s, B, false, st))) return r;
+    denorm_kernel<<<(n + 255) / 256, 256, 0, st>>>(s->y, n, s->norm, d_pred + off);
+  }
+  return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
+}
+
+int brkga_surrogate_observe(BrkgaSurrogate* s, const float* d_chrom, const double* d_makespan, int32_t P,
+                            void* stream) {
+  if (!s || P < 0 || (P > 0 && (!d_chrom || !d_makespan))) return BRKGA_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  int r;
+  set_norm_kernel<<<1, 256, 0, st>>>(d_makespan, P, s->norm);
+  for (int off = 0; off < P; off += s->max_batch) {
+    const int n = std::min(s->max_batch, P - off);
+    if ((r = features(s, d_chrom + (size_t)off * 2 * s->N, n, s->X, st))) return r;
+    ObsParams op;
+    op.makespan = d_makespan + off;
+    op.P = n;
+    op.Xsrc = s->X;
+    op.in_pad = s->in_pad;
+    op.bufX = s->bufX;
+    op.bufY = s->bufY;
+    op.cap = s->cap;
+    op.norm = s->norm;
+    observe_slots_kernel<<<1, 32, 0, st>>>(op.makespan, n, s->norm, s->count, s->cap, s->slot);
+    observe_kernel<<<n, 128, 0, st>>>(op, s->slot);
+  }
+  return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
+}
+
+static int gradients(BrkgaSurrogate* s, int B, cudaStream_t st) {
+  int r;
+  const int I = s->in_pad;
+  loss_grad_dev_kernel<<<(B + 255) / 256, 256, 0, st>>>(s->y, s->t, s->n_valid, B, s->dy, s->loss);
+  // output layer
+  col_reduce_kernel<<<(kH2 + 127) / 128, 128, 0, st>>>(s->Z2, s->dy, nullptr, nullptr, B, kH2, s->gw3);
+  col_reduce_kernel<<<1, 32, 0, st>>>(nullptr, s->dy, nullptr, nullptr, B, 1, s->gb3);
+  out_backward_kernel<<<grid_for((long long)B * kH2), 256, 0, st>>>(s->Z2, s->dy, s->w3, B, kH2, s->dZ2b, s->dZ2Tb);
+  col_reduce_kernel<<<(kH2 + 127) / 128, 128, 0, st>>>(nullptr, s->dy, s->Z2, s->w3, B, kH2, s->gb2);
+  // layer 2: dW2 = dZ2^T H1, dH1 = dZ2 W2
+  if ((r = gemm(s->dZ2Tb, B, s->H1Tb, B, s->gW2, kH1, kH2, kH1, B, s->err, st))) return r;
+  if ((r = gemm(s->dZ2b, kH2, s->W2Tb, kH2, s->dH1, kH1, B, kH1, kH2, s->err, st))) return r;
+  relu_backward_kernel<<<grid_for((long long)B * kH1), 256, 0, st>>>(s->dH1, s->Z1, B, kH1, s->dZ1Tb);
+  col_reduce_kernel<<<(kH1 + 127) / 128, 128, 0, st>>>(s->dH1, nullptr, nullptr, nullptr, B, kH1, s->gb1);
+  // layer 1: dW1 = dZ1^T X
+  if ((r = gemm(s->dZ1Tb, B, s->XT, B, s->gW1, I, kH1, I, B, s->err, st))) return r;
+  return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
+}
+
+int brkga_surrogate_gradients(BrkgaSurrogate* s, int32_t B, void* stream) {
+  // gradients of the MSE on the rows already in the activation buffers
+  // (s->X, s->XT, s->t, *n_valid) — used by tests and by brkga_surrogate_train
+  if (!s || B < 128 || B % 128 || B > s->max_batch) return BRKGA_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  int r;
+  if ((r = forward(s, B, true, st))) return r;
+  if (cudaMemsetAsync(s->loss, 0, sizeof(float), st) != cudaSuccess) return BRKGA_ERR_CUDA;
+  return gradients(s, B, st);
+}
+
+int brkga_surrogate_adam(BrkgaSurrogate* s, float lr, void* stream) {
+  if (!s) return BRKGA_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  bump_kernel<<<1, 1, 0, st>>>(s->adam_t);
+  adam_kernel<<<grid_for(s->n_params), 256, 0, st>>>(s->params, s->grads, s->mom, s->vel, (int)s->n_params, lr, 0.9f,
+                                                      0.999f, 1e-8f, s->adam_t);
+  return cast_weights(s, st);
+}
+
+int brkga_surrogate_train(BrkgaSurrogate* s, int32_t steps, int32_t batch, float lr, void* stream) {
+  if (!s || steps < 0 || batch < 128 || batch % 128 || batch > s->max_batch) return BRKGA_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  int r;
+  for (int i = 0; i < steps; ++i) {
+    gather_kernel<<<batch, 128, 0, st>>>(s->bufX, s->bufY, s->count, s->cap, batch, batch, s->in_pad,
+                                         (uint32_t)s->seed, (uint32_t)(s->seed >> 32), s->step, s->X, s->XT, s->t,
+                                         s->n_valid);
+    bump_kernel<<<1, 1, 0, st>>>(s->step);
+    if ((r = brkga_surrogate_gradients(s, batch, stream))) return r;
+    if ((r = brkga_surrogate_adam(s, lr, stream))) return r;
+  }
+  return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
+}
+
+// Put a caller-chosen minibatch in the activation buffers: X [B, in_pad] bf16
+// (device), targets t [B] (device), the first n_valid rows real.  Tests use it
+// to compare gradients with the CPU oracle.
+int brkga_surrogate_load_batch(BrkgaSurrogate* s, const void* d_X, const float* d_t, int32_t B, int32_t n_valid,
+                               void* stream) {
+  if (!s || !d_X || !d_t || B < 128 || B % 128 || B > s->max_batch || n_valid < 1 || n_valid > B)
+    return BRKGA_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (cudaMemcpyAsync(s->X, d_X, (size_t)B * s->in_pad * 2, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
+      cudaMemcpyAsync(s->t, d_t, (size_t)B * 4, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+    return BRKGA_ERR_CUDA;
+  set_int_kernel<<<1, 1, 0, st>>>(s->n_valid, n_valid);
+  transpose_bf16_kernel<<<grid_for((long long)B * s->in_pad), 256, 0, st>>>(s->X, B, s->in_pad, s->XT);
+  return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
+}
+
+// Features of P chromosomes into the first rows of the activation buffer X (tests).
+int brkga_surrogate_features(BrkgaSurrogate* s, const float* d_chrom, int32_t P, void* stream) {
+  if (!s || !d_chrom || P < 1 || P > s->max_batch) return BRKGA_ERR_INVALID_ARGUMENT;
+  return features(s, d_chrom, P, s->X, static_cast<cudaStream_t>(stream));
+}
+
+// Copy one of the surrogate's device arrays to or from host memory (tests,
+// checkpoints): 0 = parameters (fp32, flat), 1 = gradients, 2 = activations X
+// (bf16 [max_batch, in_pad]), 3 = predictions y (fp32 [max_batch]), 4 = loss
+// (fp32 [1]), 5 = target standardisation (float64 mean, std, set flag),
+// 6 = Adam moments m and v (fp32, 2 x parameters), 7 = Adam step (int64).
+int brkga_surrogate_io(BrkgaSurrogate* s, int32_t what, void* host, int64_t bytes, int32_t to_device) {
+  if (!s || !host || bytes < 0) return BRKGA_ERR_INVALID_ARGUMENT;
+  void* dev = nullptr;
+  int64_t size = 0;
+  switch (what) {
+    case 0: dev = s->params; size = s->n_params * 4; break;
+    case 1: dev = s->grads; size = s->n_params * 4; break;
+    case 2: dev = s->X; size = (int64_t)s->max_batch * s->in_pad * 2; break;
+    case 3: dev = s->y; size = (int64_t)s->max_batch * 4; break;
+    case 4: dev = s->loss; size = 4; break;
+    case 5: dev = s->norm; size = 24; break;
+    case 6: dev = s->mom; size = s->n_params * 8; break;  // mom and vel are separate allocations
+    case 7: dev = s->adam_t; size = 8; break;
+    default: return BRKGA_ERR_INVALID_ARGUMENT;
+  }
+  if (bytes > size) return BRKGA_ERR_INVALID_ARGUMENT;
+  if (what == 6) {
+    const int64_t half = s->n_params * 4;
+    char* h = static_cast<char*>(host);
+    const int64_t b1 = std::min(bytes, half), b2 = std::max<int64_t>(0, bytes - half);
+    cudaError_t e1 = to_device ? cudaMemcpy(s->mom, h, b1, cudaMemcpyHostToDevice)
+                               : cudaMemcpy(h, s->mom, b1, cudaMemcpyDeviceToHost);
+    cudaError_t e2 = b2 == 0 ? cudaSuccess
+                     : to_device ? cudaMemcpy(s->vel, h + half, b2, cudaMemcpyHostToDevice)
+                                 : cudaMemcpy(h + half, s->vel, b2, cudaMemcpyDeviceToHost);
+    return (e1 == cudaSuccess && e2 == cudaSuccess) ? BRKGA_OK : BRKGA_ERR_CUDA;
+  }
+  const cudaError_t e = to_device ? cudaMemcpy(dev, host, bytes, cudaMemcpyHostToDevice)
+                                  : cudaMemcpy(host, dev, bytes, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return BRKGA_ERR_CUDA;
+  if (to_device && what == 0) {
+    const int r = cast_weights(s, nullptr);
+    if (r) return r;
+    return cudaDeviceSynchronize() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
+  }
+  return BRKGA_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,191 @@
+// umma_gemm.cuh — bf16 GEMM on the 5th-generation tensor cores (tcgen05, sm_100a).
+//
+//   C[M, N] (fp32, row-major, ldc) = sum_k A[m, k] * B[n, k]
+//   A: bf16 [M, K] K-major (row-major, lda), B: bf16 [N, K] K-major (ldb).
+//   M % 128 == 0, N % BN == 0 (BN = 64 or 128), K % 64 == 0 (callers pad with zeros).
+//
+// One CTA of 128 threads per 128 x BN output tile.  Per 64-wide K step the
+// threads stage the A and B tiles in shared memory in the canonical K-major
+// "interleaved" layout (8 x 16-byte core matrices; core (row block, k chunk)
+// at (row_block * 8 + k_chunk) * 128 bytes, so the descriptor's leading byte
+// offset — next k chunk — is 128 B and its stride byte offset — next 8-row
+// block — is 1024 B), one elected thread issues four K=16
+// tcgen05.mma.cta_group::1.kind::f16 with the fp32 accumulator in tensor
+// memory (BN columns), and tcgen05.commit signals an mbarrier the CTA waits on.
+// The epilogue reads the accumulator with tcgen05.ld.32x32b (warp w owns
+// lanes 32w..32w+31 = output rows) and stores fp32.
+//
+// Every wait is bounded: after kSpinLimit polls the kernel records
+// BRKGA_ERR_CUDA in *err, skips its epilogue, frees its tensor memory and
+// returns.  No TMA and no multicast are used.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace umma {
+
+constexpr int kTileM = 128;
+constexpr int kTileK = 64;
+constexpr long long kSpinLimit = 20000000;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Shared-memory matrix descriptor, SWIZZLE_NONE, K-major.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo_bytes, uint32_t sbo_bytes) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo_bytes >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo_bytes >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;  // descriptor version for sm_100
+  return d;                // base offset 0, legacy LBO mode, layout type 0 (no swizzle)
+}
+
+// Instruction descriptor: D fp32, A and B bf16, both K-major, M x N.
+__host__ __device__ constexpr uint32_t instr_desc_bf16(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+
+__device__ __forceinline__ void commit_to(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ bool try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// bounded wait; false after kSpinLimit polls
+__device__ __forceinline__ bool wait_parity(uint64_t* bar, uint32_t parity) {
+  for (long long i = 0; i < kSpinLimit; ++i)
+    if (try_wait(bar, parity)) return true;
+  return false;
+}
+
+template <int BN>
+__global__ void __launch_bounds__(128) gemm_bf16_kernel(const __nv_bfloat16* __restrict__ A, int lda,
+                                                        const __nv_bfloat16* __restrict__ B, int ldb,
+                                                        float* __restrict__ C, int ldc, int K, int* err) {
+  static_assert(BN == 64 || BN == 128, "BN must be 64 or 128 (static shared memory <= 48 KB)");
+  constexpr int kCols = BN < 32 ? 32 : BN;  // tensor-memory columns (power of two >= 32)
+  __shared__ __align__(1024) uint4 sA[kTileM * kTileK / 8];
+  __shared__ __align__(1024) uint4 sB[BN * kTileK / 8];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t tmem_base;
+  __shared__ int s_fail, s_fail_kt;
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int m0 = blockIdx.x * kTileM, n0 = blockIdx.y * BN;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
+                 "r"(kCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    s_fail = 0;
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_base;
+  constexpr uint32_t idesc = instr_desc_bf16(kTileM, BN);
+
+  const int ksteps = K / kTileK;
+  for (int kt = 0; kt < ksteps; ++kt) {
+    // stage A: 128 rows x 8 chunks of 8 bf16; chunk (r, c) -> core ((r/8)*8 + c), row r%8
+    for (int i = tid; i < kTileM * 8; i += 128) {
+      const int r = i >> 3, c = i & 7;
+      sA[((r >> 3) * 8 + c) * 8 + (r & 7)] =
+          *reinterpret_cast<const uint4*>(A + (size_t)(m0 + r) * lda + kt * kTileK + c * 8);
+    }
+    for (int i = tid; i < BN * 8; i += 128) {
+      const int r = i >> 3, c = i & 7;
+      sB[((r >> 3) * 8 + c) * 8 + (r & 7)] =
+          *reinterpret_cast<const uint4*>(B + (size_t)(n0 + r) * ldb + kt * kTileK + c * 8);
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+#pragma unroll
+      for (int s = 0; s < kTileK / 16; ++s) {
+        // K = 16 is two 8-wide chunks: chunk 2s at +256*s bytes, the next one +128 B (LBO)
+        const uint64_t ad = smem_desc(a0 + 256u * s, 128u, 1024u);
+        const uint64_t bd = smem_desc(b0 + 256u * s, 128u, 1024u);
+        mma_bf16(tmem, ad, bd, idesc, (kt > 0 || s > 0) ? 1u : 0u);
+      }
+      commit_to(&bar);
+    }
+    __syncwarp();
+    if (!wait_parity(&bar, (uint32_t)(kt & 1))) {
+      if (lane == 0) {
+        atomicExch(&s_fail, 1);
+        s_fail_kt = kt;
+      }
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (s_fail) break;
+  }
+
+  if (!s_fail) {
+    const int row = m0 + warp * 32 + lane;
+#pragma unroll 1
+    for (int c0 = 0; c0 < BN; c0 += 32) {
+      uint32_t v[32];
+      const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+          "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+            "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
+            "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
+            "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+          : "r"(taddr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      float4* dst = reinterpret_cast<float4*>(C + (size_t)row * ldc + n0 + c0);
+#pragma unroll
+      for (int q = 0; q < 8; ++q)
+        dst[q] = make_float4(__uint_as_float(v[4 * q]), __uint_as_float(v[4 * q + 1]), __uint_as_float(v[4 * q + 2]),
+                             __uint_as_float(v[4 * q + 3]));
+    }
+  } else if (tid == 0) {
+    atomicExch(err, 3 /* BRKGA_ERR_CUDA */);
+    // let any MMA still in flight finish before the tensor memory is released
+    wait_parity(&bar, (uint32_t)(s_fail_kt & 1));
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols) : "memory");
+  }
+}
+
+}  // namespace umma

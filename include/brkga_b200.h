@@ -199,6 +199,49 @@ int brkga_ga_track(const double* d_fitness, const float* d_pop, int32_t P, int32
                    int64_t* d_generation, double* d_history, int32_t history_len, double* d_best_fitness,
                    float* d_best_solution, void* stream);
 
+/* ---- bf16 GEMM on the tensor cores (tcgen05) ----
+ * C[M,N] fp32 (row-major, ldc) = sum_k A[m,k] B[n,k]; A [M,K] and B [N,K]
+ * bf16 row-major (K contiguous).  M % 128 == 0, N % 64 == 0, K % 64 == 0;
+ * *d_err is set to BRKGA_ERR_CUDA if a tensor-core wait times out.  Used by
+ * the surrogate; no reference counterpart. */
+int brkga_gemm_bf16(const void* d_A, int32_t lda, const void* d_B, int32_t ldb, float* d_C, int32_t ldc,
+                    int32_t M, int32_t N, int32_t K, int32_t* d_err, void* stream);
+
+/* ---- Surrogate: MLP ranking chromosomes by predicted makespan ----
+ * No counterpart in the reference (its GA decodes every offspring,
+ * BRKGA_alg3.py:119-123).  Features: 3 per part in decode order (machine,
+ * proc time, height time) + 2 per machine (area load, time load), padded to a
+ * multiple of 64 -> 512 -> 256 -> 1 (ReLU); bf16 tensor-core GEMMs with fp32
+ * accumulation, fp32 master weights, Adam.  All device memory is allocated by
+ * brkga_surrogate_create; the other calls allocate nothing. */
+typedef struct BrkgaSurrogate BrkgaSurrogate;
+int brkga_surrogate_create(const BrkgaProblem* problem, int32_t max_batch /* % 128 == 0 */,
+                           int32_t buffer_capacity, uint64_t seed, BrkgaSurrogate** out);
+void brkga_surrogate_destroy(BrkgaSurrogate* surrogate);
+int brkga_surrogate_dims(const BrkgaSurrogate* surrogate, int32_t* in_features, int32_t* in_padded,
+                         int64_t* n_params);
+/* Predicted makespans (float64, makespan units) of P device chromosomes. */
+int brkga_surrogate_predict(BrkgaSurrogate* surrogate, const float* d_chrom, int32_t P, double* d_pred,
+                            void* stream);
+/* Append the feasible rows of (chromosome features, exact makespan) to the
+ * ring buffer of training examples; the first call fixes the target scaling. */
+int brkga_surrogate_observe(BrkgaSurrogate* surrogate, const float* d_chrom, const double* d_makespan,
+                            int32_t P, void* stream);
+/* `steps` Adam steps on minibatches of `batch` rows drawn uniformly from the buffer. */
+int brkga_surrogate_train(BrkgaSurrogate* surrogate, int32_t steps, int32_t batch, float lr, void* stream);
+/* Lower-level pieces (tests): features into the activation rows; load a
+ * minibatch; MSE gradients of the loaded minibatch; one Adam step. */
+int brkga_surrogate_features(BrkgaSurrogate* surrogate, const float* d_chrom, int32_t P, void* stream);
+int brkga_surrogate_load_batch(BrkgaSurrogate* surrogate, const void* d_X, const float* d_t, int32_t B,
+                               int32_t n_valid, void* stream);
+int brkga_surrogate_gradients(BrkgaSurrogate* surrogate, int32_t B, void* stream);
+int brkga_surrogate_adam(BrkgaSurrogate* surrogate, float lr, void* stream);
+/* Device addresses of internal arrays (any output may be NULL). */
+int brkga_surrogate_buffers(const BrkgaSurrogate* surrogate, float** params, float** grads, void** X,
+                            float** y, int32_t** err, int64_t** count, double** norm);
+/* Synchronous copy of an internal array to/from host memory (see brkga_surrogate.cu). */
+int brkga_surrogate_io(BrkgaSurrogate* surrogate, int32_t what, void* host, int64_t bytes, int32_t to_device);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,100 @@
+"""Surrogate on the GPU: the tcgen05 bf16 GEMM against a PyTorch fp32 matmul
+of the same bf16 operands, features / forward / gradients / Adam against the
+NumPy oracle, and online training that learns to rank real decodes."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from brkga_fft2_b200 import abi, instances, pack_problem
+from oracle import mlp_oracle as mo
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.fail("CUDA device required")
+    from brkga_fft2_b200 import build
+    build.build()
+    return torch
+
+
+@pytest.mark.parametrize("M,N,K", [(128, 64, 64), (256, 512, 320), (512, 320, 256), (384, 256, 512)])
+def test_gemm_bf16_matches_fp32_matmul(torch, M, N, K):
+    lib = abi.load_library()
+    g = torch.Generator(device="cuda").manual_seed(M + N + K)
+    A = torch.randn(M, K, device="cuda", generator=g).to(torch.bfloat16)
+    B = torch.randn(N, K, device="cuda", generator=g).to(torch.bfloat16)
+    C = torch.full((M, N), float("nan"), device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    st = lib.brkga_gemm_bf16(ctypes.c_void_p(A.data_ptr()), K, ctypes.c_void_p(B.data_ptr()), K,
+                             ctypes.c_void_p(C.data_ptr()), N, M, N, K, ctypes.c_void_p(err.data_ptr()),
+                             ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    assert st == 0
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    ref = A.float() @ B.float().T  # fp32 reference of the same bf16 operands
+    torch.testing.assert_close(C, ref, rtol=1e-4, atol=1e-3)
+
+
+@pytest.fixture(scope="module")
+def p100(torch):
+    from brkga_fft2_b200.evaluator import DeviceDecoder
+    from brkga_fft2_b200.surrogate import Surrogate
+    inst = instances.p100m4(0)
+    pk = pack_problem(inst.problem_data, inst.nb_parts, inst.nb_machines, inst.thresholds, inst.instance_parts)
+    dd = DeviceDecoder(pk, max_pop=4096)
+    sur = Surrogate(dd.native, max_batch=1024, buffer_capacity=20000, seed=7)
+    return inst, pk, dd, sur
+
+
+def test_features_match_oracle(torch, p100):
+    inst, pk, dd, sur = p100
+    ch = instances.chromosomes(40, inst.nb_parts, 3)
+    got = sur.features(torch.from_numpy(ch).cuda())
+    ref = mo.features(pk, ch, sur.in_pad)
+    assert sur.in_features == 3 * inst.nb_parts + 2 * inst.nb_machines
+    np.testing.assert_array_equal(got, ref)
+
+
+def test_forward_gradients_adam_match_oracle(torch, p100):
+    from brkga_fft2_b200.surrogate import split_params
+    inst, pk, dd, sur = p100
+    B, n = 256, 201
+    ch = instances.chromosomes(B, inst.nb_parts, 4)
+    X = mo.features(pk, ch, sur.in_pad)
+    t = np.random.default_rng(0).normal(size=B).astype(np.float32)
+    Xb = torch.from_numpy(X.astype(np.float32)).cuda().to(torch.bfloat16)
+    sur.load_batch(Xb, torch.from_numpy(t).cuda(), n)
+    sur.gradients(B)
+    flat = sur.params().astype(np.float64)
+    p = split_params(flat, sur.in_pad)
+    y_ref, _ = mo.forward(p, X, bf=True)
+    np.testing.assert_allclose(sur.predictions(B), y_ref, rtol=2e-3, atol=2e-3)
+    g = split_params(sur.grads().astype(np.float64), sur.in_pad)
+    gr = mo.grads(p, X, t.astype(np.float64), n, bf=True)
+    for name in gr:
+        rel = np.linalg.norm(g[name] - gr[name]) / max(np.linalg.norm(gr[name]), 1e-12)
+        assert rel < 2e-2, (name, rel)
+    # one Adam step from zero moments
+    sur.adam(1e-3)
+    new = sur.params().astype(np.float64)
+    w, _, _ = mo.adam(flat, sur.grads().astype(np.float64), 0.0, 0.0, 1, 1e-3)
+    np.testing.assert_allclose(new, w, rtol=1e-5, atol=1e-6)
+
+
+def test_online_training_learns_to_rank(torch, p100):
+    from brkga_fft2_b200.surrogate import spearman
+    inst, pk, dd, sur = p100
+    train = torch.from_numpy(instances.chromosomes(4096, inst.nb_parts, 10)).cuda()
+    ms = dd.decode(train)
+    sur.observe(train, ms)
+    test = torch.from_numpy(instances.chromosomes(1000, inst.nb_parts, 11)).cuda()
+    exact = dd.decode(test).cpu().numpy()
+    before = spearman(sur.predict(test).cpu().numpy(), exact)
+    sur.train(300, batch=512, lr=1e-3)
+    after = spearman(sur.predict(test).cpu().numpy(), exact)
+    assert after > 0.7 and after > before + 0.2, (before, after)
