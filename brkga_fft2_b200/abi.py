@@ -118,10 +118,15 @@ def load_library(path: str = LIB_PATH):
         "brkga_ga_rank": (c_int, [vp, c_i32, vp, vp]),
         "brkga_ga_breed": (c_int, [vp, vp, vp, c_i32, c_i32, c_i32, c_i32, ctypes.c_float, ctypes.c_uint64, vp, vp,
                                    vp, vp]),
+        "brkga_ga_breed_pool": (c_int, [vp, vp, vp, c_i32, c_i32, c_i32, c_i32, c_i32, ctypes.c_float,
+                                        ctypes.c_uint64, vp, vp, vp, vp]),
+        "brkga_ga_gather": (c_int, [vp, vp, c_i32, c_i32, vp, vp]),
+        "brkga_ga_screen_stats": (c_int, [vp, vp, vp, vp, c_i32, vp, vp, c_i32, vp, vp]),
         "brkga_ga_track": (c_int, [vp, vp, c_i32, c_i32, vp, vp, c_i32, vp, vp, vp]),
         "brkga_gemm_bf16": (c_int, [vp, c_i32, vp, c_i32, vp, c_i32, c_i32, c_i32, c_i32, vp, vp]),
         "brkga_surrogate_create": (c_int, [vp, c_i32, c_i32, ctypes.c_uint64, P(vp)]),
         "brkga_surrogate_destroy": (None, [vp]),
+        "brkga_surrogate_reset": (c_int, [vp]),
         "brkga_surrogate_dims": (c_int, [vp, P(c_i32), P(c_i32), P(c_i64)]),
         "brkga_surrogate_predict": (c_int, [vp, vp, c_i32, vp, vp]),
         "brkga_surrogate_observe": (c_int, [vp, vp, vp, c_i32, vp]),

@@ -107,12 +107,12 @@ __global__ void rank_kernel(const double* fit, int P, int S2, int32_t* order) {
 }
 
 // One thread per (row, 4-key block) of the new population.
-__global__ void breed_kernel(const float* pop, const double* fit, const int32_t* order, int P, int K, int ne,
-                             int nm, float rho, uint32_t k0, uint32_t k1, const long long* generation, float* next,
-                             double* next_fit) {
+__global__ void breed_kernel(const float* pop, const double* fit, const int32_t* order, int P, int out_rows, int K,
+                             int ne, int nm, float rho, uint32_t k0, uint32_t k1, const long long* generation,
+                             float* next, double* next_fit) {
   const uint32_t gen = (uint32_t)(*generation);
   const int blocks = (K + 3) >> 2;
-  const long long n = (long long)P * blocks;
+  const long long n = (long long)out_rows * blocks;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const int row = (int)(i / blocks), b = (int)(i - (long long)row * blocks);
     float* dst = next + (size_t)row * K + 4 * b;
@@ -128,13 +128,97 @@ __global__ void breed_kernel(const float* pop, const double* fit, const int32_t*
     } else {  // offspring of one elite and one non-elite parent
       const U4 pr = philox(U4{0u, (uint32_t)row, gen, kTagParents}, k0, k1);
       const int e = order[(int)mulhi32(pr.x, (uint32_t)ne)];
-      const int o = order[ne + (int)mulhi32(pr.y, (uint32_t)(P - ne))];
+      const int o = order[ne + (int)mulhi32(pr.y, (uint32_t)(P - ne))];  // non-elites of the parent population
       const U4 r = philox(U4{(uint32_t)b, (uint32_t)row, gen, kTagMask}, k0, k1);
       const uint32_t v[4] = {r.x, r.y, r.z, r.w};
       for (int q = 0; q < nk; ++q) {
         const int g = 4 * b + q;
         dst[q] = unit_float(v[q]) < rho ? pop[(size_t)e * K + g] : pop[(size_t)o * K + g];
       }
+    }
+  }
+}
+
+__global__ void gather_rows_kernel(const float* src, const int32_t* idx, int n, int K, float* dst) {
+  const long long total = (long long)n * K;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(i / K), k = (int)(i - (long long)r * K);
+    dst[i] = src[(size_t)idx[r] * K + k];
+  }
+}
+
+// Surrogate quality on the rows decoded this generation: Spearman correlation
+// of predicted and exact makespans (ranks from the two orderings; feasible
+// rows only) and the mean absolute error; stats[2g], stats[2g+1].
+__global__ void screen_stats_kernel(const double* pred, const double* exact, const int32_t* order_pred,
+                                    const int32_t* order_exact, int n, const long long* generation, double* stats,
+                                    int stats_len, int* rank_scratch) {
+  __shared__ double s_a[1024], s_b[1024], s_c[1024], s_m[1024], s_n[1024];
+  const int tid = threadIdx.x, nt = blockDim.x;
+  int* rp = rank_scratch;
+  int* re = rank_scratch + n;
+  for (int i = tid; i < n; i += nt) {
+    rp[order_pred[i]] = i;
+    re[order_exact[i]] = i;
+  }
+  __syncthreads();
+  // feasible rows keep their order among themselves; infeasible exact values rank last
+  double sa = 0, sb = 0, sab = 0, mae = 0, cnt = 0;
+  for (int i = tid; i < n; i += nt) {
+    const double e = exact[i];
+    if (e < 1e15 && e == e) {
+      sa += rp[i];
+      sb += re[i];
+      sab += (double)rp[i] * re[i];
+      mae += fabs(pred[i] - e);
+      cnt += 1;
+    }
+  }
+  s_a[tid] = sa;
+  s_b[tid] = sb;
+  s_c[tid] = sab;
+  s_m[tid] = mae;
+  s_n[tid] = cnt;
+  __syncthreads();
+  for (int h = nt >> 1; h; h >>= 1) {
+    if (tid < h) {
+      s_a[tid] += s_a[tid + h];
+      s_b[tid] += s_b[tid + h];
+      s_c[tid] += s_c[tid + h];
+      s_m[tid] += s_m[tid + h];
+      s_n[tid] += s_n[tid + h];
+    }
+    __syncthreads();
+  }
+  // second pass for the variances (ranks are permutations only when all rows are feasible)
+  double va = 0, vb = 0;
+  const double k = s_n[0];
+  const double ma = k > 0 ? s_a[0] / k : 0, mb = k > 0 ? s_b[0] / k : 0;
+  for (int i = tid; i < n; i += nt) {
+    const double e = exact[i];
+    if (e < 1e15 && e == e) {
+      va += (rp[i] - ma) * (rp[i] - ma);
+      vb += (re[i] - mb) * (re[i] - mb);
+    }
+  }
+  __syncthreads();
+  s_a[tid] = va;
+  s_b[tid] = vb;
+  __syncthreads();
+  for (int h = nt >> 1; h; h >>= 1) {
+    if (tid < h) {
+      s_a[tid] += s_a[tid + h];
+      s_b[tid] += s_b[tid + h];
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    const long long g = *generation;
+    if (g >= 0 && g < stats_len) {
+      const double cov = s_c[0] / fmax(k, 1.0) - ma * mb;
+      const double den = sqrt(s_a[0] / fmax(k, 1.0) * s_b[0] / fmax(k, 1.0));
+      stats[2 * g] = (k >= 2 && den > 0) ? cov / den : nan("");
+      stats[2 * g + 1] = k > 0 ? s_m[0] / k : nan("");
     }
   }
 }
@@ -196,6 +280,11 @@ int grid_for(long long n) {
 
 extern "C" {
 
+int brkga_ga_breed_pool(const float* d_pop, const double* d_fitness, const int32_t* d_order, int32_t P,
+                        int32_t out_rows, int32_t n_keys, int32_t n_elites, int32_t n_mutants, float rho,
+                        uint64_t seed, const int64_t* d_generation, float* d_next_pop, double* d_next_fitness,
+                        void* stream);
+
 int brkga_ga_init_population(float* d_pop, int32_t P, int32_t n_keys, uint64_t seed, int32_t skip_rows,
                              void* stream) {
   if (P < 0 || n_keys < 1 || skip_rows < 0 || (P > 0 && !d_pop)) return BRKGA_ERR_INVALID_ARGUMENT;
@@ -232,9 +321,41 @@ int brkga_ga_breed(const float* d_pop, const double* d_fitness, const int32_t* d
   if (P < 1 || n_keys < 1 || n_elites < 1 || n_mutants < 0 || n_elites + n_mutants > P || !d_pop || !d_fitness ||
       !d_order || !d_generation || !d_next_pop || !d_next_fitness || d_pop == d_next_pop)
     return BRKGA_ERR_INVALID_ARGUMENT;
-  breed_kernel<<<grid_for((long long)P * ((n_keys + 3) / 4)), 256, 0, (cudaStream_t)stream>>>(
-      d_pop, d_fitness, d_order, P, n_keys, n_elites, n_mutants, rho, (uint32_t)seed, (uint32_t)(seed >> 32),
-      reinterpret_cast<const long long*>(d_generation), d_next_pop, d_next_fitness);
+  return brkga_ga_breed_pool(d_pop, d_fitness, d_order, P, P, n_keys, n_elites, n_mutants, rho, seed, d_generation,
+                             d_next_pop, d_next_fitness, stream);
+}
+
+int brkga_ga_breed_pool(const float* d_pop, const double* d_fitness, const int32_t* d_order, int32_t P,
+                        int32_t out_rows, int32_t n_keys, int32_t n_elites, int32_t n_mutants, float rho,
+                        uint64_t seed, const int64_t* d_generation, float* d_next_pop, double* d_next_fitness,
+                        void* stream) {
+  if (P < 1 || out_rows < n_elites || n_keys < 1 || n_elites < 1 || n_elites > P || n_mutants < 0 ||
+      n_elites + n_mutants > out_rows || (n_elites + n_mutants < out_rows && n_elites >= P) || !d_pop ||
+      !d_fitness || !d_order || !d_generation || !d_next_pop || !d_next_fitness || d_pop == d_next_pop)
+    return BRKGA_ERR_INVALID_ARGUMENT;
+  breed_kernel<<<grid_for((long long)out_rows * ((n_keys + 3) / 4)), 256, 0, (cudaStream_t)stream>>>(
+      d_pop, d_fitness, d_order, P, out_rows, n_keys, n_elites, n_mutants, rho, (uint32_t)seed,
+      (uint32_t)(seed >> 32), reinterpret_cast<const long long*>(d_generation), d_next_pop, d_next_fitness);
+  return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
+}
+
+int brkga_ga_gather(const float* d_src, const int32_t* d_index, int32_t n, int32_t n_keys, float* d_dst,
+                    void* stream) {
+  if (n < 0 || n_keys < 1 || (n > 0 && (!d_src || !d_index || !d_dst))) return BRKGA_ERR_INVALID_ARGUMENT;
+  if (n == 0) return BRKGA_OK;
+  gather_rows_kernel<<<grid_for((long long)n * n_keys), 256, 0, (cudaStream_t)stream>>>(d_src, d_index, n, n_keys,
+                                                                                      d_dst);
+  return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
+}
+
+int brkga_ga_screen_stats(const double* d_pred, const double* d_exact, const int32_t* d_order_pred,
+                          const int32_t* d_order_exact, int32_t n, const int64_t* d_generation, double* d_stats,
+                          int32_t stats_len, int32_t* d_scratch, void* stream) {
+  if (n < 1 || !d_pred || !d_exact || !d_order_pred || !d_order_exact || !d_generation || !d_stats || !d_scratch)
+    return BRKGA_ERR_INVALID_ARGUMENT;
+  screen_stats_kernel<<<1, 1024, 0, (cudaStream_t)stream>>>(d_pred, d_exact, d_order_pred, d_order_exact, n,
+                                                           reinterpret_cast<const long long*>(d_generation),
+                                                           d_stats, stats_len, d_scratch);
   return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
 }
 

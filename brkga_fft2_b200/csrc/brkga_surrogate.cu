@@ -512,6 +512,26 @@ int cast_weights(BrkgaSurrogate* s, cudaStream_t st) {
 
 extern "C" {
 
+// Back to the state right after creation: initial weights, zero biases and
+// Adam moments, empty example buffer, target scaling unset.  Synchronous.
+int brkga_surrogate_reset(BrkgaSurrogate* s) {
+  if (!s) return BRKGA_ERR_INVALID_ARGUMENT;
+  const int I = s->in_pad;
+  const long long nW1 = (long long)kH1 * I, nW2 = (long long)kH2 * kH1;
+  if (cudaMemset(s->params, 0, s->n_params * 4) != cudaSuccess || cudaMemset(s->mom, 0, s->n_params * 4) ||
+      cudaMemset(s->vel, 0, s->n_params * 4) || cudaMemset(s->grads, 0, s->n_params * 4) ||
+      cudaMemset(s->count, 0, 8) || cudaMemset(s->step, 0, 8) || cudaMemset(s->adam_t, 0, 8) ||
+      cudaMemset(s->norm, 0, 24))
+    return BRKGA_ERR_CUDA;
+  const uint32_t k0 = (uint32_t)s->seed, k1 = (uint32_t)(s->seed >> 32);
+  init_weights_kernel<<<grid_for(nW1), 256>>>(s->W1, (int)nW1, s->in, s->in, I, k0, k1, 1);
+  init_weights_kernel<<<grid_for(nW2), 256>>>(s->W2, (int)nW2, kH1, kH1, kH1, k0, k1, 2);
+  init_weights_kernel<<<1, 256>>>(s->w3, kH2, kH2, kH2, kH2, k0, k1, 3);
+  const int st = cast_weights(s, nullptr);
+  if (st) return st;
+  return cudaDeviceSynchronize() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
+}
+
 int brkga_gemm_bf16(const void* d_A, int32_t lda, const void* d_B, int32_t ldb, float* d_C, int32_t ldc, int32_t M,
                     int32_t N, int32_t K, int32_t* d_err, void* stream) {
   if (!d_A || !d_B || !d_C || !d_err || M < 0 || N < 0 || K < 0 || lda < K || ldb < K || ldc < N || lda % 8 ||
@@ -587,11 +607,7 @@ int brkga_surrogate_create(const BrkgaProblem* problem, int32_t max_batch, int32
   q = s->grads;
   s->gW1 = q; q += nW1; s->gb1 = q; q += kH1; s->gW2 = q; q += nW2; s->gb2 = q; q += kH2; s->gw3 = q; q += kH2;
   s->gb3 = q;
-  const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
-  init_weights_kernel<<<grid_for(nW1), 256>>>(s->W1, (int)nW1, s->in, s->in, I, k0, k1, 1);
-  init_weights_kernel<<<grid_for(nW2), 256>>>(s->W2, (int)nW2, kH1, kH1, kH1, k0, k1, 2);
-  init_weights_kernel<<<1, 256>>>(s->w3, kH2, kH2, kH2, kH2, k0, k1, 3);
-  if ((st = cast_weights(s, nullptr)) || cudaDeviceSynchronize() != cudaSuccess) {
+  if ((st = brkga_surrogate_reset(s)) != BRKGA_OK) {
     brkga_surrogate_destroy(s);
     return st ? st : BRKGA_ERR_CUDA;
   }

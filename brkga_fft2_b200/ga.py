@@ -1,5 +1,15 @@
 """BRKGA on the GPU: the reference's GA loop with every generation on the device.
 
+With ``screening=True`` each generation breeds an ``oversample``-times larger
+candidate pool, ranks it with the online-trained surrogate
+(:mod:`brkga_fft2_b200.surrogate`) and decodes exactly only the best-predicted
+``num_individuals - num_elites`` rows; the surrogate then learns from those
+exact makespans.  Its Spearman correlation and mean absolute error on the
+decoded rows are logged for every generation (``history['spearman']``,
+``history['mae']``), and screening is switched off while the mean Spearman of
+the last ``check_every`` generations stays below ``spearman_threshold``
+(the surrogate keeps learning from plain generations meanwhile).
+
 ``DeviceBRKGA`` mirrors ``BRKGA_alg3.BRKGA`` (``BRKGA_alg3.py:23-281``): the
 same constructor parameters (``num_generations``, ``num_individuals``,
 ``num_elites``, ``num_mutants``, ``eliteCProb``, ``initialSol``), ``fit()``,
@@ -28,7 +38,10 @@ class DeviceBRKGA:
                  collision_backend=None, eval_mode="b200", eval_workers=0, eval_chunksize=1,
                  num_generations=200, num_individuals=100, num_elites=12, num_mutants=18, eliteCProb=0.7,
                  seed: int = 0, use_graph: bool = True, threshold_mode: int = THRESH_F32,
-                 packed: Optional[PackedProblem] = None, device=None):
+                 packed: Optional[PackedProblem] = None, device=None, screening: bool = False,
+                 oversample: int = 5, train_steps: int = 8, train_batch: int = 512, lr: float = 1e-3,
+                 spearman_threshold: float = 0.3, check_every: int = 5, warmup_generations: int = 5,
+                 buffer_capacity: int = 200_000, target: Optional[float] = None):
         import torch
         del collision_backend, eval_mode, eval_workers, eval_chunksize
         self.torch = torch
@@ -66,7 +79,32 @@ class DeviceBRKGA:
         self.best_fitness = -1
         self.solution = None
         self.used_bins = -1
-        self._graphs = None
+        self._graphs = {}
+        self._prepared = False
+        self.target = target
+        self.screening = bool(screening)
+        if self.screening:
+            from .surrogate import Surrogate
+            self.oversample = int(oversample)
+            self.train_steps, self.train_batch, self.lr = int(train_steps), int(train_batch), float(lr)
+            self.spearman_threshold = float(spearman_threshold)
+            self.check_every = max(1, int(check_every))
+            self.warmup_generations = int(warmup_generations)
+            rows = P - self.num_elites
+            self.pool_rows = self.num_elites + self.oversample * rows
+            if self.pool_rows - self.num_elites > 8192:
+                raise ValueError("oversampled pool too large for the single-CTA rank (8192 rows)")
+            self.pool = torch.zeros(self.pool_rows, K, dtype=torch.float32, device=dev)
+            self.pool_fit = torch.zeros(self.pool_rows, dtype=torch.float64, device=dev)
+            self.pred = torch.zeros(self.pool_rows - self.num_elites, dtype=torch.float64, device=dev)
+            self.order_pool = torch.zeros(self.pool_rows - self.num_elites, dtype=torch.int32, device=dev)
+            self.pred_sel = torch.zeros(max(rows, 1), dtype=torch.float64, device=dev)
+            self.o_pred = torch.zeros(max(rows, 1), dtype=torch.int32, device=dev)
+            self.o_exact = torch.zeros(max(rows, 1), dtype=torch.int32, device=dev)
+            self.stat_scratch = torch.zeros(2 * max(rows, 1), dtype=torch.int32, device=dev)
+            self.stats_dev = torch.full((self.num_generations + 1, 2), float("nan"), dtype=torch.float64, device=dev)
+            self.surrogate = Surrogate(self.decoder.native, max_batch=max(self.train_batch, 1024),
+                                       buffer_capacity=buffer_capacity, seed=self.seed ^ 0x5EED)
 
     # ---- kernels of one generation ------------------------------------------------
     @staticmethod
@@ -96,6 +134,64 @@ class DeviceBRKGA:
             self.decoder.decode(self.pop[nxt][ne:], out=self.fitness_buf[nxt][ne:])
         self._track(nxt)
 
+    def _rank(self, values, n, order):
+        abi.check(self.lib.brkga_ga_rank(self._ptr(values), n, self._ptr(order), self._stream()), "brkga_ga_rank")
+
+    def _monitor_and_learn(self, nxt):
+        """Surrogate quality on this generation's decoded rows, then learn from them."""
+        ne, rows = self.num_elites, self.num_individuals - self.num_elites
+        if rows < 1:
+            return
+        decoded, exact = self.pop[nxt][ne:], self.fitness_buf[nxt][ne:]
+        self.surrogate.predict(decoded, out=self.pred_sel[:rows])
+        self._rank(self.pred_sel, rows, self.o_pred)
+        self._rank(exact, rows, self.o_exact)
+        abi.check(self.lib.brkga_ga_screen_stats(self._ptr(self.pred_sel), self._ptr(exact), self._ptr(self.o_pred),
+                                                 self._ptr(self.o_exact), rows, self._ptr(self.generation),
+                                                 self._ptr(self.stats_dev), self.num_generations + 1,
+                                                 self._ptr(self.stat_scratch), self._stream()),
+                  "brkga_ga_screen_stats")
+        self.surrogate.observe(decoded, exact)
+        self.surrogate.train(self.train_steps, self.train_batch, self.lr)
+
+    def _step_learn(self, cur):
+        """Plain generation that also measures and trains the surrogate."""
+        nxt = 1 - cur
+        P, K, ne, nm = self.num_individuals, self.num_gene, self.num_elites, self.num_mutants
+        self._rank(self.fitness_buf[cur], P, self.order)
+        abi.check(self.lib.brkga_ga_breed(self._ptr(self.pop[cur]), self._ptr(self.fitness_buf[cur]),
+                                          self._ptr(self.order), P, K, ne, nm, ctypes.c_float(self.eliteCProb),
+                                          ctypes.c_uint64(self.seed), self._ptr(self.generation),
+                                          self._ptr(self.pop[nxt]), self._ptr(self.fitness_buf[nxt]),
+                                          self._stream()), "brkga_ga_breed")
+        if P > ne:
+            self.decoder.decode(self.pop[nxt][ne:], out=self.fitness_buf[nxt][ne:])
+        self._monitor_and_learn(nxt)
+        self._track(nxt)
+
+    def _step_screened(self, cur):
+        """Oversampled pool -> surrogate ranking -> exact decode of the best-predicted rows."""
+        nxt = 1 - cur
+        P, K, ne, nm = self.num_individuals, self.num_gene, self.num_elites, self.num_mutants
+        rows = P - ne
+        self._rank(self.fitness_buf[cur], P, self.order)
+        abi.check(self.lib.brkga_ga_breed_pool(self._ptr(self.pop[cur]), self._ptr(self.fitness_buf[cur]),
+                                               self._ptr(self.order), P, self.pool_rows, K, ne, nm * self.oversample,
+                                               ctypes.c_float(self.eliteCProb), ctypes.c_uint64(self.seed),
+                                               self._ptr(self.generation), self._ptr(self.pool),
+                                               self._ptr(self.pool_fit), self._stream()), "brkga_ga_breed_pool")
+        cand = self.pool_rows - ne
+        self.surrogate.predict(self.pool[ne:], out=self.pred)
+        self._rank(self.pred, cand, self.order_pool)
+        abi.check(self.lib.brkga_ga_gather(self._ptr(self.pool[ne:]), self._ptr(self.order_pool), rows, K,
+                                           self._ptr(self.pop[nxt][ne:]), self._stream()), "brkga_ga_gather")
+        self.pop[nxt][:ne].copy_(self.pool[:ne])
+        self.fitness_buf[nxt][:ne].copy_(self.pool_fit[:ne])
+        if rows > 0:
+            self.decoder.decode(self.pop[nxt][ne:], out=self.fitness_buf[nxt][ne:])
+        self._monitor_and_learn(nxt)
+        self._track(nxt)
+
     def _initial(self):
         P, K = self.num_individuals, self.num_gene
         skip = 1 if self.initialSol is not None else 0
@@ -104,27 +200,53 @@ class DeviceBRKGA:
         if skip:
             self.pop[0][0].copy_(self.torch.from_numpy(self.initialSol))
         self.decoder.decode(self.pop[0], out=self.fitness_buf[0])
+        if self.screening:
+            self.surrogate.observe(self.pop[0], self.fitness_buf[0])
+            self.surrogate.train(self.train_steps, self.train_batch, self.lr)
         self._track(0)
 
-    def _capture(self):
+    def _step_fn(self, mode):
+        return {"plain": self._step, "learn": self._step_learn, "screen": self._step_screened}[mode]
+
+    def _modes(self):
+        return ("learn", "screen") if self.screening else ("plain",)
+
+    def prepare(self):
+        """Run each kind of generation once eagerly (loads the kernels), capture
+        one CUDA graph per kind and buffer parity, then reset the surrogate:
+        afterwards ``fit`` only replays graphs."""
         torch = self.torch
-        graphs = []
-        side = torch.cuda.Stream(self.device)
-        # the first step runs eagerly (warm-up) inside fit(); capture both parities here
-        for cur in (0, 1):
-            g = torch.cuda.CUDAGraph()
-            with torch.cuda.graph(g, stream=side):
-                self._step(cur)
-            graphs.append(g)
-        return graphs
+        with torch.cuda.device(self.device):
+            self.generation.zero_()
+            self._initial()
+            for mode in self._modes():
+                self._step_fn(mode)(0)
+                self._step_fn(mode)(1)
+            torch.cuda.synchronize()
+            side = torch.cuda.Stream(self.device)
+            for mode in self._modes():
+                for cur in (0, 1):
+                    g = torch.cuda.CUDAGraph()
+                    with torch.cuda.graph(g, stream=side):  # records the launches without running them
+                        self._step_fn(mode)(cur)
+                    self._graphs[(mode, cur)] = g
+            torch.cuda.synchronize()
+            if self.screening:
+                self.surrogate.reset()
+        self._prepared = True
 
     # ---- public ---------------------------------------------------------------------
     def fit(self, verbose: bool = False):
         """Run ``num_generations`` generations (BRKGA_alg3.py:210-281)."""
         torch = self.torch
+        if self.use_graph and not self._prepared:
+            self.prepare()
         with torch.cuda.device(self.device):
             self.generation.zero_()
             self.best_fit.fill_(float("inf"))
+            if self.screening:
+                self.stats_dev.fill_(float("nan"))
+            torch.cuda.synchronize()
             start = time.perf_counter()
             ev0 = torch.cuda.Event(enable_timing=True)
             ev0.record()
@@ -135,32 +257,30 @@ class DeviceBRKGA:
             events.append(e)
             cur = 0
             G = self.num_generations
-            if self.use_graph and G >= 1:
-                # generation 1 eagerly: warms up the library before capture
-                self._step(cur)
+            base_mode = "learn" if self.screening else "plain"
+            screening_on = False
+            modes = []
+            done = 0
+            for g in range(1, G + 1):
+                mode = "screen" if screening_on else base_mode
+                if self.use_graph:
+                    self._graphs[(mode, cur)].replay()
+                else:
+                    self._step_fn(mode)(cur)
+                modes.append(mode)
                 cur = 1 - cur
                 e = torch.cuda.Event(enable_timing=True)
                 e.record()
                 events.append(e)
-                if G > 1:
-                    # capture records the launches without running them
-                    torch.cuda.synchronize()
-                    if self._graphs is None:
-                        self._graphs = self._capture()
-                    graphs = self._graphs
-                    for _ in range(G - 1):
-                        graphs[cur].replay()
-                        cur = 1 - cur
-                        e = torch.cuda.Event(enable_timing=True)
-                        e.record()
-                        events.append(e)
-            else:
-                for _ in range(G):
-                    self._step(cur)
-                    cur = 1 - cur
-                    e = torch.cuda.Event(enable_timing=True)
-                    e.record()
-                    events.append(e)
+                done = g
+                if (self.screening or self.target is not None) and g % (self.check_every if self.screening else 5) == 0:
+                    if self.screening:
+                        st = self.stats_dev[max(1, g - self.check_every + 1):g + 1, 0].cpu().numpy()
+                        rho = float(np.nanmean(st)) if np.isfinite(st).any() else float("nan")
+                        screening_on = g >= self.warmup_generations and rho >= self.spearman_threshold
+                    if self.target is not None and float(self.best_fit.item()) <= self.target:
+                        break
+            G = done
             torch.cuda.synchronize()
             wall = time.perf_counter() - start
             if int(self.decoder.status.item()) != 0:
@@ -168,7 +288,12 @@ class DeviceBRKGA:
             hist = self.history_dev.cpu().numpy()
             self.history = {"min": [float(v) for v in hist[:G + 1, 0]],
                             "mean": [float(v) for v in hist[:G + 1, 1]],
-                            "time": [ev0.elapsed_time(e) / 1000.0 for e in events]}
+                            "time": [ev0.elapsed_time(e) / 1000.0 for e in events],
+                            "mode": ["initial"] + modes}
+            if self.screening:
+                st = self.stats_dev.cpu().numpy()
+                self.history["spearman"] = [float(v) for v in st[:G + 1, 0]]
+                self.history["mae"] = [float(v) for v in st[:G + 1, 1]]
             self.best_fitness = float(self.best_fit.item())
             self.solution = self.best_sol.cpu().numpy()
             self.used_bins = int(np.floor(self.best_fitness))

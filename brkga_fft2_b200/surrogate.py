@@ -49,6 +49,10 @@ class Surrogate:
         self.max_batch = int(max_batch)
         self.capacity = int(buffer_capacity)
 
+    def reset(self):
+        """Initial weights, empty example buffer (synchronous)."""
+        abi.check(self.lib.brkga_surrogate_reset(self.handle), "brkga_surrogate_reset")
+
     def close(self):
         if getattr(self, "handle", None) is not None and self.handle.value:
             self.lib.brkga_surrogate_destroy(self.handle)

@@ -192,6 +192,27 @@ int brkga_ga_breed(const float* d_pop, const double* d_fitness, const int32_t* d
                    int32_t n_keys, int32_t n_elites, int32_t n_mutants, float rho, uint64_t seed,
                    const int64_t* d_generation, float* d_next_pop, double* d_next_fitness, void* stream);
 
+/* brkga_ga_breed writing out_rows rows (>= P allowed): the parents still come
+ * from the P-row population; rows past n_elites + n_mutants are offspring.
+ * Builds the oversampled candidate pool that the surrogate screens. */
+int brkga_ga_breed_pool(const float* d_pop, const double* d_fitness, const int32_t* d_order, int32_t P,
+                        int32_t out_rows, int32_t n_keys, int32_t n_elites, int32_t n_mutants, float rho,
+                        uint64_t seed, const int64_t* d_generation, float* d_next_pop, double* d_next_fitness,
+                        void* stream);
+
+/* d_dst[i, :] = d_src[d_index[i], :] for i < n (rows of n_keys float32). */
+int brkga_ga_gather(const float* d_src, const int32_t* d_index, int32_t n, int32_t n_keys, float* d_dst,
+                    void* stream);
+
+/* Surrogate quality for generation g = *d_generation: d_stats[2g] = Spearman
+ * correlation between predicted and exact makespans of the n decoded rows
+ * (ranks taken from the two orderings d_order_pred / d_order_exact as
+ * produced by brkga_ga_rank; infeasible rows excluded), d_stats[2g+1] = mean
+ * absolute error.  d_scratch: int32 [2n]. */
+int brkga_ga_screen_stats(const double* d_pred, const double* d_exact, const int32_t* d_order_pred,
+                          const int32_t* d_order_exact, int32_t n, const int64_t* d_generation, double* d_stats,
+                          int32_t stats_len, int32_t* d_scratch, void* stream);
+
 /* After a population is scored: history[2g] = min, history[2g+1] = mean of
  * d_fitness for g = *d_generation (BRKGA_alg3.py:224-227,255-262); copies the
  * best row into d_best_solution when it beats *d_best_fitness; then ++*d_generation. */
@@ -218,6 +239,8 @@ typedef struct BrkgaSurrogate BrkgaSurrogate;
 int brkga_surrogate_create(const BrkgaProblem* problem, int32_t max_batch /* % 128 == 0 */,
                            int32_t buffer_capacity, uint64_t seed, BrkgaSurrogate** out);
 void brkga_surrogate_destroy(BrkgaSurrogate* surrogate);
+/* Initial weights again, empty example buffer, unset target scaling (synchronous). */
+int brkga_surrogate_reset(BrkgaSurrogate* surrogate);
 int brkga_surrogate_dims(const BrkgaSurrogate* surrogate, int32_t* in_features, int32_t* in_padded,
                          int64_t* n_params);
 /* Predicted makespans (float64, makespan units) of P device chromosomes. */

@@ -80,3 +80,22 @@ def test_ga_initial_solution_kept(torch):
     pop, fit, hist, best, sol = go.run(pk, 30, 4, 5, 0.7, 1, 3, initial=init)
     np.testing.assert_array_equal(np.array(ga.history["min"]), hist[:, 0])
     assert ga.best_fitness == best
+
+
+def test_screened_ga_reports_exact_makespans(torch):
+    """With surrogate screening every reported makespan still comes from the
+    exact decoder; Spearman and MAE are logged for every generation."""
+    from brkga_fft2_b200.ga import DeviceBRKGA
+    from oracle import oracle_decode
+    inst = instances.p50m2(0)
+    pk = pack_problem(inst.problem_data, inst.nb_parts, inst.nb_machines, inst.thresholds, inst.instance_parts)
+    ga = DeviceBRKGA(None, inst.nb_parts, inst.nb_machines, inst.thresholds, inst.instance_parts,
+                     num_generations=20, num_individuals=200, num_elites=20, num_mutants=30, packed=pk, seed=3,
+                     screening=True, oversample=4, warmup_generations=4, check_every=2, spearman_threshold=-1.0)
+    ga.fit()
+    np.testing.assert_array_equal(ga.fitness, oracle_decode(pk, ga.population, n_threads=8))
+    assert ga.best_fitness == min(ga.history["min"])
+    assert oracle_decode(pk, ga.solution[None])[0] == ga.best_fitness
+    assert "screen" in ga.history["mode"]
+    assert np.isfinite(ga.history["spearman"][1:]).all() and np.isfinite(ga.history["mae"][1:]).all()
+    assert (np.diff(ga.history["min"]) <= 0).all()
