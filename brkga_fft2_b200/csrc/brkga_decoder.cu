@@ -345,11 +345,141 @@ __global__ void order_items_kernel(int n_items, int M, int N, const int32_t* cnt
   for (int i = tid; i < n_items; i += nt) order[atomicAdd(&start[infeas[i / M] ? 0 : cnt[i]], 1)] = i;
 }
 
+// Shared state of one CTA-cooperative plate search.
+struct SearchShared {
+  unsigned long long best;
+  int chunk, total, nr;
+  int rlist[4];
+};
+
+// Best placement key of part type t on one plate (kKeyNone if it does not
+// fit): the four warps pull (rotation, 32 candidate top rows) chunks from a
+// shared counter (rotations interleaved, bottom rows first), skip chunks that
+// cannot beat the best key found so far, and merge with atomicMin.  Called
+// by all threads of the CTA; contains __syncthreads.
+__device__ __forceinline__ unsigned long long search_plate(const DecodeParams& p, const MachDev& md,
+                                                           const uint32_t* grid, const uint16_t* vac, int enc,
+                                                           int t, SearchShared& sh, unsigned long long& c_tests,
+                                                           unsigned long long& c_chunks,
+                                                           unsigned long long& c_bytes) {
+  const int tid = threadIdx.x, lane = tid & 31;
+  if (tid == 0) {
+    int nr = 0, hmin = kMaxSide + 1;
+    const int nrot = p.nrot[t];
+    for (int r = 0; r < nrot; ++r) {
+      const RotDev rd = p.rot[t * 4 + r];
+      if (rd.h <= md.L && rd.w <= md.W) {  // numba_utils.py:82-84
+        sh.rlist[nr++] = r;
+        hmin = min(hmin, rd.h);
+        c_bytes += 4ull * ((unsigned long long)md.L * md.NW + (unsigned long long)rd.h * rd.mw);
+      }
+    }
+    sh.nr = nr;
+    sh.total = nr ? nr * ((md.L - hmin + 1 + 31) >> 5) : 0;
+    sh.best = kKeyNone;
+    sh.chunk = 0;
+    c_tests += nr;
+  }
+  __syncthreads();
+  const int nr = sh.nr, total = sh.total;
+  for (int guard = 0; guard < total; ++guard) {
+    int ci = 0;
+    if (lane == 0) ci = atomicAdd(&sh.chunk, 1);
+    ci = __shfl_sync(kFull, ci, 0);
+    if (ci >= total) break;
+    const int r = sh.rlist[ci % nr];
+    const int level = ci / nr;
+    const RotDev rd = p.rot[t * 4 + r];
+    const int ty_hi = md.L - rd.h - 32 * level;
+    if (ty_hi < 0) continue;
+    unsigned long long cur = 0;
+    if (lane == 0) cur = *(volatile unsigned long long*)&sh.best;
+    cur = __shfl_sync(kFull, cur, 0);
+    if (key_of(max(enc, md.L - ty_hi), ty_hi + rd.h - 1, 0, r) >= cur) continue;
+    const int ty = ty_hi - lane;
+    int x = -1;
+    if (ty >= 0 && vacancy_ok(vac, ty, rd, p.dens)) x = first_free_x(grid, md.RS, md.W, ty, rd, p.run_off, p.runs);
+    const unsigned fm = __ballot_sync(kFull, x >= 0);
+    if (lane == 0) ++c_chunks;
+    if (fm) {
+      const int l = __ffs(fm) - 1;
+      const int xb = __shfl_sync(kFull, x, l);
+      if (lane == 0) {
+        const int tyb = ty_hi - l;
+        atomicMin(&sh.best, key_of(max(enc, md.L - tyb), tyb + rd.h - 1, xb, r));
+      }
+    }
+  }
+  __syncthreads();
+  const unsigned long long key = sh.best;
+  __syncthreads();
+  return key;
+}
+
+// Insert rotation r of part type t with its top row at ty and left column x
+// (binClassNew.py:155-174): OR the mask rows into the plate words, recompute
+// the vacancy of the touched rows (numba_utils.py:160-188); thread 0 updates
+// the plate scalars.  All threads of the CTA; contains __syncthreads.
+__device__ __forceinline__ void place_part(const DecodeParams& p, const MachDev& md, uint32_t* grid, uint16_t* vac,
+                                           BinScal* scal, int t, int m, int r, int x, int ty, double a) {
+  const int tid = threadIdx.x;
+  const RotDev rd = p.rot[t * 4 + r];
+  const int sx = x & 31, wx = x >> 5, span = rd.mw + 1;
+  const uint32_t* mb = p.maskbits + rd.mask_base;
+  for (int idx = tid; idx < rd.h * span; idx += kDecodeThreads) {
+    const int i = idx / span, j = idx - i * span;
+    const uint32_t lo = j > 0 ? __ldg(mb + i * rd.mw + j - 1) : 0u;
+    const uint32_t hi = j < rd.mw ? __ldg(mb + i * rd.mw + j) : 0u;
+    const uint32_t v = __funnelshift_l(lo, hi, sx);
+    if (v) grid[(size_t)(ty + i) * md.RS + wx + j] |= v;
+  }
+  __syncthreads();
+  for (int i = tid; i < rd.h; i += kDecodeThreads)
+    vac[ty + i] = (uint16_t)max_zero_run(grid + (size_t)(ty + i) * md.RS, md.W, md.NW);
+  if (tid == 0) {
+    BinScal s = *scal;
+    s.area += a;
+    s.minrow = min(s.minrow, ty);
+    s.maxrow = max(s.maxrow, ty + rd.h - 1);
+    s.enc = (s.minrow > s.maxrow) ? 0 : md.L - s.minrow;  // binClassNew.py:147-152
+    s.pt += p.pt[(size_t)m * p.T + t];
+    const double ph = p.pth[(size_t)m * p.T + t];
+    if (ph > s.pth) s.pth = ph;
+    *scal = s;
+  }
+  __syncthreads();
+}
+
+// Empty plate: zero words, vacancy W (binClassNew.py:18-20), fresh scalars.
+__device__ __forceinline__ void open_plate(const MachDev& md, uint32_t* grid, uint16_t* vac, BinScal* scal,
+                                           int pool_index) {
+  const int tid = threadIdx.x;
+  for (int i = tid; i < md.L * md.RS; i += kDecodeThreads) grid[i] = 0u;
+  for (int i = tid; i < md.L; i += kDecodeThreads) vac[i] = (uint16_t)md.W;
+  if (tid == 0) {
+    BinScal z;
+    z.area = 0.0;
+    z.pt = 0.0;
+    z.pth = 0.0;
+    z.minrow = md.L;
+    z.maxrow = -1;
+    z.enc = 0;
+    z.pool = pool_index;
+    *scal = z;
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ void decode_key(unsigned long long key, int* r, int* x, int* y) {
+  *r = (int)(key & 3ull);
+  *x = (int)((key >> 2) & 0x1FFFull);
+  *y = kMaxSide - (int)((key >> 15) & 0x1FFFull);
+}
+
 __global__ void __launch_bounds__(kDecodeThreads) decode_kernel(DecodeParams p) {
   extern __shared__ __align__(16) uint32_t smem[];
-  __shared__ unsigned long long s_best;
-  __shared__ int s_item, s_chunk, s_total, s_nr, s_fail, s_pool;
-  __shared__ int s_rlist[4];
+  __shared__ SearchShared sh;
+  __shared__ int s_item, s_fail, s_pool;
   const int tid = threadIdx.x, lane = tid & 31;
   BinScal* bs = p.binscal + (size_t)blockIdx.x * p.N;
   unsigned long long c_tests = 0, c_chunks = 0, c_bins = 0, c_bytes = 0;
@@ -390,61 +520,10 @@ __global__ void __launch_bounds__(kDecodeThreads) decode_kernel(DecodeParams p) 
       // ---- first fit over the open plates (placement.py:56-64)
       for (int b = 0; b < nb; ++b) {
         if (bs[b].area + a > md.area) continue;  // placement.py:57-59
-        uint32_t* grid = b < p.S ? smem + (size_t)b * p.slot_words
-                                 : p.pool + (size_t)bs[b].pool * p.slot_words;
+        const uint32_t* grid = b < p.S ? smem + (size_t)b * p.slot_words
+                                       : p.pool + (size_t)bs[b].pool * p.slot_words;
         const uint16_t* vac = reinterpret_cast<const uint16_t*>(grid + p.slot_vac_off);
-        const int enc = bs[b].enc;
-        if (tid == 0) {
-          int nr = 0, hmin = kMaxSide + 1;
-          const int nrot = p.nrot[t];
-          for (int r = 0; r < nrot; ++r) {
-            const RotDev rd = p.rot[t * 4 + r];
-            if (rd.h <= md.L && rd.w <= md.W) {  // numba_utils.py:82-84
-              s_rlist[nr++] = r;
-              hmin = min(hmin, rd.h);
-              c_bytes += 4ull * ((unsigned long long)md.L * md.NW + (unsigned long long)rd.h * rd.mw);
-            }
-          }
-          s_nr = nr;
-          s_total = nr ? nr * ((md.L - hmin + 1 + 31) >> 5) : 0;
-          s_best = kKeyNone;
-          s_chunk = 0;
-          c_tests += nr;
-        }
-        __syncthreads();
-        const int nr = s_nr, total = s_total;
-        for (int guard = 0; guard < total; ++guard) {
-          int ci = 0;
-          if (lane == 0) ci = atomicAdd(&s_chunk, 1);
-          ci = __shfl_sync(kFull, ci, 0);
-          if (ci >= total) break;
-          const int r = s_rlist[ci % nr];
-          const int level = ci / nr;
-          const RotDev rd = p.rot[t * 4 + r];
-          const int ty_hi = md.L - rd.h - 32 * level;
-          if (ty_hi < 0) continue;
-          unsigned long long cur = 0;
-          if (lane == 0) cur = *(volatile unsigned long long*)&s_best;
-          cur = __shfl_sync(kFull, cur, 0);
-          if (key_of(max(enc, md.L - ty_hi), ty_hi + rd.h - 1, 0, r) >= cur) continue;
-          const int ty = ty_hi - lane;
-          int x = -1;
-          if (ty >= 0 && vacancy_ok(vac, ty, rd, p.dens))
-            x = first_free_x(grid, md.RS, md.W, ty, rd, p.run_off, p.runs);
-          const unsigned fm = __ballot_sync(kFull, x >= 0);
-          if (lane == 0) ++c_chunks;
-          if (fm) {
-            const int l = __ffs(fm) - 1;
-            const int xb = __shfl_sync(kFull, x, l);
-            if (lane == 0) {
-              const int tyb = ty_hi - l;
-              atomicMin(&s_best, key_of(max(enc, md.L - tyb), tyb + rd.h - 1, xb, r));
-            }
-          }
-        }
-        __syncthreads();
-        key = s_best;
-        __syncthreads();
+        key = search_plate(p, md, grid, vac, bs[b].enc, t, sh, c_tests, c_chunks, c_bytes);
         if (key != kKeyNone) {
           pb = b;
           break;
@@ -477,63 +556,20 @@ __global__ void __launch_bounds__(kDecodeThreads) decode_kernel(DecodeParams p) 
         }
         pb = nb++;
         uint32_t* grid = pb < p.S ? smem + (size_t)pb * p.slot_words : p.pool + (size_t)s_pool * p.slot_words;
-        uint16_t* vac = reinterpret_cast<uint16_t*>(grid + p.slot_vac_off);
-        for (int i = tid; i < md.L * md.RS; i += kDecodeThreads) grid[i] = 0u;
-        for (int i = tid; i < md.L; i += kDecodeThreads) vac[i] = (uint16_t)md.W;  // binClassNew.py:20
-        if (tid == 0) {
-          BinScal z;
-          z.area = 0.0;
-          z.pt = 0.0;
-          z.pth = 0.0;
-          z.minrow = md.L;
-          z.maxrow = -1;
-          z.enc = 0;
-          z.pool = s_pool;
-          bs[pb] = z;
-          ++c_bins;
-        }
+        open_plate(md, grid, reinterpret_cast<uint16_t*>(grid + p.slot_vac_off), &bs[pb], s_pool);
+        if (tid == 0) ++c_bins;
         x = 0;
         ty = md.L - p.rot[t * 4 + r].h;
-        __syncthreads();
       } else {
-        r = (int)(key & 3ull);
-        x = (int)((key >> 2) & 0x1FFFull);
-        const int y = kMaxSide - (int)((key >> 15) & 0x1FFFull);
+        int y;
+        decode_key(key, &r, &x, &y);
         ty = y - p.rot[t * 4 + r].h + 1;
       }
 
       // ---- insert (binClassNew.py:155-174)
-      {
-        const RotDev rd = p.rot[t * 4 + r];
-        uint32_t* grid = pb < p.S ? smem + (size_t)pb * p.slot_words
-                                  : p.pool + (size_t)bs[pb].pool * p.slot_words;
-        uint16_t* vac = reinterpret_cast<uint16_t*>(grid + p.slot_vac_off);
-        const int sx = x & 31, wx = x >> 5, span = rd.mw + 1;
-        const uint32_t* mb = p.maskbits + rd.mask_base;
-        for (int idx = tid; idx < rd.h * span; idx += kDecodeThreads) {
-          const int i = idx / span, j = idx - i * span;
-          const uint32_t lo = j > 0 ? __ldg(mb + i * rd.mw + j - 1) : 0u;
-          const uint32_t hi = j < rd.mw ? __ldg(mb + i * rd.mw + j) : 0u;
-          const uint32_t v = __funnelshift_l(lo, hi, sx);
-          if (v) grid[(size_t)(ty + i) * md.RS + wx + j] |= v;
-        }
-        __syncthreads();
-        for (int i = tid; i < rd.h; i += kDecodeThreads)
-          vac[ty + i] = (uint16_t)max_zero_run(grid + (size_t)(ty + i) * md.RS, md.W, md.NW);
-        if (tid == 0) {
-          BinScal s = bs[pb];
-          s.area += a;
-          s.minrow = min(s.minrow, ty);
-          s.maxrow = max(s.maxrow, ty + rd.h - 1);
-          s.enc = (s.minrow > s.maxrow) ? 0 : md.L - s.minrow;  // binClassNew.py:147-152
-          s.pt += p.pt[(size_t)m * p.T + t];
-          const double ph = p.pth[(size_t)m * p.T + t];
-          if (ph > s.pth) s.pth = ph;
-          bs[pb] = s;
-          if (lg) lg[k] = BrkgaPlacement{gene, pb, x, ty + rd.h - 1, r};
-        }
-        __syncthreads();
-      }
+      uint32_t* grid = pb < p.S ? smem + (size_t)pb * p.slot_words : p.pool + (size_t)bs[pb].pool * p.slot_words;
+      place_part(p, md, grid, reinterpret_cast<uint16_t*>(grid + p.slot_vac_off), &bs[pb], t, m, r, x, ty, a);
+      if (tid == 0 && lg) lg[k] = BrkgaPlacement{gene, pb, x, ty + p.rot[t * 4 + r].h - 1, r};
     }
     if (!failed && tid == 0) {  // placement.py:86-89
       double ms = 0.0;
