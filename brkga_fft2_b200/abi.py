@@ -114,6 +114,7 @@ def load_library(path: str = LIB_PATH):
         "brkga_decode": (c_int, [vp, vp, c_i32, vp, vp, vp, vp, c_sz, c_i64, vp]),
         "brkga_decode_stage": (c_int, [c_i32, vp, vp, c_i32, vp, vp, vp, vp, c_sz, c_i64, vp]),
         "brkga_decode_noalloc": (c_int, [vp, vp, c_i32, vp, vp, vp, vp]),
+        "brkga_initial_solution_host": (c_int, [vp, vp, c_i32, vp, vp, vp]),
         "brkga_ga_init_population": (c_int, [vp, c_i32, c_i32, ctypes.c_uint64, c_i32, vp]),
         "brkga_ga_rank": (c_int, [vp, c_i32, vp, vp]),
         "brkga_ga_breed": (c_int, [vp, vp, vp, c_i32, c_i32, c_i32, c_i32, ctypes.c_float, ctypes.c_uint64, vp, vp,

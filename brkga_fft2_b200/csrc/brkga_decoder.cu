@@ -79,6 +79,7 @@ struct DecodeParams {
   const uint32_t* runs;
   const uint32_t* maskbits;
   const uint8_t* newbin_ok;
+  const uint8_t* fits_flag;
   int N, M, T;
   int P;
   const uint16_t* seq;
@@ -603,6 +604,125 @@ __global__ void reduce_kernel(int P, int M, const int32_t* infeas, const double*
   out[c] = bad ? nan("") : worst;
 }
 
+// Greedy initial solution (BRKGA_alg3.py:445-603 with binClassInitialSol.py):
+// one CTA walks the parts in the given order; each part goes where the
+// system makespan after placing it is smallest (ties: the later option wins
+// over an earlier one on another machine or a new plate, the first existing
+// plate wins within a machine): a new plate on some machine (best rotation at
+// column 0, bottom row L-1) or any existing plate of the machine that can take
+// it (every plate is tested, no area filter).  Plates live in the global pool.
+struct GreedyParams {
+  DecodeParams p;  // tables, pool, slot geometry (S = 0: every plate in the pool)
+  const int32_t* order;
+  int n;
+  int32_t* out_machine;  // [n]
+  BrkgaPlacement* out;   // [n]: gene, plate index within its machine, x, bottom row y, rotation
+  int32_t* plate_machine;
+  int32_t* plate_index;  // index of the plate within its machine
+  double* machine_makespan;  // [M]
+};
+
+__global__ void __launch_bounds__(kDecodeThreads) greedy_kernel(GreedyParams g) {
+  __shared__ SearchShared sh;
+  __shared__ int s_fail;
+  const DecodeParams& p = g.p;
+  const int tid = threadIdx.x;
+  BinScal* bs = p.binscal;
+  unsigned long long c_tests = 0, c_chunks = 0, c_bytes = 0;
+  int nplates = 0;
+  double cw = 0.0;  // current_worst_makespan
+  for (int m = tid; m < p.M; m += kDecodeThreads) g.machine_makespan[m] = 0.0;
+  __syncthreads();
+  for (int k = 0; k < g.n; ++k) {
+    const int gene = g.order[k];
+    const int t = p.gene_type[gene];
+    const double a = p.part_area[t];
+    double best = INFINITY;
+    int kind = -1, cm = -1, cb = -1;  // kind 0 = new plate, 1 = existing plate
+    unsigned long long ckey = kKeyNone;
+    double ccand = 0.0;
+    for (int m = 0; m < p.M; ++m) {
+      bool placed_in_exist = false;
+      if (!p.fits_flag[t * p.M + m]) continue;  // BRKGA_alg3.py:465-470
+      const MachDev md = p.mach[m];
+      const double mm = g.machine_makespan[m];
+      const double ptm = p.pt[(size_t)m * p.T + t], pthm = p.pth[(size_t)m * p.T + t];
+      const double cand = ((mm + md.setup) + ptm) + pthm;  // :472
+      const double nm = cw > cand ? cw : cand;
+      if (nm <= best) {
+        best = nm;
+        kind = 0;
+        cm = m;
+        ccand = cand;
+      }
+      for (int b = 0; b < nplates; ++b) {
+        if (g.plate_machine[b] != m) continue;
+        const uint32_t* grid = p.pool + (size_t)bs[b].pool * p.slot_words;
+        const unsigned long long key = search_plate(p, md, grid, reinterpret_cast<const uint16_t*>(grid + p.slot_vac_off),
+                                                    bs[b].enc, t, sh, c_tests, c_chunks, c_bytes);
+        if (key == kKeyNone) continue;
+        const double bpth = bs[b].pth;
+        const double cand2 = bpth < pthm ? ((mm - bpth) + pthm) + ptm : mm + ptm;  // :486-489
+        const double nm2 = cw > cand2 ? cw : cand2;
+        if (nm2 <= best) {
+          if (placed_in_exist && nm2 == best) continue;
+          placed_in_exist = true;
+          best = nm2;
+          kind = 1;
+          cm = m;
+          cb = b;
+          ckey = key;
+          ccand = cand2;
+        }
+      }
+    }
+    if (kind < 0) {  // fits no machine: the reference crashes here (bestBatch == [])
+      if (tid == 0) raise_status(p.status, BRKGA_ERR_BAD_INSTANCE);
+      return;
+    }
+    const MachDev md = p.mach[cm];
+    int r, x, ty, b;
+    if (kind == 0) {
+      r = p.best_rot[t];
+      if (tid == 0) s_fail = (!p.newbin_ok[t * p.M + cm] || nplates >= g.n) ? 1 : 0;
+      __syncthreads();
+      if (s_fail) {
+        if (tid == 0) raise_status(p.status, BRKGA_ERR_NEW_BIN_UNFIT);
+        return;
+      }
+      b = nplates++;
+      uint32_t* grid = p.pool + (size_t)b * p.slot_words;
+      open_plate(md, grid, reinterpret_cast<uint16_t*>(grid + p.slot_vac_off), &bs[b], b);
+      if (tid == 0) {
+        int idx = 0;
+        for (int q = 0; q < b; ++q) idx += g.plate_machine[q] == cm;
+        g.plate_machine[b] = cm;
+        g.plate_index[b] = idx;
+      }
+      x = 0;
+      ty = md.L - p.rot[t * 4 + r].h;
+    } else {
+      int y;
+      decode_key(ckey, &r, &x, &y);
+      ty = y - p.rot[t * 4 + r].h + 1;
+      b = cb;
+    }
+    uint32_t* grid = p.pool + (size_t)bs[b].pool * p.slot_words;
+    place_part(p, md, grid, reinterpret_cast<uint16_t*>(grid + p.slot_vac_off), &bs[b], t, cm, r, x, ty, a);
+    if (tid == 0) {
+      g.out_machine[k] = cm;
+      g.out[k] = BrkgaPlacement{gene, g.plate_index[b], x, ty + p.rot[t * 4 + r].h - 1, r};
+      g.machine_makespan[cm] = ccand;  // :541, :565
+    }
+    cw = cw > ccand ? cw : ccand;
+    __syncthreads();
+  }
+  if (tid == 0) {
+    atomicAdd(&p.counters[0], c_tests);
+    atomicAdd(&p.counters[3], c_bytes);
+  }
+}
+
 // ---------------------------------------------------------------- host side
 
 size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
@@ -1033,6 +1153,7 @@ int brkga_decode_stage(int32_t stage, const BrkgaProblem* pb, const float* d_chr
   dp.runs = pb->d_runs;
   dp.maskbits = pb->d_maskbits;
   dp.newbin_ok = pb->d_newbin_ok;
+  dp.fits_flag = pb->d_fits;
   dp.N = pb->N;
   dp.M = pb->M;
   dp.T = pb->T;
@@ -1155,6 +1276,100 @@ int brkga_evaluate_host(BrkgaProblem* pb, const float* h_chrom, int32_t P, doubl
     return BRKGA_OK;
   }
   return BRKGA_ERR_CAPACITY;
+}
+
+int brkga_initial_solution_host(BrkgaProblem* pb, const int32_t* h_order, int32_t n, int32_t* h_machine,
+                                BrkgaPlacement* h_place, double* h_machine_makespan) {
+  if (!pb || n < 0 || (n > 0 && (!h_order || !h_machine || !h_place)) || !h_machine_makespan)
+    return BRKGA_ERR_INVALID_ARGUMENT;
+  for (int k = 0; k < n; ++k)
+    if (h_order[k] < 0 || h_order[k] >= pb->N) return BRKGA_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(pb->mu);
+  DeviceGuard guard(pb->device);
+  const int nn = std::max(n, 1);
+  // one allocation: order, outputs, plate tables, scalars, counters, status, pool (one plate per part at most)
+  size_t o = 0;
+  const size_t off_order = o;
+  o = align_up(o + (size_t)nn * 4, 256);
+  const size_t off_mach = o;
+  o = align_up(o + (size_t)nn * 4, 256);
+  const size_t off_out = o;
+  o = align_up(o + (size_t)nn * sizeof(BrkgaPlacement), 256);
+  const size_t off_pm = o;
+  o = align_up(o + (size_t)nn * 4, 256);
+  const size_t off_pi = o;
+  o = align_up(o + (size_t)nn * 4, 256);
+  const size_t off_mk = o;
+  o = align_up(o + (size_t)pb->M * 8, 256);
+  const size_t off_bs = o;
+  o = align_up(o + (size_t)nn * sizeof(BinScal), 256);
+  const size_t off_ctr = o;
+  o = align_up(o + 64, 256);
+  const size_t off_pool = o;
+  o = align_up(o + (size_t)nn * pb->slot_words * 4, 256);
+  char* d = nullptr;
+  if (cudaMalloc(&d, o) != cudaSuccess) return BRKGA_ERR_CUDA;
+  int st = BRKGA_OK;
+  do {
+    if (cudaMemset(d, 0, off_pool) != cudaSuccess ||
+        (n > 0 && cudaMemcpy(d + off_order, h_order, (size_t)n * 4, cudaMemcpyHostToDevice) != cudaSuccess)) {
+      st = BRKGA_ERR_CUDA;
+      break;
+    }
+    GreedyParams g;
+    DecodeParams& dp = g.p;
+    std::memset(&dp, 0, sizeof(dp));
+    dp.gene_type = pb->d_gene_type;
+    dp.mach = pb->d_mach;
+    dp.pt = pb->d_pt;
+    dp.pth = pb->d_pth;
+    dp.part_area = pb->d_area;
+    dp.nrot = pb->d_nrot;
+    dp.best_rot = pb->d_best;
+    dp.rot = pb->d_rot;
+    dp.dens = pb->d_dens;
+    dp.run_off = pb->d_run_off;
+    dp.runs = pb->d_runs;
+    dp.maskbits = pb->d_maskbits;
+    dp.newbin_ok = pb->d_newbin_ok;
+    dp.fits_flag = pb->d_fits;
+    dp.N = pb->N;
+    dp.M = pb->M;
+    dp.T = pb->T;
+    dp.status = reinterpret_cast<int32_t*>(d + off_ctr + 40);
+    dp.counters = reinterpret_cast<unsigned long long*>(d + off_ctr + 8);
+    dp.binscal = reinterpret_cast<BinScal*>(d + off_bs);
+    dp.pool = reinterpret_cast<uint32_t*>(d + off_pool);
+    dp.pool_bins = nn;
+    dp.S = 0;
+    dp.slot_words = pb->slot_words;
+    dp.slot_vac_off = pb->slot_vac_off;
+    g.order = reinterpret_cast<const int32_t*>(d + off_order);
+    g.n = n;
+    g.out_machine = reinterpret_cast<int32_t*>(d + off_mach);
+    g.out = reinterpret_cast<BrkgaPlacement*>(d + off_out);
+    g.plate_machine = reinterpret_cast<int32_t*>(d + off_pm);
+    g.plate_index = reinterpret_cast<int32_t*>(d + off_pi);
+    g.machine_makespan = reinterpret_cast<double*>(d + off_mk);
+    greedy_kernel<<<1, kDecodeThreads>>>(g);
+    int32_t status = 0;
+    if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess ||
+        cudaMemcpy(&status, dp.status, 4, cudaMemcpyDeviceToHost) != cudaSuccess) {
+      st = BRKGA_ERR_CUDA;
+      break;
+    }
+    if (status) {
+      st = status;
+      break;
+    }
+    if ((n > 0 && (cudaMemcpy(h_machine, g.out_machine, (size_t)n * 4, cudaMemcpyDeviceToHost) != cudaSuccess ||
+                   cudaMemcpy(h_place, g.out, (size_t)n * sizeof(BrkgaPlacement), cudaMemcpyDeviceToHost) !=
+                       cudaSuccess)) ||
+        cudaMemcpy(h_machine_makespan, g.machine_makespan, (size_t)pb->M * 8, cudaMemcpyDeviceToHost) != cudaSuccess)
+      st = BRKGA_ERR_CUDA;
+  } while (false);
+  cudaFree(d);
+  return st;
 }
 
 int brkga_last_counters(const BrkgaProblem* pb, int64_t* tests, int64_t* chunks, int64_t* bins,

@@ -43,6 +43,7 @@ class Instance:
     thresholds: List[float]
     instance_parts: np.ndarray
     masks: List[np.ndarray]
+    heights: Optional[np.ndarray] = None  # part height in mm (the greedy initial solution sorts by it)
 
 
 def _star_polygon(rng: np.random.Generator, h: int, w: int) -> np.ndarray:
@@ -152,7 +153,7 @@ def make_instance(name: str, n_parts: int, plates: Sequence[Tuple[int, int]], se
     inst_parts = np.arange(n_parts, dtype=np.int64)
     pdata = ProblemData(parts=parts, machines=machines, instance_parts=inst_parts,
                         instance_parts_unique=inst_parts.copy())
-    return Instance(name, pdata, n_parts, M, default_thresholds(M), inst_parts, masks)
+    return Instance(name, pdata, n_parts, M, default_thresholds(M), inst_parts, masks, heights)
 
 
 # Named workloads (sizes from the benchmark configurations).

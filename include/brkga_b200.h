@@ -167,6 +167,18 @@ int brkga_evaluate_host(BrkgaProblem* problem, const float* h_chrom, int32_t P,
 int brkga_last_counters(const BrkgaProblem* problem, int64_t* tests, int64_t* chunks, int64_t* bins,
                         int64_t* scan_bytes);
 
+/* Greedy initial solution (BRKGA_alg3.py:445-603, binClassInitialSol.py:41-111):
+ * the parts (gene indices, h_order[n], the reference sorts them by height and
+ * then area, both descending) are placed one by one where the largest machine
+ * makespan grows least — a new plate on a machine or any existing plate of it
+ * that can take the part.  Outputs per placement, in order: h_machine[k] and
+ * h_place[k] = (gene, plate index within the machine, x, bottom row y,
+ * rotation); h_machine_makespan[M].  Synchronous; allocates and frees its own
+ * device memory.  Building the chromosome from this is host work
+ * (brkga_fft2_b200.initial). */
+int brkga_initial_solution_host(BrkgaProblem* problem, const int32_t* h_order, int32_t n, int32_t* h_machine,
+                                BrkgaPlacement* h_place, double* h_machine_makespan);
+
 /* ---- GA generation step (device-resident population; BRKGA_alg3.py:210-265) ----
  * Randomness: Philox4x32-10 keyed by `seed`, counters (key block, row,
  * generation, stream), so results are deterministic and independent of the

@@ -207,6 +207,47 @@ static void plate_insert(Plate* p, const Rot* r, int x, int y, double part_area)
   p->enc = (p->min_row > p->max_row) ? 0 : p->L - p->min_row;
 }
 
+/* The choice part of can_insert (binClassNew.py:45-117, binClassInitialSol.py:41-111):
+ * returns 1 and (x, y, rotation) when some rotation fits. */
+static int best_position(const Plate* p, const Model* m, int t, double part_area, int* ox, int* oy, int* orot) {
+  const BrkgaProblemDesc* d = m->d;
+  int nrot = d->part_nrot[t];
+  double potential = p->area + part_area;
+  int found = 0, have_best = 0, bx = 0, by = 0, br = 0;
+  double packing_density = 0.0;
+  for (int r = 0; r < nrot; ++r) {
+    const Rot* R = &m->rots[t * 4 + r];
+    if (R->h > p->L || R->w > p->W) continue;
+    if (!vacancy_fit(p->vac, p->L, R->dens, R->h)) continue;
+    int x, y;
+    if (!bottom_left(p, R, &x, &y)) continue;
+    found = 1;
+    int top = y - R->h + 1;
+    int new_len = p->enc > (p->L - top) ? p->enc : (p->L - top);
+    double dens = potential / (double)((int64_t)new_len * p->W);
+    if (dens > packing_density) {
+      have_best = 1;
+      packing_density = dens;
+      bx = x;
+      by = y;
+      br = r;
+    } else if (have_best && dens == packing_density && y > by) {
+      bx = x;
+      by = y;
+      br = r;
+    } else if (have_best && dens == packing_density && y == by && x < bx) {
+      bx = x;
+      by = y;
+      br = r;
+    }
+  }
+  if (!found || !have_best) return 0;
+  *ox = bx;
+  *oy = by;
+  *orot = br;
+  return 1;
+}
+
 /* binClassNew.py:45-144.  Returns 1 if the part was inserted. */
 static int can_insert(Plate* p, const Model* m, int t, double part_area, double pt, double pth,
                       BrkgaPlacement* log, int gene, int bin_idx) {
@@ -425,6 +466,106 @@ int oracle_decode(const BrkgaProblemDesc* d, const float* chrom, int P, double* 
     if (jobs[i].err) err = jobs[i].err;
   free(jobs);
   free(th);
+  model_free(&m);
+  return err;
+}
+
+/* Greedy initial solution, BRKGA_alg3.py:445-566 with binClassInitialSol.BuildingPlate:
+ * parts in `order` (gene indices); each goes to the option with the smallest
+ * max(current worst makespan, machine makespan after placing it): a new plate
+ * on a machine (checked first, replaced on <=), or an existing plate of the
+ * machine (every plate tested, no area filter; within a machine an equal
+ * makespan does not replace an earlier plate).  Outputs as brkga_initial_solution_host. */
+int oracle_initial_solution(const BrkgaProblemDesc* d, const int32_t* order, int n, int32_t* out_machine,
+                            BrkgaPlacement* out, double* machine_makespan) {
+  if (!d || n < 0) return BRKGA_ERR_INVALID_ARGUMENT;
+  Model m;
+  model_init(&m, d);
+  const int M = d->n_machines, T = d->n_types;
+  Plate* plates = (Plate*)malloc(sizeof(Plate) * (size_t)(n > 0 ? n : 1));
+  int* pmach = (int*)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+  int* pidx = (int*)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+  int np = 0, err = 0;
+  double cw = 0.0;
+  for (int q = 0; q < M; ++q) machine_makespan[q] = 0.0;
+  for (int k = 0; k < n && !err; ++k) {
+    int gene = order[k], t = d->gene_type[gene];
+    double a = d->part_area[t];
+    double best = INFINITY, ccand = 0.0;
+    int kind = -1, cm = -1, cb = -1, cx = 0, cy = 0, cr = 0;
+    for (int q = 0; q < M; ++q) {
+      int placed_in_exist = 0;
+      int L = d->bin_length[q], W = d->bin_width[q];
+      int h0 = d->rot_h[t * 4], w0 = d->rot_w[t * 4];
+      if ((h0 > L || w0 > W) && (w0 > L || h0 > W)) continue; /* :465-470 */
+      double mm = machine_makespan[q];
+      double pt = d->proc_time[(size_t)q * T + t], pth = d->proc_time_height[(size_t)q * T + t];
+      double cand = ((mm + d->setup_time[q]) + pt) + pth; /* :472 */
+      double nm = cw > cand ? cw : cand;
+      if (nm <= best) {
+        best = nm;
+        kind = 0;
+        cm = q;
+        ccand = cand;
+      }
+      for (int b = 0; b < np; ++b) {
+        if (pmach[b] != q) continue;
+        int x, y, r;
+        if (!best_position(&plates[b], &m, t, a, &x, &y, &r)) continue;
+        double cand2 = plates[b].pth < pth ? ((mm - plates[b].pth) + pth) + pt : mm + pt; /* :486-489 */
+        double nm2 = cw > cand2 ? cw : cand2;
+        if (nm2 <= best) {
+          if (placed_in_exist && nm2 == best) continue;
+          placed_in_exist = 1;
+          best = nm2;
+          kind = 1;
+          cm = q;
+          cb = b;
+          cx = x;
+          cy = y;
+          cr = r;
+          ccand = cand2;
+        }
+      }
+    }
+    if (kind < 0) {
+      err = BRKGA_ERR_BAD_INSTANCE;
+      break;
+    }
+    int L = d->bin_length[cm], W = d->bin_width[cm];
+    if (kind == 0) {
+      cr = d->part_best_rot[t];
+      const Rot* R = &m.rots[t * 4 + cr];
+      if (R->h > L || R->w > W) {
+        err = BRKGA_ERR_NEW_BIN_UNFIT;
+        break;
+      }
+      cb = np++;
+      plate_init(&plates[cb], L, W);
+      pmach[cb] = cm;
+      int idx = 0;
+      for (int b = 0; b < cb; ++b) idx += pmach[b] == cm;
+      pidx[cb] = idx;
+      cx = 0;
+      cy = L - 1;
+    }
+    plate_insert(&plates[cb], &m.rots[t * 4 + cr], cx, cy, a);
+    plates[cb].pt += d->proc_time[(size_t)cm * T + t];
+    double pthc = d->proc_time_height[(size_t)cm * T + t];
+    if (pthc > plates[cb].pth) plates[cb].pth = pthc;
+    out_machine[k] = cm;
+    out[k].gene = gene;
+    out[k].bin = pidx[cb];
+    out[k].x = cx;
+    out[k].y = cy;
+    out[k].rot = cr;
+    machine_makespan[cm] = ccand;
+    if (ccand > cw) cw = ccand;
+  }
+  for (int b = 0; b < np; ++b) plate_free(&plates[b]);
+  free(plates);
+  free(pmach);
+  free(pidx);
   model_free(&m);
   return err;
 }

@@ -70,3 +70,23 @@ def oracle_decode(packed, chromosomes: np.ndarray, n_threads: int = 1, with_log:
                            log.ctypes.data_as(ctypes.c_void_p) if with_log else None, int(n_threads))
     abi.check(st, "oracle_decode")
     return (out, log) if with_log else out
+
+
+def oracle_initial_solution(packed, order):
+    """Greedy initial placements on the CPU (oracle_initial_solution in brkga_oracle.c)."""
+    lib = _load()
+    if not hasattr(lib, "_init_sol_declared"):
+        lib.oracle_initial_solution.restype = ctypes.c_int
+        lib.oracle_initial_solution.argtypes = [ctypes.POINTER(abi.BrkgaProblemDesc), ctypes.c_void_p, ctypes.c_int,
+                                                ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        lib._init_sol_declared = True
+    order = np.ascontiguousarray(order, dtype=np.int32)
+    n = order.size
+    machine = np.zeros(max(n, 1), np.int32)
+    place = np.zeros(max(n, 1), abi.PLACEMENT_DTYPE)
+    mk = np.zeros(packed.n_machines, np.float64)
+    st = lib.oracle_initial_solution(ctypes.byref(packed.desc), order.ctypes.data_as(ctypes.c_void_p), n,
+                                     machine.ctypes.data_as(ctypes.c_void_p), place.ctypes.data_as(ctypes.c_void_p),
+                                     mk.ctypes.data_as(ctypes.c_void_p))
+    abi.check(st, "oracle_initial_solution")
+    return machine[:n], place[:n], mk

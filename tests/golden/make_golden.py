@@ -30,6 +30,7 @@ from __future__ import annotations
 
 import argparse
 import glob
+import textwrap
 import json
 import os
 import sys
@@ -171,6 +172,58 @@ class Reference:
         return float(ms), log
 
 
+def reference_greedy(ref, root, rpd, nb_parts, nb_machines, thresholds, inst_parts, heights, areas, seed):
+    """Run the reference's own greedy initial solution (the block of BRKGA_alg3.py
+    from its "CREATE INITIAL SOLUTION" marker to its "CALL BRKGA" marker) on
+    our instance; returns (chromosome, makespan, placements in order as
+    (machine, plate, part, x, y, rot))."""
+    import random
+    import pandas
+    import binClassInitialSol
+    src = open(os.path.join(root, "BRKGA_alg3.py")).read()
+    q3 = "'" * 3
+    a = src.rindex("\n", 0, src.index(q3 + " CREATE INITIAL SOLUTION " + q3)) + 1
+    b = src.rindex("\n", 0, src.index(q3 + " CALL BRKGA" + q3)) + 1
+    block = textwrap.dedent(src[a:b])  # the block is indented under `if __name__ == "__main__":`
+    ids = sorted(set(int(p) for p in inst_parts))
+
+    class PandasWithAreas:  # the block reads polygon areas with pd.read_excel; serve the same numbers
+        def __getattr__(self, name):
+            return getattr(pandas, name)
+
+        def read_excel(self, *a, **k):
+            return pandas.DataFrame({"Area": [areas[i] for i in ids]}, index=pandas.Index(ids, name="part ID"))
+
+    rot_of = {}
+    for pid, p in rpd.parts.items():
+        for r, arr in enumerate(p.rotations_uint8):
+            rot_of[id(arr)] = (int(pid), r)
+    rec = []
+    orig = binClassInitialSol.BuildingPlate.insert
+
+    def insert(plate, x, y, partMatrix, shapes, partArea, gpu_tensor=None):
+        rec.append((plate, int(x), int(y)) + rot_of[id(partMatrix)])
+        return orig(plate, x, y, partMatrix, shapes, partArea, gpu_tensor=gpu_tensor)
+
+    binClassInitialSol.BuildingPlate.insert = insert
+    jobSpec = pandas.DataFrame({"height(mm)": [heights[i] for i in ids]}, index=pandas.Index(ids))
+    ns = {"np": np, "pd": PandasWithAreas(), "random": random, "problem_data": rpd, "nbMachines": nb_machines,
+          "nbParts": nb_parts, "instanceParts": np.asarray(inst_parts), "jobSpec": jobSpec,
+          "collision_backend": ref.backend, "BuildingPlate": binClassInitialSol.BuildingPlate,
+          "thresholds": list(thresholds), "print": lambda *a, **k: None}
+    random.seed(seed)
+    try:
+        exec(compile(block, "BRKGA_alg3.py:initial-solution", "exec"), ns)
+    finally:
+        binClassInitialSol.BuildingPlate.insert = orig
+    plates = {}
+    for m in range(nb_machines):
+        for b, batch in enumerate(ns["machines_dict"][f"machine_{m}"]["batches"]):
+            plates[id(batch)] = (m, b)
+    out = np.array([plates[id(pl)] + (pid, x, y, r) for pl, x, y, pid, r in rec], np.int64)
+    return np.asarray(ns["array"], np.float64), float(ns["best_makespan"]), out
+
+
 def log_to_array(log, nb_machines, nb_parts):
     """Per machine ordered placements -> int64 [M, N, 5] (part, bin, x, y, rot), -1 padded."""
     out = -np.ones((nb_machines, nb_parts, 5), np.int64)
@@ -178,6 +231,11 @@ def log_to_array(log, nb_machines, nb_parts):
         for k, rec in enumerate(log[m]):
             out[m, k] = rec
     return out
+
+
+def real_heights(root):
+    spec = read_xlsx(os.path.join(root, "data/PartsMachines/part-machine-information.xlsx"))
+    return {int(r["A"]): r["D"] for r in spec["part"][1:]}
 
 
 def real_problem(root, nb_parts, nb_machines, inst):
@@ -333,6 +391,33 @@ def main():
     # full-row and single-cell masks, plates barely larger than the parts
     edge = syn.make_instance("edge", 12, [(24, 24), (20, 31)], 11, bbox_min=1, bbox_max=18, fill=(0.3, 1.0))
     syn_case("syn_edge", edge, syn.chromosomes(48, 12, 8))
+    # --- greedy initial solutions (BRKGA_alg3.py:445-603) ------------------------
+    def greedy_case(tag, pd, nb_parts, nb_machines, thr, ip, heights, areas, seeds):
+        if not want(tag):
+            return
+        rpd = ref.problem(pd, nb_machines)
+        chroms, mks, recs = [], [], []
+        for sd in seeds:
+            c, mk, out = reference_greedy(ref, root, rpd, nb_parts, nb_machines, thr, ip, heights, areas, sd)
+            chroms.append(c)
+            mks.append(mk)
+            recs.append(out)
+        ids = sorted(set(int(p) for p in ip))
+        save_instance(os.path.join(args.out, f"{tag}.npz"), pd, nb_parts, nb_machines, thr, ip, extra={
+            "greedy_seeds": np.array(seeds), "greedy_chromosomes": np.stack(chroms), "greedy_makespans": np.array(mks),
+            "greedy_placements": np.stack(recs), "height_ids": np.array(ids),
+            "heights": np.array([heights[i] for i in ids], np.float64)})
+        print(f"{tag}: {len(seeds)} greedy runs  [{time.time() - t0:.1f}s]")
+
+    hts = real_heights(root)
+    for (n, mm, k) in ((50, 2, 0), (75, 2, 0), (100, 4, 0)):
+        pd, ip, thr = real_problem(root, n, mm, k)
+        greedy_case(f"greedy_P{n}M{mm}-{k}", pd, n, mm, thr, ip, hts, {p: pd.parts[p].area for p in pd.parts},
+                    [1, 2])
+    for inst in (syn.p50m2(0), syn.p100m4(0)):
+        hd = {p: float(inst.heights[p]) for p in range(inst.nb_parts)}
+        greedy_case(f"greedy_syn_{inst.name}", inst.problem_data, inst.nb_parts, inst.nb_machines,
+                    inst.thresholds, inst.instance_parts, hd, {p: inst.problem_data.parts[p].area for p in hd}, [3])
     print(f"done in {time.time() - t0:.1f}s")
 
 
