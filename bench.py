@@ -49,7 +49,8 @@ def parse():
 
 
 def chrom_seed(rank: int, step: int) -> int:
-    return 1_000_003 * (rank + 1) + step
+    from brkga_fft2_b200.shard import rank_seed
+    return rank_seed(rank, step)
 
 
 def load_workload():
@@ -227,12 +228,9 @@ def run_ours(args):
     status = int(dd.status.item())
     tests, chunks, bins, scan = dd.counters()  # counters of the last step
 
-    total_ms = sum(step_ms)
-    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms = float(t.item())
-    value = world * P * args.steps / (total_ms / 1000.0)
+    from brkga_fft2_b200.shard import max_over_ranks, weak_throughput
+    total_ms = max_over_ranks(sum(step_ms), dist, "cuda")
+    value = weak_throughput(P * args.steps, world, total_ms / 1000.0)
 
     # e2e through the drop-in evaluator (host buffers, pinned input)
     evaluator = B200DecoderEvaluator(inst.problem_data, inst.nb_parts, inst.nb_machines, inst.thresholds,
@@ -249,10 +247,7 @@ def run_ours(args):
         t0 = time.perf_counter()
         last = evaluator.evaluate_batch(pinned[args.warmup + s])
         e2e_t += time.perf_counter() - t0
-    t = torch.tensor([e2e_t], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_value = world * P * args.steps / float(t.item())
+    e2e_value = weak_throughput(P * args.steps, world, max_over_ranks(e2e_t, dist, "cuda"))
     ref_last = out.cpu().numpy()
     same = bool(np.array_equal(np.asarray(last), ref_last))
 
