@@ -13,6 +13,7 @@ import numpy as np
 
 ABI_VERSION = 1
 NOALLOC_SCRATCH_BYTES = 64 << 20  # BRKGA_NOALLOC_SCRATCH_BYTES
+MAX_INSTANCES = 64  # BRKGA_MAX_INSTANCES
 
 OK = 0
 ERR_INVALID_ARGUMENT = 1
@@ -138,6 +139,13 @@ def load_library(path: str = LIB_PATH):
         "brkga_surrogate_adam": (c_int, [vp, ctypes.c_float, vp]),
         "brkga_surrogate_buffers": (c_int, [vp, vp, vp, vp, vp, vp, vp, vp]),
         "brkga_surrogate_io": (c_int, [vp, c_i32, vp, c_i64, c_i32]),
+        "brkga_problem_create_multi": (c_int, [P(BrkgaProblemDesc), c_i32, P(vp)]),
+        "brkga_problem_instances": (c_int, [vp, P(c_i32)]),
+        "brkga_workspace_bytes_multi": (c_int, [vp, P(c_i32), c_i64, P(c_sz)]),
+        "brkga_decode_multi": (c_int, [vp, vp, P(c_i32), vp, vp, vp, vp, c_sz, c_i64, vp]),
+        "brkga_decode_multi_stage": (c_int, [c_i32, vp, vp, P(c_i32), vp, vp, vp, vp, c_sz, c_i64, vp]),
+        "brkga_set_launch_config": (c_int, [vp, c_i32, c_i32]),
+        "brkga_get_launch_config": (c_int, [vp, P(c_i32), P(c_i32), P(c_i32)]),
         "brkga_evaluate_host": (c_int, [vp, P(ctypes.c_float), c_i32, P(ctypes.c_double), vp]),
         "brkga_last_counters": (c_int, [vp, P(c_i64), P(c_i64), P(c_i64), P(c_i64)]),
     }

@@ -7,23 +7,31 @@
 // positions with a float FFT correlation; here the correlation is evaluated
 // exactly on bit-packed rows, which yields the same feasible set.
 //
-// Pipeline per population (three launches on one stream, no host sync):
+// A problem holds K >= 1 independent instances (own parts, machines, plate
+// sizes).  Their tables are merged into one set of device arrays: part types,
+// rotations, mask rows and machines get absolute indices, and each instance
+// records its bases (InstDev).  A launch decodes P_k chromosomes of every
+// instance k; the per-launch row/item offsets travel in the kernel
+// parameters (InstRun), so one launch of each kernel serves all instances.
+//
+// Pipeline per launch (three kernels on one stream, no host sync):
 //   1. assign_sort_kernel  one CTA per chromosome: machine of every gene from
 //      the machine keys, then a bitonic sort of (machine, sequencing key,
 //      gene) 64-bit keys in shared memory -> per-(chromosome, machine) part
-//      order (placement.py:118-135).
-//   2. decode_kernel       persistent CTAs of 4 warps pulling (chromosome,
-//      machine) items from a device counter.  A plate is L rows of
-//      ceil(W/32)+2 32-bit words (bit x of a row = cell x); the first S plates
-//      of an item live in shared memory, further ones in a global pool.  For
-//      each part: first-fit over plates (area filter, then the collision
-//      search), else a new plate with the best rotation at (0, L-1).
-//      The collision search splits (rotation, 32 candidate rows) chunks over
-//      the warps; a lane tests one candidate top row: vacancy filter, then
-//      the exact run-dilation test word by word, giving the leftmost free x.
-//      Results are merged with a 64-bit lexicographic key
-//      (newLen, -y, x, rotation) by atomicMin in shared memory, which is the
-//      reference's rotation rule (binClassNew.py:101-117) — see key_of().
+//      order (placement.py:118-135).  order_items_kernel then sorts the
+//      (chromosome, machine) items of all instances by part count.
+//   2. decode_kernel       persistent CTAs of 4 warps pulling items, longest
+//      first, from a device counter.  A plate is L rows of ceil(W/32)+2
+//      32-bit words (bit x of a row = cell x); the first S plates of an item
+//      live in shared memory, further ones in a global pool.  For each part:
+//      first-fit over plates (area filter, then the collision search), else a
+//      new plate with the best rotation at (0, L-1).  The collision search
+//      splits (rotation, 32 candidate rows) chunks over the warps; a lane
+//      tests one candidate top row: vacancy filter, then the exact
+//      run-dilation test word by word, giving the leftmost free x.  Results
+//      are merged with a 64-bit lexicographic key (newLen, -y, x, rotation)
+//      by atomicMin in shared memory, which is the reference's rotation rule
+//      (binClassNew.py:101-117) — see key_of().
 //   3. reduce_kernel       max over machines, 1e16 for infeasible chromosomes.
 
 #include <cuda_runtime.h>
@@ -43,6 +51,9 @@ constexpr int kMaxMachines = 255;
 constexpr int kMaxGenes = 8192;     // bitonic sort buffer: 8192 x 8 B = 64 KB shared memory
 constexpr int kMaxSide = 8191;      // 13-bit fields of the selection key
 constexpr int kDecodeThreads = 128; // 4 warps per item
+constexpr int kMaxInst = BRKGA_MAX_INSTANCES;
+constexpr int kMaxCtasPerSm = 32;
+constexpr int kMaxSmemPlates = 8;
 constexpr unsigned long long kKeyNone = ~0ull;
 constexpr unsigned kFull = 0xFFFFFFFFu;
 
@@ -65,55 +76,68 @@ struct BinScal {     // per-plate scalars of binClassNew.BuildingPlate
   int minrow, maxrow, enc, pool;
 };
 
-struct DecodeParams {
+// Where instance k's entries start in the merged tables.
+struct InstDev {
+  int N, M, T, mode;
+  int gbase;    // gene_type[gbase + j]: absolute part type of gene j
+  int tbase;    // first absolute part type
+  int mbase;    // mach[mbase + m]
+  int thrbase;  // thr[thrbase + m], M - 1 entries
+  int tmbase;   // pt/pth[tmbase + m*T + t], newbin_ok/fits[tmbase + t*M + m] (t local)
+};
+
+// Merged device tables of all instances of a problem.
+struct Tables {
+  const InstDev* inst;
   const int32_t* gene_type;
+  const double* thr;
   const MachDev* mach;
   const double* pt;
   const double* pth;
-  const double* part_area;
+  const double* part_area;  // [absolute type]
   const int32_t* nrot;
   const int32_t* best_rot;
-  const RotDev* rot;
+  const RotDev* rot;        // [absolute type * 4 + rotation]
   const uint16_t* dens;
   const int32_t* run_off;
   const uint32_t* runs;
   const uint32_t* maskbits;
   const uint8_t* newbin_ok;
-  const uint8_t* fits_flag;
-  int N, M, T;
-  int P;
-  const uint16_t* seq;
-  const int32_t* cnt;
-  const int32_t* infeas;
-  const int32_t* order;
+  const uint8_t* fits;
+};
+
+// One instance's slice of a launch.
+struct InstRun {
+  int P;               // chromosomes of this instance in the launch
+  int crow0;           // first row in chrom / makespan / infeas
+  int item0;           // first (chromosome, machine) item
+  int S2;              // bitonic sort width (power of two >= N)
+  long long chrom_off; // first float of its chromosomes
+  long long seq0;      // first entry of its part orders (and log entries), N per item
+};
+
+// Everything a launch needs besides the tables.
+struct Run {
+  int K, n_rows, n_items, Nmax;
+  const float* chrom;
+  double* out;
+  uint16_t* seq;
+  int32_t* cnt;
+  int32_t* infeas;
+  int32_t* order;
   double* mk;
   BrkgaPlacement* log;
   int32_t* status;
   unsigned int* item_ctr;
   unsigned int* pool_ctr;
   unsigned long long* counters;
-  BinScal* binscal;
+  BinScal* binscal;  // Nmax per resident CTA
   uint32_t* pool;
   long long pool_bins;
-  int S;
-  int slot_words;
-  int slot_vac_off;
+  int S, slot_words, slot_vac_off;
+  InstRun r[kMaxInst];
 };
-
-struct AssignParams {
-  const float* chrom;
-  const double* thr;
-  const int32_t* gene_type;
-  const uint8_t* fits;
-  int N, M, mode, S2;
-  uint16_t* seq;
-  int32_t* cnt;
-  int32_t* infeas;
-  int32_t* status;
-  unsigned int* item_ctr;
-  unsigned int* pool_ctr;
-  unsigned long long* counters;
-};
+static_assert(sizeof(Tables) + sizeof(Run) <= 4096, "kernel parameters must stay within 4 KB");
 
 // ---------------------------------------------------------------- device helpers
 
@@ -260,44 +284,72 @@ __device__ __forceinline__ void raise_status(int32_t* status, int code) {
   atomicCAS(status, 0, code);
 }
 
+
+// Instance of a launch row / item: the last instance starting at or before v
+// (instances with no rows share their start with the next one, which wins).
+__device__ __forceinline__ int inst_of_row(const Run& run, int v) {
+  int lo = 0, hi = run.K - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (run.r[mid].crow0 <= v) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ int inst_of_item(const Run& run, int v) {
+  int lo = 0, hi = run.K - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (run.r[mid].item0 <= v) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
 // ---------------------------------------------------------------- kernels
 
-__global__ void assign_sort_kernel(AssignParams p) {
+__global__ void assign_sort_kernel(const __grid_constant__ Tables tb, const __grid_constant__ Run run) {
   extern __shared__ unsigned long long keys[];
   __shared__ int s_cnt[kMaxMachines + 1];
   __shared__ int s_start[kMaxMachines + 1];
   __shared__ int s_inf;
-  const int c = blockIdx.x, tid = threadIdx.x, nt = blockDim.x;
-  const int N = p.N, M = p.M;
-  if (c == 0 && tid == 0) {
-    *p.item_ctr = 0u;
-    *p.pool_ctr = 0u;
-    p.counters[0] = p.counters[1] = p.counters[2] = p.counters[3] = 0ull;
-    *p.status = 0;
+  const int row = blockIdx.x, tid = threadIdx.x, nt = blockDim.x;
+  const int k = inst_of_row(run, row);
+  const InstRun& ir = run.r[k];
+  const InstDev id = tb.inst[k];
+  const int N = id.N, M = id.M, S2 = ir.S2, c = row - ir.crow0;
+  if (row == 0 && tid == 0) {
+    *run.item_ctr = 0u;
+    *run.pool_ctr = 0u;
+    run.counters[0] = run.counters[1] = run.counters[2] = run.counters[3] = 0ull;
+    *run.status = 0;
   }
   for (int i = tid; i <= M; i += nt) s_cnt[i] = 0;
   if (tid == 0) s_inf = 0;
   __syncthreads();
-  const float* ch = p.chrom + (size_t)c * 2 * N;
-  for (int i = tid; i < p.S2; i += nt) {
+  const float* ch = run.chrom + ir.chrom_off + (long long)c * 2 * N;
+  const double* thr = tb.thr + id.thrbase;
+  for (int i = tid; i < S2; i += nt) {
     unsigned long long key = ~0ull;
     if (i < N) {
-      const int m = machine_of(ch[N + i], p.thr, M, p.mode);
+      const int m = machine_of(ch[N + i], thr, M, id.mode);
       atomicAdd(&s_cnt[m], 1);
-      if (m < M && !p.fits[p.gene_type[i] * M + m]) s_inf = 1;  // placement.py:47-53
+      const int t = tb.gene_type[id.gbase + i] - id.tbase;
+      if (m < M && !tb.fits[id.tmbase + t * M + m]) s_inf = 1;  // placement.py:47-53
       key = ((unsigned long long)m << 48) | ((unsigned long long)ordered_bits(ch[i]) << 16) |
             (unsigned long long)i;
     }
     keys[i] = key;
   }
   __syncthreads();
-  for (int k = 2; k <= p.S2; k <<= 1) {
-    for (int j = k >> 1; j > 0; j >>= 1) {
-      for (int i = tid; i < p.S2; i += nt) {
+  for (int kk = 2; kk <= S2; kk <<= 1) {
+    for (int j = kk >> 1; j > 0; j >>= 1) {
+      for (int i = tid; i < S2; i += nt) {
         const int ixj = i ^ j;
         if (ixj > i) {
           const unsigned long long a = keys[i], b = keys[ixj];
-          const bool up = (i & k) == 0;
+          const bool up = (i & kk) == 0;
           if ((a > b) == up) {
             keys[i] = b;
             keys[ixj] = a;
@@ -315,35 +367,43 @@ __global__ void assign_sort_kernel(AssignParams p) {
     }
   }
   __syncthreads();
+  uint16_t* seq = run.seq + ir.seq0 + (long long)c * M * N;
   for (int i = tid; i < N; i += nt) {
     const unsigned long long key = keys[i];
     const int m = (int)(key >> 48);
-    if (m < M) p.seq[((size_t)c * M + m) * N + (i - s_start[m])] = (uint16_t)(key & 0xFFFFu);
+    if (m < M) seq[(long long)m * N + (i - s_start[m])] = (uint16_t)(key & 0xFFFFu);
   }
-  for (int m = tid; m < M; m += nt) p.cnt[(size_t)c * M + m] = s_cnt[m];
-  if (tid == 0) p.infeas[c] = s_inf;
+  for (int m = tid; m < M; m += nt) run.cnt[ir.item0 + c * M + m] = s_cnt[m];
+  if (tid == 0) run.infeas[row] = s_inf;
 }
 
-// Items in decreasing part count (infeasible chromosomes last): the persistent
-// CTAs pull them in this order, so the longest decodes start first.
-__global__ void order_items_kernel(int n_items, int M, int N, const int32_t* cnt, const int32_t* infeas,
-                                   int32_t* order) {
-  extern __shared__ int start[];  // N + 1 weights
-  const int tid = threadIdx.x, nt = blockDim.x;
-  for (int i = tid; i <= N; i += nt) start[i] = 0;
+// Weight of an item for the longest-first order: its part count, 0 when the
+// chromosome is infeasible (nothing to decode).
+__device__ __forceinline__ int item_weight(const Tables& tb, const Run& run, int item) {
+  const int k = inst_of_item(run, item);
+  const int row = run.r[k].crow0 + (item - run.r[k].item0) / tb.inst[k].M;
+  return run.infeas[row] ? 0 : run.cnt[item];
+}
+
+// Items of all instances in decreasing part count: the persistent CTAs pull
+// them in this order, so the longest decodes start first.
+__global__ void order_items_kernel(const __grid_constant__ Tables tb, const __grid_constant__ Run run) {
+  extern __shared__ int start[];  // Nmax + 1 weights
+  const int tid = threadIdx.x, nt = blockDim.x, Nw = run.Nmax;
+  for (int i = tid; i <= Nw; i += nt) start[i] = 0;
   __syncthreads();
-  for (int i = tid; i < n_items; i += nt) atomicAdd(&start[infeas[i / M] ? 0 : cnt[i]], 1);
+  for (int i = tid; i < run.n_items; i += nt) atomicAdd(&start[item_weight(tb, run, i)], 1);
   __syncthreads();
   if (tid == 0) {
     int acc = 0;
-    for (int w = N; w >= 0; --w) {
+    for (int w = Nw; w >= 0; --w) {
       const int h = start[w];
       start[w] = acc;
       acc += h;
     }
   }
   __syncthreads();
-  for (int i = tid; i < n_items; i += nt) order[atomicAdd(&start[infeas[i / M] ? 0 : cnt[i]], 1)] = i;
+  for (int i = tid; i < run.n_items; i += nt) run.order[atomicAdd(&start[item_weight(tb, run, i)], 1)] = i;
 }
 
 // Shared state of one CTA-cooperative plate search.
@@ -353,12 +413,12 @@ struct SearchShared {
   int rlist[4];
 };
 
-// Best placement key of part type t on one plate (kKeyNone if it does not
-// fit): the four warps pull (rotation, 32 candidate top rows) chunks from a
-// shared counter (rotations interleaved, bottom rows first), skip chunks that
-// cannot beat the best key found so far, and merge with atomicMin.  Called
-// by all threads of the CTA; contains __syncthreads.
-__device__ __forceinline__ unsigned long long search_plate(const DecodeParams& p, const MachDev& md,
+// Best placement key of part type t (absolute) on one plate (kKeyNone if it
+// does not fit): the four warps pull (rotation, 32 candidate top rows) chunks
+// from a shared counter (rotations interleaved, bottom rows first), skip
+// chunks that cannot beat the best key found so far, and merge with
+// atomicMin.  Called by all threads of the CTA; contains __syncthreads.
+__device__ __forceinline__ unsigned long long search_plate(const Tables& tb, const MachDev& md,
                                                            const uint32_t* grid, const uint16_t* vac, int enc,
                                                            int t, SearchShared& sh, unsigned long long& c_tests,
                                                            unsigned long long& c_chunks,
@@ -366,9 +426,9 @@ __device__ __forceinline__ unsigned long long search_plate(const DecodeParams& p
   const int tid = threadIdx.x, lane = tid & 31;
   if (tid == 0) {
     int nr = 0, hmin = kMaxSide + 1;
-    const int nrot = p.nrot[t];
+    const int nrot = tb.nrot[t];
     for (int r = 0; r < nrot; ++r) {
-      const RotDev rd = p.rot[t * 4 + r];
+      const RotDev rd = tb.rot[t * 4 + r];
       if (rd.h <= md.L && rd.w <= md.W) {  // numba_utils.py:82-84
         sh.rlist[nr++] = r;
         hmin = min(hmin, rd.h);
@@ -390,7 +450,7 @@ __device__ __forceinline__ unsigned long long search_plate(const DecodeParams& p
     if (ci >= total) break;
     const int r = sh.rlist[ci % nr];
     const int level = ci / nr;
-    const RotDev rd = p.rot[t * 4 + r];
+    const RotDev rd = tb.rot[t * 4 + r];
     const int ty_hi = md.L - rd.h - 32 * level;
     if (ty_hi < 0) continue;
     unsigned long long cur = 0;
@@ -399,7 +459,7 @@ __device__ __forceinline__ unsigned long long search_plate(const DecodeParams& p
     if (key_of(max(enc, md.L - ty_hi), ty_hi + rd.h - 1, 0, r) >= cur) continue;
     const int ty = ty_hi - lane;
     int x = -1;
-    if (ty >= 0 && vacancy_ok(vac, ty, rd, p.dens)) x = first_free_x(grid, md.RS, md.W, ty, rd, p.run_off, p.runs);
+    if (ty >= 0 && vacancy_ok(vac, ty, rd, tb.dens)) x = first_free_x(grid, md.RS, md.W, ty, rd, tb.run_off, tb.runs);
     const unsigned fm = __ballot_sync(kFull, x >= 0);
     if (lane == 0) ++c_chunks;
     if (fm) {
@@ -417,16 +477,18 @@ __device__ __forceinline__ unsigned long long search_plate(const DecodeParams& p
   return key;
 }
 
-// Insert rotation r of part type t with its top row at ty and left column x
-// (binClassNew.py:155-174): OR the mask rows into the plate words, recompute
-// the vacancy of the touched rows (numba_utils.py:160-188); thread 0 updates
-// the plate scalars.  All threads of the CTA; contains __syncthreads.
-__device__ __forceinline__ void place_part(const DecodeParams& p, const MachDev& md, uint32_t* grid, uint16_t* vac,
-                                           BinScal* scal, int t, int m, int r, int x, int ty, double a) {
+// Insert rotation r of part type t (absolute) with its top row at ty and left
+// column x (binClassNew.py:155-174): OR the mask rows into the plate words,
+// recompute the vacancy of the touched rows (numba_utils.py:160-188); thread 0
+// updates the plate scalars with the part's area and times on this machine.
+// All threads of the CTA; contains __syncthreads.
+__device__ __forceinline__ void place_part(const Tables& tb, const MachDev& md, uint32_t* grid, uint16_t* vac,
+                                           BinScal* scal, int t, int r, int x, int ty, double a, double ptv,
+                                           double pthv) {
   const int tid = threadIdx.x;
-  const RotDev rd = p.rot[t * 4 + r];
+  const RotDev rd = tb.rot[t * 4 + r];
   const int sx = x & 31, wx = x >> 5, span = rd.mw + 1;
-  const uint32_t* mb = p.maskbits + rd.mask_base;
+  const uint32_t* mb = tb.maskbits + rd.mask_base;
   for (int idx = tid; idx < rd.h * span; idx += kDecodeThreads) {
     const int i = idx / span, j = idx - i * span;
     const uint32_t lo = j > 0 ? __ldg(mb + i * rd.mw + j - 1) : 0u;
@@ -443,9 +505,8 @@ __device__ __forceinline__ void place_part(const DecodeParams& p, const MachDev&
     s.minrow = min(s.minrow, ty);
     s.maxrow = max(s.maxrow, ty + rd.h - 1);
     s.enc = (s.minrow > s.maxrow) ? 0 : md.L - s.minrow;  // binClassNew.py:147-152
-    s.pt += p.pt[(size_t)m * p.T + t];
-    const double ph = p.pth[(size_t)m * p.T + t];
-    if (ph > s.pth) s.pth = ph;
+    s.pt += ptv;
+    if (pthv > s.pth) s.pth = pthv;
     *scal = s;
   }
   __syncthreads();
@@ -477,54 +538,89 @@ __device__ __forceinline__ void decode_key(unsigned long long key, int* r, int* 
   *y = kMaxSide - (int)((key >> 15) & 0x1FFFull);
 }
 
-__global__ void __launch_bounds__(kDecodeThreads) decode_kernel(DecodeParams p) {
+// The item a CTA is decoding, set up by thread 0.
+struct ItemCtx {
+  int item;      // global item index, -1 when the queue is empty
+  int row;       // chromosome row of the launch
+  int m, M, T;   // machine (local), machines and part types of the instance
+  int n;         // parts on this machine
+  int N;         // genes of the instance (log entries per item)
+  int gbase, tbase, tmbase;
+  int infeas;
+  long long seq; // first entry of its part order / log
+  MachDev md;
+};
+
+// At least 8 resident CTAs per SM: 64 registers per thread, no spills (left
+// free, the compiler picks fewer and spills; 56 or 48 measured slower).
+__global__ void __launch_bounds__(kDecodeThreads, 8) decode_kernel(const __grid_constant__ Tables tb,
+                                                                   const __grid_constant__ Run run) {
   extern __shared__ __align__(16) uint32_t smem[];
   __shared__ SearchShared sh;
-  __shared__ int s_item, s_fail, s_pool;
+  __shared__ ItemCtx ctx;
+  __shared__ int s_fail, s_pool;
   const int tid = threadIdx.x, lane = tid & 31;
-  BinScal* bs = p.binscal + (size_t)blockIdx.x * p.N;
+  BinScal* bs = run.binscal + (size_t)blockIdx.x * run.Nmax;
   unsigned long long c_tests = 0, c_chunks = 0, c_bins = 0, c_bytes = 0;
-  const int n_items = p.P * p.M;
 
   for (;;) {
     if (tid == 0) {
-      const int q = (int)atomicAdd(p.item_ctr, 1u);
-      s_item = q < n_items ? p.order[q] : n_items;
+      const int q = (int)atomicAdd(run.item_ctr, 1u);
+      ctx.item = -1;
+      if (q < run.n_items) {
+        const int item = run.order[q];
+        const int k = inst_of_item(run, item);
+        const InstDev id = tb.inst[k];
+        const int li = item - run.r[k].item0, c = li / id.M;
+        ctx.item = item;
+        ctx.row = run.r[k].crow0 + c;
+        ctx.m = li - c * id.M;
+        ctx.M = id.M;
+        ctx.T = id.T;
+        ctx.n = run.cnt[item];
+        ctx.N = id.N;
+        ctx.gbase = id.gbase;
+        ctx.tbase = id.tbase;
+        ctx.tmbase = id.tmbase;
+        ctx.infeas = run.infeas[ctx.row];
+        ctx.seq = run.r[k].seq0 + (long long)li * id.N;
+        ctx.md = tb.mach[id.mbase + ctx.m];
+      }
     }
     __syncthreads();
-    const int item = s_item;
-    __syncthreads();
-    if (item >= n_items) break;
-
-    const int c = item / p.M, m = item - c * p.M;
-    const MachDev md = p.mach[m];
-    BrkgaPlacement* lg = p.log ? p.log + (size_t)item * p.N : nullptr;
-    const int n = p.cnt[item];
-    if (p.infeas[c]) {  // any part too large for its machine: the whole chromosome scores 1e16
+    const int item = ctx.item;
+    if (item < 0) break;
+    const MachDev md = ctx.md;
+    const int n = ctx.n;
+    BrkgaPlacement* lg = run.log ? run.log + ctx.seq : nullptr;
+    const uint16_t* seq = run.seq + ctx.seq;
+    const int N = ctx.N;
+    if (ctx.infeas) {  // any part too large for its machine: the whole chromosome scores 1e16
       if (lg)
-        for (int k = tid; k < p.N; k += kDecodeThreads) lg[k] = BrkgaPlacement{-1, -1, -1, -1, -1};
-      if (tid == 0) p.mk[item] = 0.0;
+        for (int k = tid; k < N; k += kDecodeThreads) lg[k] = BrkgaPlacement{-1, -1, -1, -1, -1};
+      if (tid == 0) run.mk[item] = 0.0;
+      __syncthreads();
       continue;
     }
     if (lg)
-      for (int k = n + tid; k < p.N; k += kDecodeThreads) lg[k] = BrkgaPlacement{-1, -1, -1, -1, -1};
+      for (int k = n + tid; k < N; k += kDecodeThreads) lg[k] = BrkgaPlacement{-1, -1, -1, -1, -1};
 
     int nb = 0;
     bool failed = false;
     for (int k = 0; k < n && !failed; ++k) {
-      const int gene = p.seq[(size_t)item * p.N + k];
-      const int t = p.gene_type[gene];
-      const double a = p.part_area[t];
+      const int gene = seq[k];
+      const int t = tb.gene_type[ctx.gbase + gene];
+      const double a = tb.part_area[t];
       int pb = -1;
       unsigned long long key = kKeyNone;
 
       // ---- first fit over the open plates (placement.py:56-64)
       for (int b = 0; b < nb; ++b) {
         if (bs[b].area + a > md.area) continue;  // placement.py:57-59
-        const uint32_t* grid = b < p.S ? smem + (size_t)b * p.slot_words
-                                       : p.pool + (size_t)bs[b].pool * p.slot_words;
-        const uint16_t* vac = reinterpret_cast<const uint16_t*>(grid + p.slot_vac_off);
-        key = search_plate(p, md, grid, vac, bs[b].enc, t, sh, c_tests, c_chunks, c_bytes);
+        const uint32_t* grid = b < run.S ? smem + (size_t)b * run.slot_words
+                                         : run.pool + (size_t)bs[b].pool * run.slot_words;
+        const uint16_t* vac = reinterpret_cast<const uint16_t*>(grid + run.slot_vac_off);
+        key = search_plate(tb, md, grid, vac, bs[b].enc, t, sh, c_tests, c_chunks, c_bytes);
         if (key != kKeyNone) {
           pb = b;
           break;
@@ -534,74 +630,79 @@ __global__ void __launch_bounds__(kDecodeThreads) decode_kernel(DecodeParams p) 
       int r, x, ty;
       if (pb < 0) {
         // ---- new plate, best rotation at column 0, bottom row L-1 (placement.py:66-83)
-        r = p.best_rot[t];
+        r = tb.best_rot[t];
         if (tid == 0) {
           s_fail = 0;
           s_pool = -1;
-          if (!p.newbin_ok[t * p.M + m]) {
+          if (!tb.newbin_ok[ctx.tmbase + (t - ctx.tbase) * ctx.M + ctx.m]) {
             s_fail = BRKGA_ERR_NEW_BIN_UNFIT;
-          } else if (nb >= p.S) {
-            const unsigned idx = atomicAdd(p.pool_ctr, 1u);
-            if ((long long)idx >= p.pool_bins) s_fail = BRKGA_ERR_CAPACITY;
+          } else if (nb >= run.S) {
+            const unsigned idx = atomicAdd(run.pool_ctr, 1u);
+            if ((long long)idx >= run.pool_bins) s_fail = BRKGA_ERR_CAPACITY;
             else s_pool = (int)idx;
           }
         }
         __syncthreads();
         if (s_fail) {
           if (tid == 0) {
-            raise_status(p.status, s_fail);
-            p.mk[item] = nan("");
+            raise_status(run.status, s_fail);
+            run.mk[item] = nan("");
           }
           failed = true;
           break;
         }
         pb = nb++;
-        uint32_t* grid = pb < p.S ? smem + (size_t)pb * p.slot_words : p.pool + (size_t)s_pool * p.slot_words;
-        open_plate(md, grid, reinterpret_cast<uint16_t*>(grid + p.slot_vac_off), &bs[pb], s_pool);
+        uint32_t* grid = pb < run.S ? smem + (size_t)pb * run.slot_words : run.pool + (size_t)s_pool * run.slot_words;
+        open_plate(md, grid, reinterpret_cast<uint16_t*>(grid + run.slot_vac_off), &bs[pb], s_pool);
         if (tid == 0) ++c_bins;
         x = 0;
-        ty = md.L - p.rot[t * 4 + r].h;
+        ty = md.L - tb.rot[t * 4 + r].h;
       } else {
         int y;
         decode_key(key, &r, &x, &y);
-        ty = y - p.rot[t * 4 + r].h + 1;
+        ty = y - tb.rot[t * 4 + r].h + 1;
       }
 
       // ---- insert (binClassNew.py:155-174)
-      uint32_t* grid = pb < p.S ? smem + (size_t)pb * p.slot_words : p.pool + (size_t)bs[pb].pool * p.slot_words;
-      place_part(p, md, grid, reinterpret_cast<uint16_t*>(grid + p.slot_vac_off), &bs[pb], t, m, r, x, ty, a);
-      if (tid == 0 && lg) lg[k] = BrkgaPlacement{gene, pb, x, ty + p.rot[t * 4 + r].h - 1, r};
+      uint32_t* grid = pb < run.S ? smem + (size_t)pb * run.slot_words : run.pool + (size_t)bs[pb].pool * run.slot_words;
+      const size_t tm = (size_t)ctx.tmbase + (size_t)ctx.m * ctx.T + (t - ctx.tbase);
+      place_part(tb, md, grid, reinterpret_cast<uint16_t*>(grid + run.slot_vac_off), &bs[pb], t, r, x, ty, a,
+                 tb.pt[tm], tb.pth[tm]);
+      if (tid == 0 && lg) lg[k] = BrkgaPlacement{gene, pb, x, ty + tb.rot[t * 4 + r].h - 1, r};
     }
     if (!failed && tid == 0) {  // placement.py:86-89
       double ms = 0.0;
       for (int b = 0; b < nb; ++b) ms += (bs[b].pt + bs[b].pth) + md.setup;
-      p.mk[item] = ms;
+      run.mk[item] = ms;
     }
     __syncthreads();
   }
   if (tid == 0) {
-    atomicAdd(&p.counters[0], c_tests);
-    atomicAdd(&p.counters[2], c_bins);
-    atomicAdd(&p.counters[3], c_bytes);
+    atomicAdd(&run.counters[0], c_tests);
+    atomicAdd(&run.counters[2], c_bins);
+    atomicAdd(&run.counters[3], c_bytes);
   }
-  if (lane == 0) atomicAdd(&p.counters[1], c_chunks);
+  if (lane == 0) atomicAdd(&run.counters[1], c_chunks);
 }
 
-__global__ void reduce_kernel(int P, int M, const int32_t* infeas, const double* mk, double* out) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= P) return;
-  if (infeas[c]) {
-    out[c] = 1e16;  // placement.py:9,151-153
+__global__ void reduce_kernel(const __grid_constant__ Tables tb, const __grid_constant__ Run run) {
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= run.n_rows) return;
+  if (run.infeas[row]) {
+    run.out[row] = 1e16;  // placement.py:9,151-153
     return;
   }
+  const int k = inst_of_row(run, row);
+  const int M = tb.inst[k].M;
+  const double* mk = run.mk + run.r[k].item0 + (long long)(row - run.r[k].crow0) * M;
   double worst = 0.0;
   bool bad = false;
   for (int m = 0; m < M; ++m) {
-    const double v = mk[(size_t)c * M + m];
+    const double v = mk[m];
     if (v != v) bad = true;
     else if (v > worst) worst = v;  // placement.py:154-156
   }
-  out[c] = bad ? nan("") : worst;
+  run.out[row] = bad ? nan("") : worst;
 }
 
 // Greedy initial solution (BRKGA_alg3.py:445-603 with binClassInitialSol.py):
@@ -611,8 +712,14 @@ __global__ void reduce_kernel(int P, int M, const int32_t* infeas, const double*
 // plate wins within a machine): a new plate on some machine (best rotation at
 // column 0, bottom row L-1) or any existing plate of the machine that can take
 // it (every plate is tested, no area filter).  Plates live in the global pool.
-struct GreedyParams {
-  DecodeParams p;  // tables, pool, slot geometry (S = 0: every plate in the pool)
+// Single-instance problems only, so every table base is 0.
+struct GreedyArgs {
+  int N, M, T;
+  int32_t* status;
+  unsigned long long* counters;
+  BinScal* binscal;
+  uint32_t* pool;
+  int slot_words, slot_vac_off;
   const int32_t* order;
   int n;
   int32_t* out_machine;  // [n]
@@ -622,31 +729,31 @@ struct GreedyParams {
   double* machine_makespan;  // [M]
 };
 
-__global__ void __launch_bounds__(kDecodeThreads) greedy_kernel(GreedyParams g) {
+__global__ void __launch_bounds__(kDecodeThreads) greedy_kernel(const __grid_constant__ Tables tb,
+                                                                const __grid_constant__ GreedyArgs g) {
   __shared__ SearchShared sh;
   __shared__ int s_fail;
-  const DecodeParams& p = g.p;
   const int tid = threadIdx.x;
-  BinScal* bs = p.binscal;
+  BinScal* bs = g.binscal;
   unsigned long long c_tests = 0, c_chunks = 0, c_bytes = 0;
   int nplates = 0;
   double cw = 0.0;  // current_worst_makespan
-  for (int m = tid; m < p.M; m += kDecodeThreads) g.machine_makespan[m] = 0.0;
+  for (int m = tid; m < g.M; m += kDecodeThreads) g.machine_makespan[m] = 0.0;
   __syncthreads();
   for (int k = 0; k < g.n; ++k) {
     const int gene = g.order[k];
-    const int t = p.gene_type[gene];
-    const double a = p.part_area[t];
+    const int t = tb.gene_type[gene];
+    const double a = tb.part_area[t];
     double best = INFINITY;
     int kind = -1, cm = -1, cb = -1;  // kind 0 = new plate, 1 = existing plate
     unsigned long long ckey = kKeyNone;
     double ccand = 0.0;
-    for (int m = 0; m < p.M; ++m) {
+    for (int m = 0; m < g.M; ++m) {
       bool placed_in_exist = false;
-      if (!p.fits_flag[t * p.M + m]) continue;  // BRKGA_alg3.py:465-470
-      const MachDev md = p.mach[m];
+      if (!tb.fits[t * g.M + m]) continue;  // BRKGA_alg3.py:465-470
+      const MachDev md = tb.mach[m];
       const double mm = g.machine_makespan[m];
-      const double ptm = p.pt[(size_t)m * p.T + t], pthm = p.pth[(size_t)m * p.T + t];
+      const double ptm = tb.pt[(size_t)m * g.T + t], pthm = tb.pth[(size_t)m * g.T + t];
       const double cand = ((mm + md.setup) + ptm) + pthm;  // :472
       const double nm = cw > cand ? cw : cand;
       if (nm <= best) {
@@ -657,8 +764,8 @@ __global__ void __launch_bounds__(kDecodeThreads) greedy_kernel(GreedyParams g) 
       }
       for (int b = 0; b < nplates; ++b) {
         if (g.plate_machine[b] != m) continue;
-        const uint32_t* grid = p.pool + (size_t)bs[b].pool * p.slot_words;
-        const unsigned long long key = search_plate(p, md, grid, reinterpret_cast<const uint16_t*>(grid + p.slot_vac_off),
+        const uint32_t* grid = g.pool + (size_t)bs[b].pool * g.slot_words;
+        const unsigned long long key = search_plate(tb, md, grid, reinterpret_cast<const uint16_t*>(grid + g.slot_vac_off),
                                                     bs[b].enc, t, sh, c_tests, c_chunks, c_bytes);
         if (key == kKeyNone) continue;
         const double bpth = bs[b].pth;
@@ -677,22 +784,22 @@ __global__ void __launch_bounds__(kDecodeThreads) greedy_kernel(GreedyParams g) 
       }
     }
     if (kind < 0) {  // fits no machine: the reference crashes here (bestBatch == [])
-      if (tid == 0) raise_status(p.status, BRKGA_ERR_BAD_INSTANCE);
+      if (tid == 0) raise_status(g.status, BRKGA_ERR_BAD_INSTANCE);
       return;
     }
-    const MachDev md = p.mach[cm];
+    const MachDev md = tb.mach[cm];
     int r, x, ty, b;
     if (kind == 0) {
-      r = p.best_rot[t];
-      if (tid == 0) s_fail = (!p.newbin_ok[t * p.M + cm] || nplates >= g.n) ? 1 : 0;
+      r = tb.best_rot[t];
+      if (tid == 0) s_fail = (!tb.newbin_ok[t * g.M + cm] || nplates >= g.n) ? 1 : 0;
       __syncthreads();
       if (s_fail) {
-        if (tid == 0) raise_status(p.status, BRKGA_ERR_NEW_BIN_UNFIT);
+        if (tid == 0) raise_status(g.status, BRKGA_ERR_NEW_BIN_UNFIT);
         return;
       }
       b = nplates++;
-      uint32_t* grid = p.pool + (size_t)b * p.slot_words;
-      open_plate(md, grid, reinterpret_cast<uint16_t*>(grid + p.slot_vac_off), &bs[b], b);
+      uint32_t* grid = g.pool + (size_t)b * g.slot_words;
+      open_plate(md, grid, reinterpret_cast<uint16_t*>(grid + g.slot_vac_off), &bs[b], b);
       if (tid == 0) {
         int idx = 0;
         for (int q = 0; q < b; ++q) idx += g.plate_machine[q] == cm;
@@ -700,26 +807,27 @@ __global__ void __launch_bounds__(kDecodeThreads) greedy_kernel(GreedyParams g) 
         g.plate_index[b] = idx;
       }
       x = 0;
-      ty = md.L - p.rot[t * 4 + r].h;
+      ty = md.L - tb.rot[t * 4 + r].h;
     } else {
       int y;
       decode_key(ckey, &r, &x, &y);
-      ty = y - p.rot[t * 4 + r].h + 1;
+      ty = y - tb.rot[t * 4 + r].h + 1;
       b = cb;
     }
-    uint32_t* grid = p.pool + (size_t)bs[b].pool * p.slot_words;
-    place_part(p, md, grid, reinterpret_cast<uint16_t*>(grid + p.slot_vac_off), &bs[b], t, cm, r, x, ty, a);
+    uint32_t* grid = g.pool + (size_t)bs[b].pool * g.slot_words;
+    place_part(tb, md, grid, reinterpret_cast<uint16_t*>(grid + g.slot_vac_off), &bs[b], t, r, x, ty, a,
+               tb.pt[(size_t)cm * g.T + t], tb.pth[(size_t)cm * g.T + t]);
     if (tid == 0) {
       g.out_machine[k] = cm;
-      g.out[k] = BrkgaPlacement{gene, g.plate_index[b], x, ty + p.rot[t * 4 + r].h - 1, r};
+      g.out[k] = BrkgaPlacement{gene, g.plate_index[b], x, ty + tb.rot[t * 4 + r].h - 1, r};
       g.machine_makespan[cm] = ccand;  // :541, :565
     }
     cw = cw > ccand ? cw : ccand;
     __syncthreads();
   }
   if (tid == 0) {
-    atomicAdd(&p.counters[0], c_tests);
-    atomicAdd(&p.counters[3], c_bytes);
+    atomicAdd(&g.counters[0], c_tests);
+    atomicAdd(&g.counters[3], c_bytes);
   }
 }
 
@@ -729,6 +837,11 @@ size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 struct Layout {
   size_t off_ctr, off_seq, off_cnt, off_inf, off_ord, off_mk, off_bins, off_pool, total;
+};
+
+// Sizes of one launch: chromosome rows, (chromosome, machine) items, part-order entries.
+struct LaunchCounts {
+  int64_t rows = 0, items = 0, seq = 0;
 };
 
 }  // namespace
@@ -741,13 +854,21 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[BRKGA_NOALLOC_S
 struct BrkgaProblem {
   int device = 0;
   void* noalloc_scratch = nullptr;  // device address of g_noalloc_scratch on `device`
-  int N = 0, M = 0, T = 0, mode = 0;
+  int K = 0;                        // instances
+  std::vector<InstDev> inst;
+  std::vector<int> s2;              // bitonic sort width per instance
+  int S2max = 1, Nmax = 0;
+  int N = 0, M = 0, T = 0, mode = 0;  // instance 0 (the single-instance entry points)
   int sm_count = 0;
+  int req_ctas = 0, req_plates = -1;  // requested launch shape (0 / -1 = automatic)
+  int ctas_per_sm = 0;
   int S = 0, slot_words = 0, slot_vac_off = 0;
   int n_slots = 0;
   size_t decode_smem = 0;
   std::vector<MachDev> mach;
   std::vector<void*> allocations;
+  Tables tb{};
+  InstDev* d_inst = nullptr;
   int32_t* d_gene_type = nullptr;
   double* d_thr = nullptr;
   MachDev* d_mach = nullptr;
@@ -781,31 +902,43 @@ struct BrkgaProblem {
 
 namespace {
 
-Layout layout_of(const BrkgaProblem* pb, int32_t P, int64_t pool_bins) {
+int counts_of(const BrkgaProblem* pb, const int32_t* pops, LaunchCounts* lc) {
+  LaunchCounts c;
+  for (int k = 0; k < pb->K; ++k) {
+    if (pops[k] < 0) return BRKGA_ERR_INVALID_ARGUMENT;
+    c.rows += pops[k];
+    c.items += (int64_t)pops[k] * pb->inst[k].M;
+    c.seq += (int64_t)pops[k] * pb->inst[k].M * pb->inst[k].N;
+  }
+  if (c.rows >= ((int64_t)1 << 31) || c.items >= ((int64_t)1 << 31)) return BRKGA_ERR_INVALID_ARGUMENT;
+  *lc = c;
+  return BRKGA_OK;
+}
+
+Layout layout_of(const BrkgaProblem* pb, const LaunchCounts& lc, int64_t pool_bins) {
   Layout l;
   size_t o = 0;
   l.off_ctr = o;
   o += 64;
   l.off_seq = o = align_up(o, 256);
-  o += (size_t)P * pb->M * pb->N * sizeof(uint16_t);
+  o += (size_t)lc.seq * sizeof(uint16_t);
   l.off_cnt = o = align_up(o, 256);
-  o += (size_t)P * pb->M * sizeof(int32_t);
+  o += (size_t)lc.items * sizeof(int32_t);
   l.off_inf = o = align_up(o, 256);
-  o += (size_t)P * sizeof(int32_t);
+  o += (size_t)lc.rows * sizeof(int32_t);
   l.off_ord = o = align_up(o, 256);
-  o += (size_t)P * pb->M * sizeof(int32_t);
+  o += (size_t)lc.items * sizeof(int32_t);
   l.off_mk = o = align_up(o, 256);
-  o += (size_t)P * pb->M * sizeof(double);
+  o += (size_t)lc.items * sizeof(double);
   l.off_bins = o = align_up(o, 256);
-  o += (size_t)pb->n_slots * std::max(pb->N, 1) * sizeof(BinScal);
+  o += (size_t)pb->n_slots * std::max(pb->Nmax, 1) * sizeof(BinScal);
   l.off_pool = o = align_up(o, 256);
   o += (size_t)pool_bins * pb->slot_words * sizeof(uint32_t);
   l.total = align_up(o, 256);
   return l;
 }
 
-int64_t default_pool_bins(const BrkgaProblem* pb, int32_t P) {
-  const int64_t items = (int64_t)P * pb->M;
+int64_t default_pool_bins(const BrkgaProblem* pb, int64_t items) {
   return std::max<int64_t>(256, items * (pb->S > 0 ? 2 : 4));
 }
 
@@ -833,7 +966,12 @@ class DeviceGuard {
   int prev_ = 0;
 };
 
-int configure(BrkgaProblem* pb) {
+// Shared-memory plate slots and resident CTAs per SM of the decode kernel.
+// ctas_req = 0 picks the shape automatically (aim at 8 resident items per
+// SM, fewer when one plate does not fit that share of shared memory; at most
+// 4 plates per item in shared memory); plates_req = -1 keeps as many plates
+// as fit (at most 4).  An explicit shape that cannot be resident is refused.
+int configure(BrkgaProblem* pb, int ctas_req, int plates_req) {
   cudaDeviceProp prop;
   if (cudaGetDeviceProperties(&prop, pb->device) != cudaSuccess) return BRKGA_ERR_CUDA;
   pb->sm_count = prop.multiProcessorCount;
@@ -842,42 +980,63 @@ int configure(BrkgaProblem* pb) {
     Lmax = std::max(Lmax, m.L);
     RSmax = std::max(RSmax, m.RS);
   }
-  pb->slot_vac_off = Lmax * RSmax;
-  pb->slot_words = (int)align_up((size_t)pb->slot_vac_off + (size_t)(Lmax + 1) / 2, 4);
-  const size_t slot_bytes = (size_t)pb->slot_words * 4;
+  const int slot_vac_off = Lmax * RSmax;
+  const int slot_words = (int)align_up((size_t)slot_vac_off + (size_t)(Lmax + 1) / 2, 4);
+  const size_t slot_bytes = (size_t)slot_words * 4;
   const size_t per_sm = prop.sharedMemPerMultiprocessor;
   const size_t per_block_max = prop.sharedMemPerBlockOptin;
   const size_t reserve = 1024 + 256;  // per-block system reservation + static shared variables
-  // Aim at 8 resident items per SM (32 warps); fewer when one plate does not fit that share.
-  int S = 0, ctas = 8;
-  for (; ctas >= 1; --ctas) {
-    const size_t share = per_sm / ctas;
-    if (share <= reserve) continue;
-    S = (int)std::min<size_t>((share - reserve) / slot_bytes, (per_block_max - 256) / slot_bytes);
-    if (S >= 1) break;
-  }
-  if (S < 1) {  // plates larger than shared memory: all of them in the global pool
-    S = 0;
-    ctas = 8;
-  }
-  S = std::min(S, 4);
-  pb->S = S;
-  pb->decode_smem = (size_t)S * slot_bytes;
-  if (cudaFuncSetAttribute(decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)std::max<size_t>(pb->decode_smem, 1)) != cudaSuccess)
+  const int max_fit = (int)std::min<size_t>(kMaxSmemPlates, (per_block_max - 256) / slot_bytes);
+  if (cudaFuncSetAttribute(decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(per_block_max - 256)) !=
+      cudaSuccess)
     return BRKGA_ERR_CUDA;
-  if (cudaFuncSetAttribute(assign_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           kMaxGenes * 8) != cudaSuccess)
+  if (cudaFuncSetAttribute(assign_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxGenes * 8) !=
+      cudaSuccess)
     return BRKGA_ERR_CUDA;
   if (cudaFuncSetAttribute(order_items_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (kMaxGenes + 1) * (int)sizeof(int)) != cudaSuccess)
     return BRKGA_ERR_CUDA;
+  auto fit_for = [&](int ctas) {  // plates per item that fit when `ctas` CTAs share an SM
+    const size_t share = per_sm / ctas;
+    if (share <= reserve) return 0;
+    return (int)std::min<size_t>((share - reserve) / slot_bytes, (size_t)max_fit);
+  };
+  int S = 0, ctas = 0;
+  if (ctas_req == 0) {
+    if (plates_req >= 0) {
+      S = plates_req;
+      ctas = 8;
+      while (ctas > 1 && fit_for(ctas) < S) --ctas;
+    } else {
+      for (ctas = 8; ctas >= 1; --ctas) {
+        S = fit_for(ctas);
+        if (S >= 1) break;
+      }
+      if (S < 1) {  // plates larger than shared memory: all of them in the global pool
+        S = 0;
+        ctas = 8;
+      }
+      S = std::min(S, 4);
+    }
+  } else {
+    ctas = ctas_req;
+    S = plates_req >= 0 ? plates_req : std::min(fit_for(ctas), 4);
+  }
+  if (S > max_fit) return BRKGA_ERR_INVALID_ARGUMENT;
+  const size_t smem = (size_t)S * slot_bytes;
   int occ = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, decode_kernel, kDecodeThreads, pb->decode_smem) !=
-      cudaSuccess)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, decode_kernel, kDecodeThreads, smem) != cudaSuccess)
     return BRKGA_ERR_CUDA;
-  occ = std::max(1, std::min(occ, ctas));
-  pb->n_slots = pb->sm_count * occ;
+  if (occ < 1 || (ctas_req > 0 && occ < ctas_req) || (ctas_req == 0 && plates_req >= 0 && fit_for(ctas) < S))
+    return BRKGA_ERR_INVALID_ARGUMENT;
+  pb->slot_vac_off = slot_vac_off;
+  pb->slot_words = slot_words;
+  pb->S = S;
+  pb->decode_smem = smem;
+  pb->ctas_per_sm = std::max(1, std::min(occ, ctas));
+  pb->n_slots = pb->sm_count * pb->ctas_per_sm;
+  pb->req_ctas = ctas_req;
+  pb->req_plates = plates_req;
   return BRKGA_OK;
 }
 
@@ -923,17 +1082,180 @@ int validate(const BrkgaProblemDesc* d) {
   return BRKGA_OK;
 }
 
+// Host copies of the merged tables while a problem is built.
+struct Merged {
+  std::vector<InstDev> inst;
+  std::vector<int32_t> gene_type, nrot, best;
+  std::vector<double> thr, pt, pth, area, bin_area;
+  std::vector<RotDev> rot;
+  std::vector<uint16_t> dens;
+  std::vector<int32_t> run_off;
+  std::vector<uint32_t> runs, maskbits;
+  std::vector<uint8_t> fits, newbin_ok;
+  std::vector<MachDev> mach;
+};
+
+// Append one instance: derived part tables (densities, runs of ones,
+// bit-packed rows) with absolute indices, machines, times, flags.
+void merge_instance(const BrkgaProblemDesc* d, Merged& g) {
+  const int N = d->n_genes, M = d->n_machines, T = d->n_types;
+  InstDev id;
+  id.N = N;
+  id.M = M;
+  id.T = T;
+  id.mode = d->threshold_mode;
+  id.gbase = (int)g.gene_type.size();
+  id.tbase = (int)g.area.size();
+  id.mbase = (int)g.mach.size();
+  id.thrbase = (int)g.thr.size();
+  id.tmbase = (int)g.pt.size();
+  for (int t = 0; t < T; ++t) {
+    for (int r = 0; r < 4; ++r) {
+      RotDev rd{};
+      if (r < d->part_nrot[t]) {
+        const int k = t * 4 + r, h = d->rot_h[k], w = d->rot_w[k];
+        const uint8_t* mk = d->masks + d->rot_mask_offset[k];
+        rd.h = h;
+        rd.w = w;
+        rd.mw = (w + 31) / 32;
+        rd.dens_row = (int)g.dens.size();
+        rd.run_row = (int)g.run_off.size();
+        rd.mask_base = (int)g.maskbits.size();
+        rd.imax = 0;
+        rd.dmax = 0;
+        for (int i = 0; i < h; ++i) {
+          g.run_off.push_back((int32_t)g.runs.size());
+          int best = 0, j = 0;
+          while (j < w) {
+            if (mk[(size_t)i * w + j]) {
+              const int s = j;
+              while (j < w && mk[(size_t)i * w + j]) ++j;
+              g.runs.push_back((uint32_t)s | ((uint32_t)(j - s) << 16));
+              best = std::max(best, j - s);
+            } else {
+              ++j;
+            }
+          }
+          g.dens.push_back((uint16_t)best);
+          if (best > rd.dmax) {
+            rd.dmax = best;
+            rd.imax = i;
+          }
+          for (int wd = 0; wd < rd.mw; ++wd) {
+            uint32_t v = 0;
+            for (int bit = 0; bit < 32 && wd * 32 + bit < w; ++bit)
+              if (mk[(size_t)i * w + wd * 32 + bit]) v |= 1u << bit;
+            g.maskbits.push_back(v);
+          }
+        }
+        g.run_off.push_back((int32_t)g.runs.size());
+      }
+      g.rot.push_back(rd);
+    }
+    g.area.push_back(d->part_area[t]);
+    g.nrot.push_back(d->part_nrot[t]);
+    g.best.push_back(d->part_best_rot[t]);
+  }
+  std::vector<uint8_t> fits((size_t)T * M), newbin_ok((size_t)T * M);
+  for (int m = 0; m < M; ++m) {
+    MachDev md;
+    md.L = d->bin_length[m];
+    md.W = d->bin_width[m];
+    md.NW = (md.W + 31) / 32;
+    md.RS = md.NW + 2;
+    md.area = d->bin_area[m];
+    md.setup = d->setup_time[m];
+    g.mach.push_back(md);
+    g.bin_area.push_back(d->bin_area[m]);
+    for (int t = 0; t < T; ++t) {
+      const int h0 = d->rot_h[t * 4], w0 = d->rot_w[t * 4];
+      fits[(size_t)t * M + m] = !((h0 > md.L || w0 > md.W) && (w0 > md.L || h0 > md.W));
+      const int rb = d->part_best_rot[t];
+      newbin_ok[(size_t)t * M + m] = d->rot_h[t * 4 + rb] <= md.L && d->rot_w[t * 4 + rb] <= md.W;
+    }
+  }
+  g.fits.insert(g.fits.end(), fits.begin(), fits.end());
+  g.newbin_ok.insert(g.newbin_ok.end(), newbin_ok.begin(), newbin_ok.end());
+  for (int m = 0; m + 1 < M; ++m)
+    g.thr.push_back(d->threshold_mode == BRKGA_THRESH_F32 ? (double)(float)d->thresholds[m] : d->thresholds[m]);
+  for (int j = 0; j < N; ++j) g.gene_type.push_back(id.tbase + d->gene_type[j]);
+  g.pt.insert(g.pt.end(), d->proc_time, d->proc_time + (size_t)M * T);
+  g.pth.insert(g.pth.end(), d->proc_time_height, d->proc_time_height + (size_t)M * T);
+  g.inst.push_back(id);
+}
+
+int fill_run(const BrkgaProblem* pb, const int32_t* pops, const LaunchCounts& lc, const Layout& l, char* ws,
+             const float* d_chrom, double* d_out, BrkgaPlacement* d_log, int32_t* d_status, int64_t pool_bins,
+             Run* run) {
+  std::memset(run, 0, sizeof(Run));
+  run->K = pb->K;
+  run->n_rows = (int)lc.rows;
+  run->n_items = (int)lc.items;
+  run->Nmax = pb->Nmax;
+  run->chrom = d_chrom;
+  run->out = d_out;
+  run->seq = reinterpret_cast<uint16_t*>(ws + l.off_seq);
+  run->cnt = reinterpret_cast<int32_t*>(ws + l.off_cnt);
+  run->infeas = reinterpret_cast<int32_t*>(ws + l.off_inf);
+  run->order = reinterpret_cast<int32_t*>(ws + l.off_ord);
+  run->mk = reinterpret_cast<double*>(ws + l.off_mk);
+  run->log = d_log;
+  run->status = d_status;
+  unsigned int* ctr = reinterpret_cast<unsigned int*>(ws + l.off_ctr);
+  run->item_ctr = ctr;
+  run->pool_ctr = ctr + 1;
+  run->counters = reinterpret_cast<unsigned long long*>(ws + l.off_ctr + 8);
+  run->binscal = reinterpret_cast<BinScal*>(ws + l.off_bins);
+  run->pool = reinterpret_cast<uint32_t*>(ws + l.off_pool);
+  run->pool_bins = pool_bins;
+  run->S = pb->S;
+  run->slot_words = pb->slot_words;
+  run->slot_vac_off = pb->slot_vac_off;
+  int64_t row = 0, item = 0, seq = 0, chrom = 0;
+  for (int k = 0; k < pb->K; ++k) {
+    const InstDev& id = pb->inst[k];
+    InstRun& r = run->r[k];
+    r.P = pops[k];
+    r.crow0 = (int)row;
+    r.item0 = (int)item;
+    r.S2 = pb->s2[k];
+    r.chrom_off = chrom;
+    r.seq0 = seq;
+    row += pops[k];
+    item += (int64_t)pops[k] * id.M;
+    seq += (int64_t)pops[k] * id.M * id.N;
+    chrom += (int64_t)pops[k] * 2 * id.N;
+  }
+  return BRKGA_OK;
+}
+
+int launch(const BrkgaProblem* pb, int stage, const Run& run, cudaStream_t s) {
+  if (run.n_rows == 0) return BRKGA_OK;
+  if (stage == 0 || stage == 1) {
+    const int at = std::min(1024, std::max(64, pb->S2max / 2));
+    assign_sort_kernel<<<run.n_rows, at, (size_t)pb->S2max * 8, s>>>(pb->tb, run);
+    order_items_kernel<<<1, 1024, (size_t)(pb->Nmax + 1) * sizeof(int), s>>>(pb->tb, run);
+  }
+  if (stage == 0 || stage == 2) {
+    const int grid = (int)std::min<int64_t>(pb->n_slots, run.n_items);
+    decode_kernel<<<grid, kDecodeThreads, pb->decode_smem, s>>>(pb->tb, run);
+  }
+  if (stage == 0 || stage == 3) reduce_kernel<<<(run.n_rows + 255) / 256, 256, 0, s>>>(pb->tb, run);
+  return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
+}
+
 }  // namespace
 
 extern "C" {
 
 int brkga_abi_version(void) { return BRKGA_ABI_VERSION; }
 
-// Device tables for the surrogate (same library, not part of the public ABI).
+// Device tables for the surrogate (same library, not part of the public ABI;
+// single-instance problems, whose table bases are all 0).
 __attribute__((visibility("hidden"))) int brkga_internal_problem_tables(
     const BrkgaProblem* pb, int* N, int* M, int* T, int* mode, const double** thr, const int32_t** gene_type,
     const double** part_area, const double** pt, const double** pth, const double** bin_area) {
-  if (!pb) return BRKGA_ERR_INVALID_ARGUMENT;
+  if (!pb || pb->K != 1) return BRKGA_ERR_INVALID_ARGUMENT;
   *N = pb->N;
   *M = pb->M;
   *T = pb->T;
@@ -976,112 +1298,69 @@ void brkga_problem_destroy(BrkgaProblem* pb) {
   delete pb;
 }
 
-int brkga_problem_create(const BrkgaProblemDesc* d, BrkgaProblem** out) {
+int brkga_problem_create_multi(const BrkgaProblemDesc* descs, int32_t K, BrkgaProblem** out) {
   if (!out) return BRKGA_ERR_INVALID_ARGUMENT;
   *out = nullptr;
-  int st = validate(d);
-  if (st) return st;
+  if (!descs || K < 1 || K > kMaxInst) return BRKGA_ERR_INVALID_ARGUMENT;
+  for (int k = 0; k < K; ++k) {
+    const int st = validate(&descs[k]);
+    if (st) return st;
+  }
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
     cudaGetLastError();
     return BRKGA_ERR_NO_DEVICE;
   }
+  Merged g;
+  for (int k = 0; k < K; ++k) merge_instance(&descs[k], g);
+  if (g.maskbits.size() >= ((size_t)1 << 31) || g.runs.size() >= ((size_t)1 << 31)) return BRKGA_ERR_BAD_INSTANCE;
   BrkgaProblem* pb = new BrkgaProblem();
   cudaGetDevice(&pb->device);
-  pb->N = d->n_genes;
-  pb->M = d->n_machines;
-  pb->T = d->n_types;
-  pb->mode = d->threshold_mode;
-  const int N = pb->N, M = pb->M, T = pb->T;
-
-  // derived part tables: densities, runs of ones, bit-packed rows
-  std::vector<RotDev> rot((size_t)T * 4);
-  std::vector<uint16_t> dens;
-  std::vector<int32_t> run_off;
-  std::vector<uint32_t> runs, maskbits;
-  for (int t = 0; t < T; ++t) {
-    for (int r = 0; r < 4; ++r) {
-      RotDev rd{};
-      if (r < d->part_nrot[t]) {
-        const int k = t * 4 + r, h = d->rot_h[k], w = d->rot_w[k];
-        const uint8_t* mk = d->masks + d->rot_mask_offset[k];
-        rd.h = h;
-        rd.w = w;
-        rd.mw = (w + 31) / 32;
-        rd.dens_row = (int)dens.size();
-        rd.run_row = (int)run_off.size();
-        rd.mask_base = (int)maskbits.size();
-        rd.imax = 0;
-        rd.dmax = 0;
-        for (int i = 0; i < h; ++i) {
-          run_off.push_back((int32_t)runs.size());
-          int best = 0, j = 0;
-          while (j < w) {
-            if (mk[(size_t)i * w + j]) {
-              const int s = j;
-              while (j < w && mk[(size_t)i * w + j]) ++j;
-              runs.push_back((uint32_t)s | ((uint32_t)(j - s) << 16));
-              best = std::max(best, j - s);
-            } else {
-              ++j;
-            }
-          }
-          dens.push_back((uint16_t)best);
-          if (best > rd.dmax) {
-            rd.dmax = best;
-            rd.imax = i;
-          }
-          for (int wd = 0; wd < rd.mw; ++wd) {
-            uint32_t v = 0;
-            for (int bit = 0; bit < 32 && wd * 32 + bit < w; ++bit)
-              if (mk[(size_t)i * w + wd * 32 + bit]) v |= 1u << bit;
-            maskbits.push_back(v);
-          }
-        }
-        run_off.push_back((int32_t)runs.size());
-      }
-      rot[(size_t)t * 4 + r] = rd;
-    }
+  pb->K = K;
+  pb->inst = g.inst;
+  pb->mach = g.mach;
+  for (const InstDev& id : g.inst) {
+    int s2 = 1;
+    while (s2 < id.N) s2 <<= 1;
+    pb->s2.push_back(s2);
+    pb->S2max = std::max(pb->S2max, s2);
+    pb->Nmax = std::max(pb->Nmax, id.N);
   }
-  pb->mach.resize(M);
-  std::vector<uint8_t> fits((size_t)T * M), newbin_ok((size_t)T * M);
-  for (int m = 0; m < M; ++m) {
-    MachDev& md = pb->mach[m];
-    md.L = d->bin_length[m];
-    md.W = d->bin_width[m];
-    md.NW = (md.W + 31) / 32;
-    md.RS = md.NW + 2;
-    md.area = d->bin_area[m];
-    md.setup = d->setup_time[m];
-    for (int t = 0; t < T; ++t) {
-      const int h0 = d->rot_h[t * 4], w0 = d->rot_w[t * 4];
-      fits[(size_t)t * M + m] = !((h0 > md.L || w0 > md.W) && (w0 > md.L || h0 > md.W));
-      const int rb = d->part_best_rot[t];
-      newbin_ok[(size_t)t * M + m] = d->rot_h[t * 4 + rb] <= md.L && d->rot_w[t * 4 + rb] <= md.W;
-    }
-  }
-  std::vector<double> thr(std::max(1, M - 1), 0.0);
-  for (int m = 0; m + 1 < M; ++m)
-    thr[m] = d->threshold_mode == BRKGA_THRESH_F32 ? (double)(float)d->thresholds[m] : d->thresholds[m];
-  std::vector<int32_t> gene_type(d->gene_type, d->gene_type + N);
-  std::vector<double> pt(d->proc_time, d->proc_time + (size_t)M * T);
-  std::vector<double> pth(d->proc_time_height, d->proc_time_height + (size_t)M * T);
-  std::vector<double> area(d->part_area, d->part_area + T);
-  std::vector<int32_t> nrot(d->part_nrot, d->part_nrot + T), best(d->part_best_rot, d->part_best_rot + T);
+  pb->N = g.inst[0].N;
+  pb->M = g.inst[0].M;
+  pb->T = g.inst[0].T;
+  pb->mode = g.inst[0].mode;
 
-  if ((st = upload(pb, &pb->d_gene_type, gene_type)) || (st = upload(pb, &pb->d_thr, thr)) ||
-      (st = upload(pb, &pb->d_mach, pb->mach)) || (st = upload(pb, &pb->d_pt, pt)) ||
-      (st = upload(pb, &pb->d_pth, pth)) || (st = upload(pb, &pb->d_area, area)) ||
-      (st = upload(pb, &pb->d_nrot, nrot)) || (st = upload(pb, &pb->d_best, best)) ||
-      (st = upload(pb, &pb->d_rot, rot)) || (st = upload(pb, &pb->d_dens, dens)) ||
-      (st = upload(pb, &pb->d_run_off, run_off)) || (st = upload(pb, &pb->d_runs, runs)) ||
-      (st = upload(pb, &pb->d_maskbits, maskbits)) || (st = upload(pb, &pb->d_fits, fits)) ||
-      (st = upload(pb, &pb->d_newbin_ok, newbin_ok)) ||
-      (st = upload(pb, &pb->d_bin_area, std::vector<double>(d->bin_area, d->bin_area + M))) ||
-      (st = configure(pb))) {
+  int st;
+  if ((st = upload(pb, &pb->d_inst, g.inst)) || (st = upload(pb, &pb->d_gene_type, g.gene_type)) ||
+      (st = upload(pb, &pb->d_thr, g.thr)) || (st = upload(pb, &pb->d_mach, g.mach)) ||
+      (st = upload(pb, &pb->d_pt, g.pt)) || (st = upload(pb, &pb->d_pth, g.pth)) ||
+      (st = upload(pb, &pb->d_area, g.area)) || (st = upload(pb, &pb->d_nrot, g.nrot)) ||
+      (st = upload(pb, &pb->d_best, g.best)) || (st = upload(pb, &pb->d_rot, g.rot)) ||
+      (st = upload(pb, &pb->d_dens, g.dens)) || (st = upload(pb, &pb->d_run_off, g.run_off)) ||
+      (st = upload(pb, &pb->d_runs, g.runs)) || (st = upload(pb, &pb->d_maskbits, g.maskbits)) ||
+      (st = upload(pb, &pb->d_fits, g.fits)) || (st = upload(pb, &pb->d_newbin_ok, g.newbin_ok)) ||
+      (st = upload(pb, &pb->d_bin_area, g.bin_area)) || (st = configure(pb, 0, -1))) {
     brkga_problem_destroy(pb);
     return st;
   }
+  Tables& tb = pb->tb;
+  tb.inst = pb->d_inst;
+  tb.gene_type = pb->d_gene_type;
+  tb.thr = pb->d_thr;
+  tb.mach = pb->d_mach;
+  tb.pt = pb->d_pt;
+  tb.pth = pb->d_pth;
+  tb.part_area = pb->d_area;
+  tb.nrot = pb->d_nrot;
+  tb.best_rot = pb->d_best;
+  tb.rot = pb->d_rot;
+  tb.dens = pb->d_dens;
+  tb.run_off = pb->d_run_off;
+  tb.runs = pb->d_runs;
+  tb.maskbits = pb->d_maskbits;
+  tb.newbin_ok = pb->d_newbin_ok;
+  tb.fits = pb->d_fits;
   if (cudaGetSymbolAddress(&pb->noalloc_scratch, g_noalloc_scratch) != cudaSuccess) {
     brkga_problem_destroy(pb);
     return BRKGA_ERR_CUDA;
@@ -1090,94 +1369,84 @@ int brkga_problem_create(const BrkgaProblemDesc* d, BrkgaProblem** out) {
   return BRKGA_OK;
 }
 
-int brkga_workspace_bytes(const BrkgaProblem* pb, int32_t P, int64_t pool_bins, size_t* bytes) {
-  if (!pb || !bytes || P < 0 || pool_bins < 0) return BRKGA_ERR_INVALID_ARGUMENT;
-  if (pool_bins == 0) pool_bins = default_pool_bins(pb, P);
-  *bytes = layout_of(pb, P, pool_bins).total;
+int brkga_problem_create(const BrkgaProblemDesc* d, BrkgaProblem** out) {
+  if (!out) return BRKGA_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (!d) return BRKGA_ERR_INVALID_ARGUMENT;
+  return brkga_problem_create_multi(d, 1, out);
+}
+
+int brkga_problem_instances(const BrkgaProblem* pb, int32_t* K) {
+  if (!pb || !K) return BRKGA_ERR_INVALID_ARGUMENT;
+  *K = pb->K;
   return BRKGA_OK;
+}
+
+int brkga_set_launch_config(BrkgaProblem* pb, int32_t ctas_per_sm, int32_t smem_plates) {
+  if (!pb || ctas_per_sm < 0 || ctas_per_sm > kMaxCtasPerSm || smem_plates < -1 || smem_plates > kMaxSmemPlates)
+    return BRKGA_ERR_INVALID_ARGUMENT;
+  DeviceGuard g(pb->device);
+  const int old_ctas = pb->req_ctas, old_plates = pb->req_plates;
+  const int st = configure(pb, ctas_per_sm, smem_plates);
+  if (st) configure(pb, old_ctas, old_plates);
+  return st;
+}
+
+int brkga_get_launch_config(const BrkgaProblem* pb, int32_t* ctas_per_sm, int32_t* smem_plates,
+                            int32_t* resident_ctas) {
+  if (!pb) return BRKGA_ERR_INVALID_ARGUMENT;
+  if (ctas_per_sm) *ctas_per_sm = pb->ctas_per_sm;
+  if (smem_plates) *smem_plates = pb->S;
+  if (resident_ctas) *resident_ctas = pb->n_slots;
+  return BRKGA_OK;
+}
+
+int brkga_workspace_bytes_multi(const BrkgaProblem* pb, const int32_t* pops, int64_t pool_bins, size_t* bytes) {
+  if (!pb || !pops || !bytes || pool_bins < 0) return BRKGA_ERR_INVALID_ARGUMENT;
+  LaunchCounts lc;
+  const int st = counts_of(pb, pops, &lc);
+  if (st) return st;
+  if (pool_bins == 0) pool_bins = default_pool_bins(pb, lc.items);
+  *bytes = layout_of(pb, lc, pool_bins).total;
+  return BRKGA_OK;
+}
+
+int brkga_workspace_bytes(const BrkgaProblem* pb, int32_t P, int64_t pool_bins, size_t* bytes) {
+  if (!pb || pb->K != 1) return BRKGA_ERR_INVALID_ARGUMENT;
+  return brkga_workspace_bytes_multi(pb, &P, pool_bins, bytes);
+}
+
+int brkga_decode_multi_stage(int32_t stage, const BrkgaProblem* pb, const float* d_chrom, const int32_t* pops,
+                             double* d_makespan, BrkgaPlacement* d_log, int32_t* d_status, void* d_ws,
+                             size_t ws_bytes, int64_t pool_bins, void* stream) {
+  if (!pb || !pops || pool_bins < 0 || stage < 0 || stage > 3) return BRKGA_ERR_INVALID_ARGUMENT;
+  LaunchCounts lc;
+  int st = counts_of(pb, pops, &lc);
+  if (st) return st;
+  if (lc.rows == 0) return BRKGA_OK;
+  if (!d_chrom || !d_makespan || !d_status || !d_ws) return BRKGA_ERR_INVALID_ARGUMENT;
+  if (pool_bins == 0) pool_bins = default_pool_bins(pb, lc.items);
+  const Layout l = layout_of(pb, lc, pool_bins);
+  if (ws_bytes < l.total) return BRKGA_ERR_WORKSPACE;
+  DeviceGuard g(pb->device);
+  Run run;
+  fill_run(pb, pops, lc, l, static_cast<char*>(d_ws), d_chrom, d_makespan, d_log, d_status, pool_bins, &run);
+  return launch(pb, stage, run, static_cast<cudaStream_t>(stream));
+}
+
+int brkga_decode_multi(const BrkgaProblem* pb, const float* d_chrom, const int32_t* pops, double* d_makespan,
+                       BrkgaPlacement* d_log, int32_t* d_status, void* d_ws, size_t ws_bytes, int64_t pool_bins,
+                       void* stream) {
+  return brkga_decode_multi_stage(0, pb, d_chrom, pops, d_makespan, d_log, d_status, d_ws, ws_bytes, pool_bins,
+                                  stream);
 }
 
 int brkga_decode_stage(int32_t stage, const BrkgaProblem* pb, const float* d_chrom, int32_t P,
                        double* d_makespan, BrkgaPlacement* d_log, int32_t* d_status, void* d_ws,
                        size_t ws_bytes, int64_t pool_bins, void* stream) {
-  if (!pb || P < 0 || pool_bins < 0 || stage < 0 || stage > 3) return BRKGA_ERR_INVALID_ARGUMENT;
-  if (P == 0) return BRKGA_OK;
-  if (!d_chrom || !d_makespan || !d_status || !d_ws) return BRKGA_ERR_INVALID_ARGUMENT;
-  if ((int64_t)P * pb->M >= (int64_t)1 << 31) return BRKGA_ERR_INVALID_ARGUMENT;
-  if (pool_bins == 0) pool_bins = default_pool_bins(pb, P);
-  const Layout l = layout_of(pb, P, pool_bins);
-  if (ws_bytes < l.total) return BRKGA_ERR_WORKSPACE;
-  DeviceGuard g(pb->device);
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
-  char* ws = static_cast<char*>(d_ws);
-  unsigned int* ctr = reinterpret_cast<unsigned int*>(ws + l.off_ctr);
-  unsigned long long* counters = reinterpret_cast<unsigned long long*>(ws + l.off_ctr + 8);
-
-  AssignParams ap;
-  ap.chrom = d_chrom;
-  ap.thr = pb->d_thr;
-  ap.gene_type = pb->d_gene_type;
-  ap.fits = pb->d_fits;
-  ap.N = pb->N;
-  ap.M = pb->M;
-  ap.mode = pb->mode;
-  int S2 = 1;
-  while (S2 < pb->N) S2 <<= 1;
-  ap.S2 = S2;
-  ap.seq = reinterpret_cast<uint16_t*>(ws + l.off_seq);
-  ap.cnt = reinterpret_cast<int32_t*>(ws + l.off_cnt);
-  ap.infeas = reinterpret_cast<int32_t*>(ws + l.off_inf);
-  ap.status = d_status;
-  ap.item_ctr = ctr;
-  ap.pool_ctr = ctr + 1;
-  ap.counters = counters;
-  const int at = std::min(1024, std::max(64, S2 / 2));
-  int32_t* order = reinterpret_cast<int32_t*>(ws + l.off_ord);
-  if (stage == 0 || stage == 1) {
-    assign_sort_kernel<<<P, at, (size_t)S2 * 8, s>>>(ap);
-    order_items_kernel<<<1, 1024, (size_t)(pb->N + 1) * sizeof(int), s>>>(P * pb->M, pb->M, pb->N, ap.cnt,
-                                                                          ap.infeas, order);
-  }
-
-  DecodeParams dp;
-  dp.gene_type = pb->d_gene_type;
-  dp.mach = pb->d_mach;
-  dp.pt = pb->d_pt;
-  dp.pth = pb->d_pth;
-  dp.part_area = pb->d_area;
-  dp.nrot = pb->d_nrot;
-  dp.best_rot = pb->d_best;
-  dp.rot = pb->d_rot;
-  dp.dens = pb->d_dens;
-  dp.run_off = pb->d_run_off;
-  dp.runs = pb->d_runs;
-  dp.maskbits = pb->d_maskbits;
-  dp.newbin_ok = pb->d_newbin_ok;
-  dp.fits_flag = pb->d_fits;
-  dp.N = pb->N;
-  dp.M = pb->M;
-  dp.T = pb->T;
-  dp.P = P;
-  dp.seq = ap.seq;
-  dp.cnt = ap.cnt;
-  dp.infeas = ap.infeas;
-  dp.order = order;
-  dp.mk = reinterpret_cast<double*>(ws + l.off_mk);
-  dp.log = d_log;
-  dp.status = d_status;
-  dp.item_ctr = ctr;
-  dp.pool_ctr = ctr + 1;
-  dp.counters = counters;
-  dp.binscal = reinterpret_cast<BinScal*>(ws + l.off_bins);
-  dp.pool = reinterpret_cast<uint32_t*>(ws + l.off_pool);
-  dp.pool_bins = pool_bins;
-  dp.S = pb->S;
-  dp.slot_words = pb->slot_words;
-  dp.slot_vac_off = pb->slot_vac_off;
-  const int grid = (int)std::min<int64_t>(pb->n_slots, (int64_t)P * pb->M);
-  if (stage == 0 || stage == 2) decode_kernel<<<grid, kDecodeThreads, pb->decode_smem, s>>>(dp);
-  if (stage == 0 || stage == 3) reduce_kernel<<<(P + 255) / 256, 256, 0, s>>>(P, pb->M, ap.infeas, dp.mk, d_makespan);
-  return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
+  if (!pb || pb->K != 1 || P < 0) return BRKGA_ERR_INVALID_ARGUMENT;
+  return brkga_decode_multi_stage(stage, pb, d_chrom, &P, d_makespan, d_log, d_status, d_ws, ws_bytes, pool_bins,
+                                  stream);
 }
 
 int brkga_decode(const BrkgaProblem* pb, const float* d_chrom, int32_t P, double* d_makespan,
@@ -1191,14 +1460,16 @@ int brkga_decode(const BrkgaProblem* pb, const float* d_chrom, int32_t P, double
 // whatever that array has left after the per-population tables.
 int brkga_decode_noalloc(const BrkgaProblem* pb, const float* d_chrom, int32_t P, double* d_makespan,
                          BrkgaPlacement* d_log, int32_t* d_status, void* stream) {
-  if (!pb || P < 0) return BRKGA_ERR_INVALID_ARGUMENT;
+  if (!pb || pb->K != 1 || P < 0) return BRKGA_ERR_INVALID_ARGUMENT;
   if (P == 0) return BRKGA_OK;
   if (!pb->noalloc_scratch) return BRKGA_ERR_INVALID_ARGUMENT;
   const size_t cap = (size_t)BRKGA_NOALLOC_SCRATCH_BYTES;
-  const Layout fixed = layout_of(pb, P, 0);  // offsets up to the pool do not depend on the pool size
+  LaunchCounts lc;
+  if (counts_of(pb, &P, &lc)) return BRKGA_ERR_INVALID_ARGUMENT;
+  const Layout fixed = layout_of(pb, lc, 0);  // offsets up to the pool do not depend on the pool size
   if (fixed.off_pool >= cap) return BRKGA_ERR_WORKSPACE;
   int64_t pool_bins = (int64_t)((cap - fixed.off_pool) / ((size_t)pb->slot_words * sizeof(uint32_t)));
-  while (pool_bins > 0 && layout_of(pb, P, pool_bins).total > cap) --pool_bins;  // 256-byte rounding
+  while (pool_bins > 0 && layout_of(pb, lc, pool_bins).total > cap) --pool_bins;  // 256-byte rounding
   if (pool_bins < 1) return BRKGA_ERR_WORKSPACE;
   return brkga_decode_stage(0, pb, d_chrom, P, d_makespan, d_log, d_status, pb->noalloc_scratch, cap,
                             pool_bins, stream);
@@ -1206,7 +1477,7 @@ int brkga_decode_noalloc(const BrkgaProblem* pb, const float* d_chrom, int32_t P
 
 int brkga_evaluate_host(BrkgaProblem* pb, const float* h_chrom, int32_t P, double* h_makespan,
                         BrkgaPlacement* h_log) {
-  if (!pb || P < 0 || (P > 0 && (!h_chrom || !h_makespan))) return BRKGA_ERR_INVALID_ARGUMENT;
+  if (!pb || pb->K != 1 || P < 0 || (P > 0 && (!h_chrom || !h_makespan))) return BRKGA_ERR_INVALID_ARGUMENT;
   if (P == 0) return BRKGA_OK;
   std::lock_guard<std::mutex> lock(pb->mu);
   DeviceGuard g(pb->device);
@@ -1234,19 +1505,21 @@ int brkga_evaluate_host(BrkgaProblem* pb, const float* h_chrom, int32_t P, doubl
     pb->e_cap_log = want_log || pb->e_cap_log;
     pb->e_cap_P = cap;
   }
-  if (pb->e_pool_bins < default_pool_bins(pb, P)) pb->e_pool_bins = default_pool_bins(pb, P);
+  LaunchCounts lc;
+  if (counts_of(pb, &P, &lc)) return BRKGA_ERR_INVALID_ARGUMENT;
+  if (pb->e_pool_bins < default_pool_bins(pb, lc.items)) pb->e_pool_bins = default_pool_bins(pb, lc.items);
   if (cudaMemcpyAsync(pb->e_chrom, h_chrom, (size_t)P * 2 * pb->N * sizeof(float), cudaMemcpyHostToDevice,
                       pb->stream) != cudaSuccess)
     return BRKGA_ERR_CUDA;
   for (int attempt = 0; attempt < 12; ++attempt) {
-    const size_t need = layout_of(pb, P, pb->e_pool_bins).total;
-    if (need > pb->e_ws_bytes) {
+    const Layout l = layout_of(pb, lc, pb->e_pool_bins);
+    if (l.total > pb->e_ws_bytes) {
       if (cudaStreamSynchronize(pb->stream) != cudaSuccess) return BRKGA_ERR_CUDA;
       cudaFree(pb->e_ws);
       pb->e_ws = nullptr;
       pb->e_ws_bytes = 0;
-      if (cudaMalloc(&pb->e_ws, need) != cudaSuccess) return BRKGA_ERR_CUDA;
-      pb->e_ws_bytes = need;
+      if (cudaMalloc(&pb->e_ws, l.total) != cudaSuccess) return BRKGA_ERR_CUDA;
+      pb->e_ws_bytes = l.total;
     }
     int st = brkga_decode(pb, pb->e_chrom, P, pb->e_out, want_log ? pb->e_log : nullptr, pb->e_status, pb->e_ws,
                           pb->e_ws_bytes, pb->e_pool_bins, pb->stream);
@@ -1258,7 +1531,6 @@ int brkga_evaluate_host(BrkgaProblem* pb, const float* h_chrom, int32_t P, doubl
                         pb->stream) != cudaSuccess)
       return BRKGA_ERR_CUDA;
     unsigned long long counters[4] = {0, 0, 0, 0};
-    const Layout l = layout_of(pb, P, pb->e_pool_bins);
     if (cudaMemcpyAsync(counters, static_cast<char*>(pb->e_ws) + l.off_ctr + 8, sizeof(counters),
                         cudaMemcpyDeviceToHost, pb->stream) != cudaSuccess)
       return BRKGA_ERR_CUDA;
@@ -1280,7 +1552,7 @@ int brkga_evaluate_host(BrkgaProblem* pb, const float* h_chrom, int32_t P, doubl
 
 int brkga_initial_solution_host(BrkgaProblem* pb, const int32_t* h_order, int32_t n, int32_t* h_machine,
                                 BrkgaPlacement* h_place, double* h_machine_makespan) {
-  if (!pb || n < 0 || (n > 0 && (!h_order || !h_machine || !h_place)) || !h_machine_makespan)
+  if (!pb || pb->K != 1 || n < 0 || (n > 0 && (!h_order || !h_machine || !h_place)) || !h_machine_makespan)
     return BRKGA_ERR_INVALID_ARGUMENT;
   for (int k = 0; k < n; ++k)
     if (h_order[k] < 0 || h_order[k] >= pb->N) return BRKGA_ERR_INVALID_ARGUMENT;
@@ -1316,34 +1588,17 @@ int brkga_initial_solution_host(BrkgaProblem* pb, const int32_t* h_order, int32_
       st = BRKGA_ERR_CUDA;
       break;
     }
-    GreedyParams g;
-    DecodeParams& dp = g.p;
-    std::memset(&dp, 0, sizeof(dp));
-    dp.gene_type = pb->d_gene_type;
-    dp.mach = pb->d_mach;
-    dp.pt = pb->d_pt;
-    dp.pth = pb->d_pth;
-    dp.part_area = pb->d_area;
-    dp.nrot = pb->d_nrot;
-    dp.best_rot = pb->d_best;
-    dp.rot = pb->d_rot;
-    dp.dens = pb->d_dens;
-    dp.run_off = pb->d_run_off;
-    dp.runs = pb->d_runs;
-    dp.maskbits = pb->d_maskbits;
-    dp.newbin_ok = pb->d_newbin_ok;
-    dp.fits_flag = pb->d_fits;
-    dp.N = pb->N;
-    dp.M = pb->M;
-    dp.T = pb->T;
-    dp.status = reinterpret_cast<int32_t*>(d + off_ctr + 40);
-    dp.counters = reinterpret_cast<unsigned long long*>(d + off_ctr + 8);
-    dp.binscal = reinterpret_cast<BinScal*>(d + off_bs);
-    dp.pool = reinterpret_cast<uint32_t*>(d + off_pool);
-    dp.pool_bins = nn;
-    dp.S = 0;
-    dp.slot_words = pb->slot_words;
-    dp.slot_vac_off = pb->slot_vac_off;
+    GreedyArgs g;
+    std::memset(&g, 0, sizeof(g));
+    g.N = pb->N;
+    g.M = pb->M;
+    g.T = pb->T;
+    g.status = reinterpret_cast<int32_t*>(d + off_ctr + 40);
+    g.counters = reinterpret_cast<unsigned long long*>(d + off_ctr + 8);
+    g.binscal = reinterpret_cast<BinScal*>(d + off_bs);
+    g.pool = reinterpret_cast<uint32_t*>(d + off_pool);
+    g.slot_words = pb->slot_words;
+    g.slot_vac_off = pb->slot_vac_off;
     g.order = reinterpret_cast<const int32_t*>(d + off_order);
     g.n = n;
     g.out_machine = reinterpret_cast<int32_t*>(d + off_mach);
@@ -1351,10 +1606,10 @@ int brkga_initial_solution_host(BrkgaProblem* pb, const int32_t* h_order, int32_
     g.plate_machine = reinterpret_cast<int32_t*>(d + off_pm);
     g.plate_index = reinterpret_cast<int32_t*>(d + off_pi);
     g.machine_makespan = reinterpret_cast<double*>(d + off_mk);
-    greedy_kernel<<<1, kDecodeThreads>>>(g);
+    greedy_kernel<<<1, kDecodeThreads>>>(pb->tb, g);
     int32_t status = 0;
     if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess ||
-        cudaMemcpy(&status, dp.status, 4, cudaMemcpyDeviceToHost) != cudaSuccess) {
+        cudaMemcpy(&status, g.status, 4, cudaMemcpyDeviceToHost) != cudaSuccess) {
       st = BRKGA_ERR_CUDA;
       break;
     }

@@ -24,15 +24,30 @@ from .problem import THRESH_F32, PackedProblem, pack_problem
 
 
 class _NativeProblem:
-    """Owns one ``BrkgaProblem*`` (device-resident tables)."""
+    """Owns one ``BrkgaProblem*`` (device-resident tables of one or more instances)."""
 
-    def __init__(self, packed: PackedProblem):
+    def __init__(self, packed):
         self.lib = abi.load_library()
         self.packed = packed
         handle = ctypes.c_void_p()
-        st = self.lib.brkga_problem_create(ctypes.byref(packed.desc), ctypes.byref(handle))
-        abi.check(st, "brkga_problem_create")
+        if isinstance(packed, (list, tuple)):
+            descs = (abi.BrkgaProblemDesc * len(packed))(*[p.desc for p in packed])
+            st = self.lib.brkga_problem_create_multi(descs, len(packed), ctypes.byref(handle))
+            abi.check(st, "brkga_problem_create_multi")
+        else:
+            st = self.lib.brkga_problem_create(ctypes.byref(packed.desc), ctypes.byref(handle))
+            abi.check(st, "brkga_problem_create")
         self.handle = handle
+
+    def launch_config(self):
+        """(CTAs per SM, plates per item in shared memory, resident CTAs) of the decode kernel."""
+        c, s, r = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        abi.check(self.lib.brkga_get_launch_config(self.handle, ctypes.byref(c), ctypes.byref(s), ctypes.byref(r)))
+        return c.value, s.value, r.value
+
+    def set_launch_config(self, ctas_per_sm: int, smem_plates: int):
+        abi.check(self.lib.brkga_set_launch_config(self.handle, int(ctas_per_sm), int(smem_plates)),
+                  "brkga_set_launch_config")
 
     def close(self):
         if getattr(self, "handle", None) is not None and self.handle.value:
@@ -159,6 +174,19 @@ class DeviceDecoder:
         abi.check(self.lib.brkga_workspace_bytes(self.native.handle, int(P), self.pool_bins, ctypes.byref(nbytes)))
         return nbytes.value
 
+    def launch_config(self):
+        """(CTAs per SM, plates per item in shared memory, resident CTAs) of the decode kernel."""
+        return self.native.launch_config()
+
+    def set_launch_config(self, ctas_per_sm: int, smem_plates: int):
+        """Change the decode kernel's launch shape (0 / -1 = automatic) and
+        regrow the workspace when the new shape needs more."""
+        self.native.set_launch_config(ctas_per_sm, smem_plates)
+        need = self.workspace_bytes(self.max_pop)
+        if need > self.ws_bytes:
+            self.workspace = self.torch.empty(need, dtype=self.torch.uint8, device=self.device)
+        self.ws_bytes = max(need, self.ws_bytes)
+
     def decode(self, chrom, out=None, log=None, stream=None, kernel_events=None):
         """Decode ``chrom`` (cuda float32 [P, 2N]) into ``out`` (cuda float64 [P]).
 
@@ -197,3 +225,115 @@ class DeviceDecoder:
         """(placement tests, row chunks, plates, scan bytes) of the last decode (synchronises)."""
         c = self.workspace[8:8 + 32].view(self.torch.int64).cpu().tolist()
         return tuple(int(v) for v in c)
+
+
+class MultiDecoder:
+    """Decodes populations of several independent instances in one launch.
+
+    ``packs`` is a list of ``PackedProblem`` (up to ``abi.MAX_INSTANCES``),
+    each with its own parts, machines and plate sizes; ``max_pops[k]`` bounds
+    the rows of instance k per call.  ``decode`` takes one CUDA float32
+    tensor [P_k, 2 N_k] per instance (``decode_concat`` the rows already
+    concatenated) and returns the makespans of all rows, instance after
+    instance, from one launch of each kernel: every (chromosome, machine)
+    item of every instance goes to the same persistent decode kernel.
+    Stream-ordered, no allocation: capturable in a CUDA graph.
+    """
+
+    def __init__(self, packs, max_pops, pool_bins: int = 0, device=None):
+        import torch
+        self.torch = torch
+        self.packs = list(packs)
+        if len(max_pops) != len(self.packs):
+            raise ValueError("one population bound per instance")
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.n_genes = [p.n_genes for p in self.packs]
+        self.n_machines = [p.n_machines for p in self.packs]
+        with torch.cuda.device(self.device):
+            torch.cuda.init()
+            self.native = _NativeProblem(self.packs)
+            self.lib = self.native.lib
+            self.max_pops = np.ascontiguousarray(max_pops, dtype=np.int32)
+            self.pool_bins = int(pool_bins)
+            self.ws_bytes = self.workspace_bytes(self.max_pops)
+            self.workspace = torch.empty(self.ws_bytes, dtype=torch.uint8, device=self.device)
+            self.status = torch.zeros(1, dtype=torch.int32, device=self.device)
+
+    @property
+    def n_instances(self) -> int:
+        return len(self.packs)
+
+    def workspace_bytes(self, pops) -> int:
+        pops = np.ascontiguousarray(pops, dtype=np.int32)
+        nbytes = ctypes.c_size_t()
+        abi.check(self.lib.brkga_workspace_bytes_multi(self.native.handle, abi.ptr(pops, ctypes.c_int32),
+                                                       self.pool_bins, ctypes.byref(nbytes)),
+                  "brkga_workspace_bytes_multi")
+        return nbytes.value
+
+    def launch_config(self):
+        return self.native.launch_config()
+
+    def set_launch_config(self, ctas_per_sm: int, smem_plates: int):
+        self.native.set_launch_config(ctas_per_sm, smem_plates)
+        need = self.workspace_bytes(self.max_pops)
+        if need > self.ws_bytes:
+            self.workspace = self.torch.empty(need, dtype=self.torch.uint8, device=self.device)
+        self.ws_bytes = max(need, self.ws_bytes)
+
+    def _check_pops(self, pops) -> np.ndarray:
+        pops = np.ascontiguousarray(pops, dtype=np.int32)
+        if pops.shape != (self.n_instances,) or (pops < 0).any() or (pops > self.max_pops).any():
+            raise RuntimeError("population sizes must be 0 <= P_k <= max_pops[k], one per instance")
+        return pops
+
+    def decode_concat(self, chrom, pops, out=None, log=None, stream=None, kernel_events=None):
+        """Decode rows already concatenated instance after instance (flat
+        float32 CUDA tensor of sum_k P_k * 2 N_k keys) into ``out`` (float64 [sum P_k])."""
+        torch = self.torch
+        pops = self._check_pops(pops)
+        n_keys = int(sum(int(p) * 2 * n for p, n in zip(pops, self.n_genes)))
+        if chrom.dtype != torch.float32 or not chrom.is_cuda or not chrom.is_contiguous() or chrom.numel() != n_keys:
+            raise RuntimeError(f"chromosomes must be a contiguous float32 CUDA tensor of {n_keys} keys")
+        rows = int(pops.sum())
+        if out is None:
+            out = torch.empty(rows, dtype=torch.float64, device=chrom.device)
+        n_log = int(sum(int(p) * m * n for p, m, n in zip(pops, self.n_machines, self.n_genes)))
+        if log is not None and (log.dtype != torch.int32 or log.numel() != n_log * 5):
+            raise RuntimeError(f"log must be int32 with {n_log} x 5 entries")
+        s = stream if stream is not None else torch.cuda.current_stream(chrom.device)
+        args = (self.native.handle, ctypes.c_void_p(chrom.data_ptr()), abi.ptr(pops, ctypes.c_int32),
+                ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(log.data_ptr()) if log is not None else None,
+                ctypes.c_void_p(self.status.data_ptr()), ctypes.c_void_p(self.workspace.data_ptr()),
+                self.ws_bytes, self.pool_bins, ctypes.c_void_p(s.cuda_stream))
+        if kernel_events is None:
+            abi.check(self.lib.brkga_decode_multi(*args), "brkga_decode_multi")
+        else:
+            abi.check(self.lib.brkga_decode_multi_stage(1, *args), "brkga_decode_multi_stage")
+            kernel_events[0].record(s)
+            abi.check(self.lib.brkga_decode_multi_stage(2, *args), "brkga_decode_multi_stage")
+            kernel_events[1].record(s)
+            abi.check(self.lib.brkga_decode_multi_stage(3, *args), "brkga_decode_multi_stage")
+        return out
+
+    def decode(self, chroms, stream=None):
+        """Makespans (list of float64 CUDA tensors, one per instance) of one
+        population per instance (float32 CUDA tensors [P_k, 2 N_k])."""
+        torch = self.torch
+        if len(chroms) != self.n_instances:
+            raise RuntimeError("one population per instance")
+        for c, n in zip(chroms, self.n_genes):
+            if c.dim() != 2 or c.shape[1] != 2 * n:
+                raise RuntimeError("population k must be [P_k, 2 N_k]")
+        pops = [int(c.shape[0]) for c in chroms]
+        flat = torch.cat([c.reshape(-1) for c in chroms]).contiguous()
+        out = self.decode_concat(flat, pops, stream=stream)
+        return list(torch.split(out, pops))
+
+    def counters(self):
+        """(placement tests, row chunks, plates, scan bytes) of the last decode (synchronises)."""
+        c = self.workspace[8:8 + 32].view(self.torch.int64).cpu().tolist()
+        return tuple(int(v) for v in c)
+
+    def close(self):
+        self.native.close()

@@ -150,6 +150,65 @@ int brkga_decode_stage(int32_t stage, const BrkgaProblem* problem, const float* 
 int brkga_decode_noalloc(const BrkgaProblem* problem, const float* d_chrom, int32_t P,
                          double* d_makespan, BrkgaPlacement* d_log, int32_t* d_status, void* stream);
 
+/* ---- Several independent instances per launch ----
+ * No reference counterpart: the reference builds one evaluator per instance
+ * (FullNativeDecoderEvaluator, full_native_decoder.py:2937-2981) and decodes
+ * one population at a time.  Here a problem may hold up to
+ * BRKGA_MAX_INSTANCES instances with their own parts, machines and plate
+ * sizes; one launch decodes P_k chromosomes of each instance k, every
+ * (chromosome, machine) item of every instance in one persistent decode
+ * kernel, longest items first.  The single-instance entry points above
+ * (brkga_decode, brkga_decode_stage, brkga_workspace_bytes,
+ * brkga_decode_noalloc, brkga_evaluate_host, brkga_initial_solution_host,
+ * the surrogate) refuse a problem of more than one instance with
+ * BRKGA_ERR_INVALID_ARGUMENT. */
+#define BRKGA_MAX_INSTANCES 64
+
+/* brkga_problem_create for descs[0..K-1] (1 <= K <= BRKGA_MAX_INSTANCES);
+ * brkga_problem_create(d) is brkga_problem_create_multi(d, 1). */
+int brkga_problem_create_multi(const BrkgaProblemDesc* descs, int32_t K, BrkgaProblem** out);
+
+/* Number of instances of a problem. */
+int brkga_problem_instances(const BrkgaProblem* problem, int32_t* K);
+
+/* Workspace bytes for pops[k] chromosomes of instance k (pops: host int32 [K]). */
+int brkga_workspace_bytes_multi(const BrkgaProblem* problem, const int32_t* pops, int64_t pool_bins,
+                                size_t* bytes);
+
+/* Decode pops[k] chromosomes of every instance k in one launch of each kernel.
+ *   pops        host int32 [K], read during the call (values go into the
+ *               kernel parameters, so a captured graph keeps them)
+ *   d_chrom     device float32: instance 0's pops[0] rows of 2*N_0 keys, then
+ *               instance 1's rows of 2*N_1 keys, and so on
+ *   d_makespan  device float64 [sum pops], rows in the same order
+ *   d_log       NULL or device BrkgaPlacement: per row, M_k * N_k entries
+ *               (machine-major, as brkga_decode), rows in order
+ * Otherwise as brkga_decode (stream-ordered, no allocation, no host sync). */
+int brkga_decode_multi(const BrkgaProblem* problem, const float* d_chrom, const int32_t* pops,
+                       double* d_makespan, BrkgaPlacement* d_log, int32_t* d_status, void* d_ws,
+                       size_t ws_bytes, int64_t pool_bins, void* stream);
+
+/* One stage (1, 2, 3; 0 = all) of brkga_decode_multi, as brkga_decode_stage. */
+int brkga_decode_multi_stage(int32_t stage, const BrkgaProblem* problem, const float* d_chrom,
+                             const int32_t* pops, double* d_makespan, BrkgaPlacement* d_log,
+                             int32_t* d_status, void* d_ws, size_t ws_bytes, int64_t pool_bins,
+                             void* stream);
+
+/* Launch shape of the decode kernel (the autotuner's knobs; no reference
+ * counterpart): ctas_per_sm resident CTAs of 4 warps per SM (1..32, 0 =
+ * automatic) and smem_plates plates of each item kept in shared memory
+ * (0..8, the rest in the global pool; -1 = as many as fit, at most 4).
+ * A shape that cannot be resident is refused with BRKGA_ERR_INVALID_ARGUMENT
+ * and the previous one kept.  The workspace size depends on the shape: query
+ * brkga_workspace_bytes again after a change.  Not to be called while a
+ * decode of this problem is being launched from another thread. */
+int brkga_set_launch_config(BrkgaProblem* problem, int32_t ctas_per_sm, int32_t smem_plates);
+
+/* The shape in use: CTAs per SM, plates per item in shared memory, and the
+ * decode kernel's grid (SMs x CTAs per SM); any output may be NULL. */
+int brkga_get_launch_config(const BrkgaProblem* problem, int32_t* ctas_per_sm, int32_t* smem_plates,
+                            int32_t* resident_ctas);
+
 /* Host-to-host evaluation, the drop-in for NativeFullDecoder::evaluate_batch
  * (full_native_decoder.py:563-641): copies h_chrom [P, 2N] float32 to the
  * device, decodes, and writes h_makespan [P] float64.  Grows its internal

@@ -84,3 +84,20 @@ def test_null_problem_arguments(lib):
     assert lib.brkga_decode(None, None, 1, None, None, None, None, 0, 0, None) == abi.ERR_INVALID_ARGUMENT
     assert lib.brkga_evaluate_host(None, None, 1, None, None) == abi.ERR_INVALID_ARGUMENT
     lib.brkga_problem_destroy(None)
+
+
+def test_multi_instance_arguments(lib):
+    pk = [_packed(), _packed()]
+    descs = (abi.BrkgaProblemDesc * 2)(*[p.desc for p in pk])
+    h = ctypes.c_void_p()
+    assert lib.brkga_problem_create_multi(descs, 0, ctypes.byref(h)) == abi.ERR_INVALID_ARGUMENT
+    assert lib.brkga_problem_create_multi(descs, abi.MAX_INSTANCES + 1, ctypes.byref(h)) == abi.ERR_INVALID_ARGUMENT
+    assert lib.brkga_problem_create_multi(None, 1, ctypes.byref(h)) == abi.ERR_INVALID_ARGUMENT
+    pk[1].arrays["part_area"][0] = 0.0  # a bad second instance is caught before any device work
+    assert lib.brkga_problem_create_multi(descs, 2, ctypes.byref(h)) == abi.ERR_BAD_INSTANCE
+    pops = np.array([3, 4], np.int32)
+    n = ctypes.c_size_t()
+    assert lib.brkga_workspace_bytes_multi(None, abi.ptr(pops, ctypes.c_int32), 0, ctypes.byref(n)) == \
+        abi.ERR_INVALID_ARGUMENT
+    assert lib.brkga_set_launch_config(None, 1, 0) == abi.ERR_INVALID_ARGUMENT
+    assert lib.brkga_get_launch_config(None, None, None, None) == abi.ERR_INVALID_ARGUMENT
