@@ -1,0 +1,104 @@
+"""Launch-shape autotuner for the decode kernel.
+
+The decode kernel's two knobs (``brkga_set_launch_config``) trade against
+each other: more resident CTAs per SM hide more latency, more plates per item
+in shared memory keep more collision searches off the global pool, and both
+draw on the same 228 KB of shared memory per SM, whose share per plate grows
+with the plate grid (a 500 x 500 plate is 36 KB as bit-packed rows, a
+150 x 150 one 3.6 KB).  ``autotune`` times each feasible shape on a sample of
+the caller's own population (CUDA events around the decode kernel alone),
+keeps the fastest, and remembers it per device and grid size in a JSON
+cache, so later runs on the same plate grids skip the search.
+
+The reference has no counterpart (its kernels use fixed launch shapes,
+full_native_decoder.py:2570-2755).
+"""
+from __future__ import annotations
+
+import json
+import os
+from typing import Iterable, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import abi
+
+DEFAULT_SHAPES: Tuple[Tuple[int, int], ...] = tuple((c, s) for c in (2, 4, 6, 8) for s in (0, 1, 2, 4))
+
+
+def grid_key(packs: Sequence, device_index: int = 0) -> str:
+    """Cache key: device, SM count, the largest plate grid, genes and machines."""
+    import torch
+    props = torch.cuda.get_device_properties(device_index)
+    L = max(int(max(p.arrays["bin_length"])) for p in packs)
+    W = max(int(max(p.arrays["bin_width"])) for p in packs)
+    N = max(p.n_genes for p in packs)
+    M = max(p.n_machines for p in packs)
+    return f"{props.name}|sm{props.multi_processor_count}|grid{L}x{W}|N{N}|M{M}|K{len(packs)}"
+
+
+def _time_decode(decoder, run, repeats: int) -> float:
+    import torch
+    times = []
+    for _ in range(repeats + 1):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        run((e0, e1))
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    st = int(decoder.status.item())
+    if st != 0:
+        raise abi.BrkgaError(st, "decode during autotuning")
+    return float(np.median(times[1:]))
+
+
+def autotune(decoder, chrom, pops=None, shapes: Optional[Iterable[Tuple[int, int]]] = None, repeats: int = 2,
+             cache_path: Optional[str] = None, key: Optional[str] = None) -> dict:
+    """Pick the fastest decode-kernel launch shape for ``decoder``.
+
+    ``decoder`` is a ``DeviceDecoder`` (``chrom``: float32 CUDA [P, 2N]) or a
+    ``MultiDecoder`` (``chrom``: the flat concatenated rows, ``pops``: rows per
+    instance).  Shapes that cannot be resident are skipped.  Returns
+    ``{"key", "shape", "ms", "table": [(ctas_per_sm, smem_plates, ms), ...],
+    "cached"}`` and leaves the decoder on the chosen shape.
+    """
+    import torch
+    packs = decoder.packs if hasattr(decoder, "packs") else [decoder.packed]
+    key = key or grid_key(packs, decoder.device.index or 0)
+    cache = {}
+    if cache_path and os.path.exists(cache_path):
+        with open(cache_path) as f:
+            cache = json.load(f)
+    if key in cache:
+        c, s = cache[key]["shape"]
+        decoder.set_launch_config(c, s)
+        return {"key": key, "shape": (c, s), "ms": cache[key]["ms"], "table": cache[key]["table"], "cached": True}
+
+    if pops is None:
+        out = torch.empty(chrom.shape[0], dtype=torch.float64, device=chrom.device)
+        run = lambda ev: decoder.decode(chrom, out=out, kernel_events=ev)  # noqa: E731
+    else:
+        out = torch.empty(int(np.sum(pops)), dtype=torch.float64, device=chrom.device)
+        run = lambda ev: decoder.decode_concat(chrom, pops, out=out, kernel_events=ev)  # noqa: E731
+    reference = None
+    table = []
+    for c, s in (shapes or DEFAULT_SHAPES):
+        try:
+            decoder.set_launch_config(c, s)
+        except abi.BrkgaError:
+            continue
+        ms = _time_decode(decoder, run, repeats)
+        if reference is None:
+            reference = out.clone()
+        elif not torch.equal(out, reference):
+            raise RuntimeError(f"launch shape {(c, s)} changed the makespans")
+        table.append((c, s, ms))
+    if not table:
+        raise RuntimeError("no launch shape could be resident")
+    c, s, ms = min(table, key=lambda t: t[2])
+    decoder.set_launch_config(c, s)
+    if cache_path:
+        cache[key] = {"shape": [c, s], "ms": ms, "table": table}
+        os.makedirs(os.path.dirname(os.path.abspath(cache_path)), exist_ok=True)
+        with open(cache_path, "w") as f:
+            json.dump(cache, f, indent=1, sort_keys=True)
+    return {"key": key, "shape": (c, s), "ms": ms, "table": table, "cached": False}

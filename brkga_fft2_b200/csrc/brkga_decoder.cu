@@ -113,6 +113,7 @@ struct InstRun {
   int item0;           // first (chromosome, machine) item
   int S2;              // bitonic sort width (power of two >= N)
   long long chrom_off; // first float of its chromosomes
+  long long out_off;   // first makespan
   long long seq0;      // first entry of its part orders (and log entries), N per item
 };
 
@@ -551,10 +552,10 @@ struct ItemCtx {
   MachDev md;
 };
 
-// At least 8 resident CTAs per SM: 64 registers per thread, no spills (left
-// free, the compiler picks fewer and spills; 56 or 48 measured slower).
-__global__ void __launch_bounds__(kDecodeThreads, 8) decode_kernel(const __grid_constant__ Tables tb,
-                                                                   const __grid_constant__ Run run) {
+// The tables go by value (every access has a fixed parameter offset); only
+// the per-launch instance array, which is searched, is a grid constant.
+__global__ void __launch_bounds__(kDecodeThreads) decode_kernel(const Tables tb,
+                                                                const __grid_constant__ Run run) {
   extern __shared__ __align__(16) uint32_t smem[];
   __shared__ SearchShared sh;
   __shared__ ItemCtx ctx;
@@ -688,11 +689,12 @@ __global__ void __launch_bounds__(kDecodeThreads, 8) decode_kernel(const __grid_
 __global__ void reduce_kernel(const __grid_constant__ Tables tb, const __grid_constant__ Run run) {
   const int row = blockIdx.x * blockDim.x + threadIdx.x;
   if (row >= run.n_rows) return;
+  const int k = inst_of_row(run, row);
+  double* out = run.out + run.r[k].out_off + (row - run.r[k].crow0);
   if (run.infeas[row]) {
-    run.out[row] = 1e16;  // placement.py:9,151-153
+    *out = 1e16;  // placement.py:9,151-153
     return;
   }
-  const int k = inst_of_row(run, row);
   const int M = tb.inst[k].M;
   const double* mk = run.mk + run.r[k].item0 + (long long)(row - run.r[k].crow0) * M;
   double worst = 0.0;
@@ -702,7 +704,7 @@ __global__ void reduce_kernel(const __grid_constant__ Tables tb, const __grid_co
     if (v != v) bad = true;
     else if (v > worst) worst = v;  // placement.py:154-156
   }
-  run.out[row] = bad ? nan("") : worst;
+  *out = bad ? nan("") : worst;
 }
 
 // Greedy initial solution (BRKGA_alg3.py:445-603 with binClassInitialSol.py):
@@ -1184,9 +1186,11 @@ void merge_instance(const BrkgaProblemDesc* d, Merged& g) {
   g.inst.push_back(id);
 }
 
-int fill_run(const BrkgaProblem* pb, const int32_t* pops, const LaunchCounts& lc, const Layout& l, char* ws,
-             const float* d_chrom, double* d_out, BrkgaPlacement* d_log, int32_t* d_status, int64_t pool_bins,
-             Run* run) {
+// chrom_offs / out_offs (host [K], may be NULL): where each instance's
+// chromosomes (in floats) and makespans start; NULL = packed one after another.
+int fill_run(const BrkgaProblem* pb, const int32_t* pops, const int64_t* chrom_offs, const int64_t* out_offs,
+             const LaunchCounts& lc, const Layout& l, char* ws, const float* d_chrom, double* d_out,
+             BrkgaPlacement* d_log, int32_t* d_status, int64_t pool_bins, Run* run) {
   std::memset(run, 0, sizeof(Run));
   run->K = pb->K;
   run->n_rows = (int)lc.rows;
@@ -1219,7 +1223,8 @@ int fill_run(const BrkgaProblem* pb, const int32_t* pops, const LaunchCounts& lc
     r.crow0 = (int)row;
     r.item0 = (int)item;
     r.S2 = pb->s2[k];
-    r.chrom_off = chrom;
+    r.chrom_off = chrom_offs ? chrom_offs[k] : chrom;
+    r.out_off = out_offs ? out_offs[k] : row;
     r.seq0 = seq;
     row += pops[k];
     item += (int64_t)pops[k] * id.M;
@@ -1416,13 +1421,17 @@ int brkga_workspace_bytes(const BrkgaProblem* pb, int32_t P, int64_t pool_bins, 
   return brkga_workspace_bytes_multi(pb, &P, pool_bins, bytes);
 }
 
-int brkga_decode_multi_stage(int32_t stage, const BrkgaProblem* pb, const float* d_chrom, const int32_t* pops,
-                             double* d_makespan, BrkgaPlacement* d_log, int32_t* d_status, void* d_ws,
-                             size_t ws_bytes, int64_t pool_bins, void* stream) {
+int brkga_decode_multi_at(int32_t stage, const BrkgaProblem* pb, const float* d_chrom, const int64_t* chrom_offsets,
+                          const int32_t* pops, double* d_makespan, const int64_t* makespan_offsets,
+                          BrkgaPlacement* d_log, int32_t* d_status, void* d_ws, size_t ws_bytes, int64_t pool_bins,
+                          void* stream) {
   if (!pb || !pops || pool_bins < 0 || stage < 0 || stage > 3) return BRKGA_ERR_INVALID_ARGUMENT;
   LaunchCounts lc;
   int st = counts_of(pb, pops, &lc);
   if (st) return st;
+  for (int k = 0; k < pb->K; ++k)
+    if ((chrom_offsets && chrom_offsets[k] < 0) || (makespan_offsets && makespan_offsets[k] < 0))
+      return BRKGA_ERR_INVALID_ARGUMENT;
   if (lc.rows == 0) return BRKGA_OK;
   if (!d_chrom || !d_makespan || !d_status || !d_ws) return BRKGA_ERR_INVALID_ARGUMENT;
   if (pool_bins == 0) pool_bins = default_pool_bins(pb, lc.items);
@@ -1430,8 +1439,16 @@ int brkga_decode_multi_stage(int32_t stage, const BrkgaProblem* pb, const float*
   if (ws_bytes < l.total) return BRKGA_ERR_WORKSPACE;
   DeviceGuard g(pb->device);
   Run run;
-  fill_run(pb, pops, lc, l, static_cast<char*>(d_ws), d_chrom, d_makespan, d_log, d_status, pool_bins, &run);
+  fill_run(pb, pops, chrom_offsets, makespan_offsets, lc, l, static_cast<char*>(d_ws), d_chrom, d_makespan, d_log,
+           d_status, pool_bins, &run);
   return launch(pb, stage, run, static_cast<cudaStream_t>(stream));
+}
+
+int brkga_decode_multi_stage(int32_t stage, const BrkgaProblem* pb, const float* d_chrom, const int32_t* pops,
+                             double* d_makespan, BrkgaPlacement* d_log, int32_t* d_status, void* d_ws,
+                             size_t ws_bytes, int64_t pool_bins, void* stream) {
+  return brkga_decode_multi_at(stage, pb, d_chrom, nullptr, pops, d_makespan, nullptr, d_log, d_status, d_ws,
+                               ws_bytes, pool_bins, stream);
 }
 
 int brkga_decode_multi(const BrkgaProblem* pb, const float* d_chrom, const int32_t* pops, double* d_makespan,

@@ -316,6 +316,37 @@ class MultiDecoder:
             abi.check(self.lib.brkga_decode_multi_stage(3, *args), "brkga_decode_multi_stage")
         return out
 
+    def decode_at(self, chrom, chrom_offsets, pops, out, out_offsets, stream=None, kernel_events=None):
+        """Decode instance k's ``pops[k]`` rows starting at float ``chrom_offsets[k]``
+        of ``chrom`` into ``out`` from element ``out_offsets[k]`` (one launch of
+        each kernel; both tensors are flat CUDA buffers the caller lays out)."""
+        torch = self.torch
+        pops = self._check_pops(pops)
+        co = np.ascontiguousarray(chrom_offsets, dtype=np.int64)
+        oo = np.ascontiguousarray(out_offsets, dtype=np.int64)
+        if co.shape != pops.shape or oo.shape != pops.shape:
+            raise RuntimeError("one chromosome offset and one makespan offset per instance")
+        for k, p in enumerate(pops):
+            if p and (co[k] < 0 or co[k] + int(p) * 2 * self.n_genes[k] > chrom.numel() or oo[k] < 0
+                      or oo[k] + int(p) > out.numel()):
+                raise RuntimeError(f"instance {k}: rows outside the buffers")
+        if chrom.dtype != torch.float32 or out.dtype != torch.float64 or not (chrom.is_cuda and out.is_cuda):
+            raise RuntimeError("chrom must be float32 and out float64 CUDA tensors")
+        s = stream if stream is not None else torch.cuda.current_stream(chrom.device)
+        args = (self.native.handle, ctypes.c_void_p(chrom.data_ptr()), abi.ptr(co, ctypes.c_int64),
+                abi.ptr(pops, ctypes.c_int32), ctypes.c_void_p(out.data_ptr()), abi.ptr(oo, ctypes.c_int64), None,
+                ctypes.c_void_p(self.status.data_ptr()), ctypes.c_void_p(self.workspace.data_ptr()),
+                self.ws_bytes, self.pool_bins, ctypes.c_void_p(s.cuda_stream))
+        if kernel_events is None:
+            abi.check(self.lib.brkga_decode_multi_at(0, *args), "brkga_decode_multi_at")
+        else:
+            abi.check(self.lib.brkga_decode_multi_at(1, *args), "brkga_decode_multi_at")
+            kernel_events[0].record(s)
+            abi.check(self.lib.brkga_decode_multi_at(2, *args), "brkga_decode_multi_at")
+            kernel_events[1].record(s)
+            abi.check(self.lib.brkga_decode_multi_at(3, *args), "brkga_decode_multi_at")
+        return out
+
     def decode(self, chroms, stream=None):
         """Makespans (list of float64 CUDA tensors, one per instance) of one
         population per instance (float32 CUDA tensors [P_k, 2 N_k])."""

@@ -194,6 +194,16 @@ int brkga_decode_multi_stage(int32_t stage, const BrkgaProblem* problem, const f
                              int32_t* d_status, void* d_ws, size_t ws_bytes, int64_t pool_bins,
                              void* stream);
 
+/* brkga_decode_multi_stage with each instance's rows at an explicit place:
+ * instance k's pops[k] chromosomes start at float chrom_offsets[k] of d_chrom
+ * and its makespans at element makespan_offsets[k] of d_makespan (host int64
+ * [K]; either may be NULL = packed one after another).  Lets a GA decode the
+ * non-elite rows of every instance's population block in place. */
+int brkga_decode_multi_at(int32_t stage, const BrkgaProblem* problem, const float* d_chrom,
+                          const int64_t* chrom_offsets, const int32_t* pops, double* d_makespan,
+                          const int64_t* makespan_offsets, BrkgaPlacement* d_log, int32_t* d_status,
+                          void* d_ws, size_t ws_bytes, int64_t pool_bins, void* stream);
+
 /* Launch shape of the decode kernel (the autotuner's knobs; no reference
  * counterpart): ctas_per_sm resident CTAs of 4 warps per SM (1..32, 0 =
  * automatic) and smem_plates plates of each item kept in shared memory
