@@ -1,14 +1,20 @@
 """Launch-shape autotuner for the decode kernel.
 
-The decode kernel's two knobs (``brkga_set_launch_config``) trade against
-each other: more resident CTAs per SM hide more latency, more plates per item
-in shared memory keep more collision searches off the global pool, and both
-draw on the same 228 KB of shared memory per SM, whose share per plate grows
-with the plate grid (a 500 x 500 plate is 36 KB as bit-packed rows, a
-150 x 150 one 3.6 KB).  ``autotune`` times each feasible shape on a sample of
-the caller's own population (CUDA events around the decode kernel alone),
-keeps the fastest, and remembers it per device and grid size in a JSON
-cache, so later runs on the same plate grids skip the search.
+The decode kernel has three knobs (``brkga_set_launch_config``).  Two trade
+against each other: more resident CTAs per SM hide more latency, more plates
+per item in shared memory keep more collision searches off the global pool,
+and both draw on the same 228 KB of shared memory per SM, whose share per
+plate grows with the plate grid (a 500 x 500 plate is 36 KB as bit-packed
+rows, a 150 x 150 one 3.6 KB).  The third, ``task_max``, decides when a warp
+deals (candidate row, 32-column word) pairs of the exact collision test
+across its lanes instead of giving each lane one candidate row: dealing wins
+while the pairs are few, loses on wide plates with many surviving candidates
+(long, uneven chains), so its best value depends on the grid and masks.
+``autotune`` times the shapes first (``task_max`` at its default), then the
+``task_max`` values at the best shape, each on the caller's own population
+(CUDA events around the decode kernel alone), keeps the fastest, and
+remembers it per device and grid size in a JSON cache, so later runs on the
+same plate grids skip the search.
 
 The reference has no counterpart (its kernels use fixed launch shapes,
 full_native_decoder.py:2570-2755).
@@ -24,6 +30,7 @@ import numpy as np
 from . import abi
 
 DEFAULT_SHAPES: Tuple[Tuple[int, int], ...] = tuple((c, s) for c in (2, 4, 6, 8) for s in (0, 1, 2, 4))
+DEFAULT_TASK_MAX: Tuple[int, ...] = (0, 64, 256, 1024, 8192)
 
 
 def grid_key(packs: Sequence, device_index: int = 0) -> str:
@@ -51,15 +58,17 @@ def _time_decode(decoder, run, repeats: int) -> float:
     return float(np.median(times[1:]))
 
 
-def autotune(decoder, chrom, pops=None, shapes: Optional[Iterable[Tuple[int, int]]] = None, repeats: int = 2,
-             cache_path: Optional[str] = None, key: Optional[str] = None) -> dict:
-    """Pick the fastest decode-kernel launch shape for ``decoder``.
+def autotune(decoder, chrom, pops=None, shapes: Optional[Iterable[Tuple[int, int]]] = None,
+             task_max_values: Optional[Iterable[int]] = None, repeats: int = 2, cache_path: Optional[str] = None,
+             key: Optional[str] = None) -> dict:
+    """Pick the fastest decode-kernel configuration for ``decoder``.
 
     ``decoder`` is a ``DeviceDecoder`` (``chrom``: float32 CUDA [P, 2N]) or a
     ``MultiDecoder`` (``chrom``: the flat concatenated rows, ``pops``: rows per
     instance).  Shapes that cannot be resident are skipped.  Returns
-    ``{"key", "shape", "ms", "table": [(ctas_per_sm, smem_plates, ms), ...],
-    "cached"}`` and leaves the decoder on the chosen shape.
+    ``{"key", "config": (ctas_per_sm, smem_plates, task_max), "ms", "table":
+    [(ctas_per_sm, smem_plates, task_max, ms), ...], "cached"}`` and leaves the
+    decoder on the chosen configuration.
     """
     import torch
     packs = decoder.packs if hasattr(decoder, "packs") else [decoder.packed]
@@ -69,9 +78,10 @@ def autotune(decoder, chrom, pops=None, shapes: Optional[Iterable[Tuple[int, int
         with open(cache_path) as f:
             cache = json.load(f)
     if key in cache:
-        c, s = cache[key]["shape"]
-        decoder.set_launch_config(c, s)
-        return {"key": key, "shape": (c, s), "ms": cache[key]["ms"], "table": cache[key]["table"], "cached": True}
+        c, s, t = cache[key]["config"]
+        decoder.set_launch_config(c, s, t)
+        return {"key": key, "config": (c, s, t), "ms": cache[key]["ms"], "table": cache[key]["table"],
+                "cached": True}
 
     if pops is None:
         out = torch.empty(chrom.shape[0], dtype=torch.float64, device=chrom.device)
@@ -79,26 +89,34 @@ def autotune(decoder, chrom, pops=None, shapes: Optional[Iterable[Tuple[int, int
     else:
         out = torch.empty(int(np.sum(pops)), dtype=torch.float64, device=chrom.device)
         run = lambda ev: decoder.decode_concat(chrom, pops, out=out, kernel_events=ev)  # noqa: E731
-    reference = None
+    reference = []
     table = []
-    for c, s in (shapes or DEFAULT_SHAPES):
+
+    def trial(c, s, t):
         try:
-            decoder.set_launch_config(c, s)
+            decoder.set_launch_config(c, s, t)
         except abi.BrkgaError:
-            continue
+            return
         ms = _time_decode(decoder, run, repeats)
-        if reference is None:
-            reference = out.clone()
-        elif not torch.equal(out, reference):
-            raise RuntimeError(f"launch shape {(c, s)} changed the makespans")
-        table.append((c, s, ms))
+        if not reference:
+            reference.append(out.clone())
+        elif not torch.equal(out, reference[0]):
+            raise RuntimeError(f"launch configuration {(c, s, t)} changed the makespans")
+        table.append((c, s, t, ms))
+
+    for c, s in (shapes or DEFAULT_SHAPES):
+        trial(c, s, -1)
     if not table:
         raise RuntimeError("no launch shape could be resident")
-    c, s, ms = min(table, key=lambda t: t[2])
-    decoder.set_launch_config(c, s)
+    c, s, _, _ = min(table, key=lambda r: r[3])
+    for t in (task_max_values if task_max_values is not None else DEFAULT_TASK_MAX):
+        trial(c, s, t)
+    c, s, t, ms = min(table, key=lambda r: r[3])
+    decoder.set_launch_config(c, s, t)
+    t = decoder.launch_config()[3]
     if cache_path:
-        cache[key] = {"shape": [c, s], "ms": ms, "table": table}
+        cache[key] = {"config": [c, s, t], "ms": ms, "table": table}
         os.makedirs(os.path.dirname(os.path.abspath(cache_path)), exist_ok=True)
         with open(cache_path, "w") as f:
             json.dump(cache, f, indent=1, sort_keys=True)
-    return {"key": key, "shape": (c, s), "ms": ms, "table": table, "cached": False}
+    return {"key": key, "config": (c, s, t), "ms": ms, "table": table, "cached": False}

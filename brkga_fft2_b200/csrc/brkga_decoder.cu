@@ -54,13 +54,15 @@ constexpr int kDecodeThreads = 128; // 4 warps per item
 constexpr int kMaxInst = BRKGA_MAX_INSTANCES;
 constexpr int kMaxCtasPerSm = 32;
 constexpr int kMaxSmemPlates = 8;
+constexpr int kDefaultTaskMax = 512;
+constexpr int kMaxTaskMax = 32 * 256;  // 32 candidates x the output words of the widest plate
 constexpr unsigned long long kKeyNone = ~0ull;
 constexpr unsigned kFull = 0xFFFFFFFFu;
 
 struct RotDev {
   int h, w, mw;      // rows, columns, 32-bit words per mask row
   int dens_row;      // first entry in dens[] (h entries)
-  int run_row;       // first entry in run_off[] (h + 1 entries, absolute indices into runs[])
+  int trun, ntrun;   // runs of ones of all rows in test order: truns[trun .. trun + ntrun)
   int mask_base;     // first word in maskbits[] (h * mw words)
   int imax, dmax;    // row with the longest run of ones and that length
 };
@@ -99,8 +101,7 @@ struct Tables {
   const int32_t* best_rot;
   const RotDev* rot;        // [absolute type * 4 + rotation]
   const uint16_t* dens;
-  const int32_t* run_off;
-  const uint32_t* runs;
+  const uint2* truns;       // (start | length << 16, row) per run of ones
   const uint32_t* maskbits;
   const uint8_t* newbin_ok;
   const uint8_t* fits;
@@ -136,6 +137,7 @@ struct Run {
   uint32_t* pool;
   long long pool_bins;
   int S, slot_words, slot_vac_off;
+  int task_max;  // most (survivor, word) pairs of a chunk dealt across lanes
   InstRun r[kMaxInst];
 };
 static_assert(sizeof(Tables) + sizeof(Run) <= 4096, "kernel parameters must stay within 4 KB");
@@ -216,38 +218,71 @@ __device__ __forceinline__ uint32_t blocked(const uint32_t* row, int p0, int d) 
   return res;
 }
 
+#ifndef BRKGA_TEST_ILP
+#define BRKGA_TEST_ILP 2
+#endif
+#ifndef BRKGA_VAC_ILP
+#define BRKGA_VAC_ILP 4
+#endif
+
+// Necessary condition for the rotation to fit with its top row at ty: every
+// plate row it covers has a free run at least as long as the mask row's
+// longest run (numba_utils.py:50-94).  Widest row first, then bottom to top,
+// BRKGA_VAC_ILP rows per step so their loads overlap.
 __device__ __forceinline__ bool vacancy_ok(const uint16_t* vac, int ty, const RotDev& rd,
                                            const uint16_t* dens) {
-  if (vac[ty + rd.imax] < rd.dmax) return false;  // widest row first, then bottom to top
+  if (vac[ty + rd.imax] < rd.dmax) return false;
   const uint16_t* d = dens + rd.dens_row;
-  for (int i = rd.h - 1; i >= 0; --i)
-    if (vac[ty + i] < __ldg(d + i)) return false;
+  const uint16_t* v = vac + ty;
+  int i = rd.h - 1;
+  for (; i >= BRKGA_VAC_ILP - 1; i -= BRKGA_VAC_ILP) {
+    bool bad = false;
+#pragma unroll
+    for (int u = 0; u < BRKGA_VAC_ILP; ++u) bad |= v[i - u] < __ldg(d + i - u);
+    if (bad) return false;
+  }
+  for (; i >= 0; --i)
+    if (v[i] < __ldg(d + i)) return false;
   return true;
 }
 
-// Leftmost x at which the rotation fits with its top row at ty, or -1.
-// Output words (32 candidate x each) are tried left to right; inside a word
-// the mask rows go widest row first, then bottom to top: plates fill from
-// the bottom, so those rows reject a blocked candidate soonest.
-__device__ int first_free_x(const uint32_t* grid, int RS, int W, int ty, const RotDev& rd,
-                            const int32_t* run_off, const uint32_t* runs) {
+// The bits of F (candidate columns base .. base + 31) at which the rotation
+// fits with its top row at plate row g0: every run of ones of the mask, in
+// test order (widest row, then bottom to top: plates fill from the bottom, so
+// those rows reject a blocked candidate soonest), clears the columns it would
+// overlap; BRKGA_TEST_ILP independent runs per step, stop when F is empty.
+__device__ __forceinline__ uint32_t word_free(const uint32_t* g0, int RS, int base, uint32_t F, const RotDev& rd,
+                                              const uint2* truns) {
+  const uint2* e = truns + rd.trun;
+  const int n = rd.ntrun;
+  int q = 0;
+  for (; q + BRKGA_TEST_ILP <= n && F; q += BRKGA_TEST_ILP) {
+    uint32_t bl = 0u;
+#pragma unroll
+    for (int u = 0; u < BRKGA_TEST_ILP; ++u) {
+      const uint2 r = __ldg(e + q + u);
+      bl |= blocked(g0 + (int)r.y * RS, base + (int)(r.x & 0xFFFFu), (int)(r.x >> 16));
+    }
+    F &= ~bl;
+  }
+  for (; q < n && F; ++q) {
+    const uint2 r = __ldg(e + q);
+    F &= ~blocked(g0 + (int)r.y * RS, base + (int)(r.x & 0xFFFFu), (int)(r.x >> 16));
+  }
+  return F;
+}
+
+// Leftmost x at which the rotation fits with its top row at ty, or -1
+// (output words of 32 candidate columns tried left to right).
+__device__ __forceinline__ int first_free_x(const uint32_t* grid, int RS, int W, int ty, const RotDev& rd,
+                                            const uint2* truns) {
   const int nx = W - rd.w + 1;
   const int nwo = (nx + 31) >> 5;
-  const int32_t* ro = run_off + rd.run_row;
+  const uint32_t* g0 = grid + (size_t)ty * RS;
   for (int k = 0; k < nwo; ++k) {
-    uint32_t F = (k == nwo - 1 && (nx & 31)) ? ((1u << (nx & 31)) - 1u) : 0xFFFFFFFFu;
-    const int base = k << 5;
-    for (int ii = -1; ii < rd.h && F; ++ii) {
-      const int i = ii < 0 ? rd.imax : rd.h - 1 - ii;
-      if (ii >= 0 && i == rd.imax) continue;
-      const uint32_t* row = grid + (size_t)(ty + i) * RS;
-      const int q1 = __ldg(ro + i + 1);
-      for (int q = __ldg(ro + i); q < q1 && F; ++q) {
-        const uint32_t rr = __ldg(runs + q);
-        F &= ~blocked(row, base + (int)(rr & 0xFFFFu), (int)(rr >> 16));
-      }
-    }
-    if (F) return base + __ffs(F) - 1;
+    const uint32_t F0 = (k == nwo - 1 && (nx & 31)) ? ((1u << (nx & 31)) - 1u) : 0xFFFFFFFFu;
+    const uint32_t F = word_free(g0, RS, k << 5, F0, rd, truns);
+    if (F) return (k << 5) + __ffs(F) - 1;
   }
   return -1;
 }
@@ -412,6 +447,7 @@ struct SearchShared {
   unsigned long long best;
   int chunk, total, nr;
   int rlist[4];
+  unsigned char surv[kDecodeThreads / 32][32];  // per warp: lanes whose candidate passed the vacancy filter
 };
 
 // Best placement key of part type t (absolute) on one plate (kKeyNone if it
@@ -421,7 +457,8 @@ struct SearchShared {
 // atomicMin.  Called by all threads of the CTA; contains __syncthreads.
 __device__ __forceinline__ unsigned long long search_plate(const Tables& tb, const MachDev& md,
                                                            const uint32_t* grid, const uint16_t* vac, int enc,
-                                                           int t, SearchShared& sh, unsigned long long& c_tests,
+                                                           int t, int task_max, SearchShared& sh,
+                                                           unsigned long long& c_tests,
                                                            unsigned long long& c_chunks,
                                                            unsigned long long& c_bytes) {
   const int tid = threadIdx.x, lane = tid & 31;
@@ -459,16 +496,58 @@ __device__ __forceinline__ unsigned long long search_plate(const Tables& tb, con
     cur = __shfl_sync(kFull, cur, 0);
     if (key_of(max(enc, md.L - ty_hi), ty_hi + rd.h - 1, 0, r) >= cur) continue;
     const int ty = ty_hi - lane;
-    int x = -1;
-    if (ty >= 0 && vacancy_ok(vac, ty, rd, tb.dens)) x = first_free_x(grid, md.RS, md.W, ty, rd, tb.run_off, tb.runs);
-    const unsigned fm = __ballot_sync(kFull, x >= 0);
     if (lane == 0) ++c_chunks;
-    if (fm) {
-      const int l = __ffs(fm) - 1;
-      const int xb = __shfl_sync(kFull, x, l);
-      if (lane == 0) {
-        const int tyb = ty_hi - l;
-        atomicMin(&sh.best, key_of(max(enc, md.L - tyb), tyb + rd.h - 1, xb, r));
+    // Vacancy filter one candidate per lane.  Then, when there are few enough
+    // (survivor, output word) pairs, they are dealt to the lanes, bottom-most
+    // survivor and leftmost word first, so lanes whose candidate failed the
+    // filter take part in the exact test of the others, and the first pair
+    // with a free column is the bottom-most candidate's leftmost x.
+    // Otherwise each lane tests its own candidate's words left to right.
+    const bool pass = ty >= 0 && vacancy_ok(vac, ty, rd, tb.dens);
+    const unsigned S = __ballot_sync(kFull, pass);
+    if (!S) continue;
+    const int nx = md.W - rd.w + 1, nwo = (nx + 31) >> 5;
+    const int ntask = __popc(S) * nwo;
+    if (ntask <= task_max) {
+      unsigned char* surv = sh.surv[tid >> 5];
+      if (pass) surv[__popc(S & ((1u << lane) - 1u))] = (unsigned char)lane;
+      __syncwarp();
+      const uint32_t Flast = (nx & 31) ? ((1u << (nx & 31)) - 1u) : kFull;
+      for (int t0 = 0; t0 < ntask; t0 += 32) {
+        const int t = t0 + lane;
+        uint32_t F = 0u;
+        int k = 0, sl = 0;
+        if (t < ntask) {
+          const int si = t / nwo;
+          k = t - si * nwo;
+          sl = surv[si];
+          F = word_free(grid + (size_t)(ty_hi - sl) * md.RS, md.RS, k << 5, k == nwo - 1 ? Flast : kFull, rd,
+                        tb.truns);
+        }
+        const unsigned fm = __ballot_sync(kFull, F != 0u);
+        if (fm) {
+          const int l = __ffs(fm) - 1;
+          const uint32_t Fb = __shfl_sync(kFull, F, l);
+          const int kb = __shfl_sync(kFull, k, l);
+          const int slb = __shfl_sync(kFull, sl, l);
+          if (lane == 0) {
+            const int tyb = ty_hi - slb;
+            atomicMin(&sh.best, key_of(max(enc, md.L - tyb), tyb + rd.h - 1, (kb << 5) + __ffs(Fb) - 1, r));
+          }
+          break;
+        }
+      }
+      __syncwarp();
+    } else {
+      const int x = pass ? first_free_x(grid, md.RS, md.W, ty, rd, tb.truns) : -1;
+      const unsigned fm = __ballot_sync(kFull, x >= 0);
+      if (fm) {
+        const int l = __ffs(fm) - 1;
+        const int xb = __shfl_sync(kFull, x, l);
+        if (lane == 0) {
+          const int tyb = ty_hi - l;
+          atomicMin(&sh.best, key_of(max(enc, md.L - tyb), tyb + rd.h - 1, xb, r));
+        }
       }
     }
   }
@@ -554,8 +633,11 @@ struct ItemCtx {
 
 // The tables go by value (every access has a fixed parameter offset); only
 // the per-launch instance array, which is searched, is a grid constant.
-__global__ void __launch_bounds__(kDecodeThreads) decode_kernel(const Tables tb,
-                                                                const __grid_constant__ Run run) {
+#ifndef BRKGA_DECODE_MINB
+#define BRKGA_DECODE_MINB 8
+#endif
+__global__ void __launch_bounds__(kDecodeThreads, BRKGA_DECODE_MINB) decode_kernel(const Tables tb,
+                                                                                   const __grid_constant__ Run run) {
   extern __shared__ __align__(16) uint32_t smem[];
   __shared__ SearchShared sh;
   __shared__ ItemCtx ctx;
@@ -621,7 +703,7 @@ __global__ void __launch_bounds__(kDecodeThreads) decode_kernel(const Tables tb,
         const uint32_t* grid = b < run.S ? smem + (size_t)b * run.slot_words
                                          : run.pool + (size_t)bs[b].pool * run.slot_words;
         const uint16_t* vac = reinterpret_cast<const uint16_t*>(grid + run.slot_vac_off);
-        key = search_plate(tb, md, grid, vac, bs[b].enc, t, sh, c_tests, c_chunks, c_bytes);
+        key = search_plate(tb, md, grid, vac, bs[b].enc, t, run.task_max, sh, c_tests, c_chunks, c_bytes);
         if (key != kKeyNone) {
           pb = b;
           break;
@@ -767,8 +849,9 @@ __global__ void __launch_bounds__(kDecodeThreads) greedy_kernel(const __grid_con
       for (int b = 0; b < nplates; ++b) {
         if (g.plate_machine[b] != m) continue;
         const uint32_t* grid = g.pool + (size_t)bs[b].pool * g.slot_words;
-        const unsigned long long key = search_plate(tb, md, grid, reinterpret_cast<const uint16_t*>(grid + g.slot_vac_off),
-                                                    bs[b].enc, t, sh, c_tests, c_chunks, c_bytes);
+        const unsigned long long key =
+            search_plate(tb, md, grid, reinterpret_cast<const uint16_t*>(grid + g.slot_vac_off), bs[b].enc, t,
+                         kDefaultTaskMax, sh, c_tests, c_chunks, c_bytes);
         if (key == kKeyNone) continue;
         const double bpth = bs[b].pth;
         const double cand2 = bpth < pthm ? ((mm - bpth) + pthm) + ptm : mm + ptm;  // :486-489
@@ -863,6 +946,7 @@ struct BrkgaProblem {
   int N = 0, M = 0, T = 0, mode = 0;  // instance 0 (the single-instance entry points)
   int sm_count = 0;
   int req_ctas = 0, req_plates = -1;  // requested launch shape (0 / -1 = automatic)
+  int task_max = kDefaultTaskMax;
   int ctas_per_sm = 0;
   int S = 0, slot_words = 0, slot_vac_off = 0;
   int n_slots = 0;
@@ -881,8 +965,7 @@ struct BrkgaProblem {
   int32_t* d_best = nullptr;
   RotDev* d_rot = nullptr;
   uint16_t* d_dens = nullptr;
-  int32_t* d_run_off = nullptr;
-  uint32_t* d_runs = nullptr;
+  uint2* d_truns = nullptr;
   uint32_t* d_maskbits = nullptr;
   uint8_t* d_fits = nullptr;
   uint8_t* d_newbin_ok = nullptr;
@@ -985,11 +1068,13 @@ int configure(BrkgaProblem* pb, int ctas_req, int plates_req) {
   const int slot_vac_off = Lmax * RSmax;
   const int slot_words = (int)align_up((size_t)slot_vac_off + (size_t)(Lmax + 1) / 2, 4);
   const size_t slot_bytes = (size_t)slot_words * 4;
+  cudaFuncAttributes fa;
+  if (cudaFuncGetAttributes(&fa, decode_kernel) != cudaSuccess) return BRKGA_ERR_CUDA;
   const size_t per_sm = prop.sharedMemPerMultiprocessor;
-  const size_t per_block_max = prop.sharedMemPerBlockOptin;
-  const size_t reserve = 1024 + 256;  // per-block system reservation + static shared variables
-  const int max_fit = (int)std::min<size_t>(kMaxSmemPlates, (per_block_max - 256) / slot_bytes);
-  if (cudaFuncSetAttribute(decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(per_block_max - 256)) !=
+  const size_t per_block_max = prop.sharedMemPerBlockOptin - fa.sharedSizeBytes;  // dynamic part
+  const size_t reserve = 1024 + fa.sharedSizeBytes;  // per-block system reservation + static shared variables
+  const int max_fit = (int)std::min<size_t>(kMaxSmemPlates, per_block_max / slot_bytes);
+  if (cudaFuncSetAttribute(decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)per_block_max) !=
       cudaSuccess)
     return BRKGA_ERR_CUDA;
   if (cudaFuncSetAttribute(assign_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxGenes * 8) !=
@@ -1091,8 +1176,8 @@ struct Merged {
   std::vector<double> thr, pt, pth, area, bin_area;
   std::vector<RotDev> rot;
   std::vector<uint16_t> dens;
-  std::vector<int32_t> run_off;
-  std::vector<uint32_t> runs, maskbits;
+  std::vector<uint2> truns;
+  std::vector<uint32_t> maskbits;
   std::vector<uint8_t> fits, newbin_ok;
   std::vector<MachDev> mach;
 };
@@ -1121,18 +1206,17 @@ void merge_instance(const BrkgaProblemDesc* d, Merged& g) {
         rd.w = w;
         rd.mw = (w + 31) / 32;
         rd.dens_row = (int)g.dens.size();
-        rd.run_row = (int)g.run_off.size();
         rd.mask_base = (int)g.maskbits.size();
         rd.imax = 0;
         rd.dmax = 0;
+        std::vector<std::vector<uint32_t>> row_runs(h);
         for (int i = 0; i < h; ++i) {
-          g.run_off.push_back((int32_t)g.runs.size());
           int best = 0, j = 0;
           while (j < w) {
             if (mk[(size_t)i * w + j]) {
               const int s = j;
               while (j < w && mk[(size_t)i * w + j]) ++j;
-              g.runs.push_back((uint32_t)s | ((uint32_t)(j - s) << 16));
+              row_runs[i].push_back((uint32_t)s | ((uint32_t)(j - s) << 16));
               best = std::max(best, j - s);
             } else {
               ++j;
@@ -1150,7 +1234,15 @@ void merge_instance(const BrkgaProblemDesc* d, Merged& g) {
             g.maskbits.push_back(v);
           }
         }
-        g.run_off.push_back((int32_t)g.runs.size());
+        // collision-test order: the widest row, then the others bottom to top
+        // (plates fill from the bottom, so those rows reject soonest)
+        rd.trun = (int)g.truns.size();
+        for (int ii = -1; ii < h; ++ii) {
+          const int i = ii < 0 ? rd.imax : h - 1 - ii;
+          if (ii >= 0 && i == rd.imax) continue;
+          for (uint32_t r : row_runs[i]) g.truns.push_back(make_uint2(r, (unsigned)i));
+        }
+        rd.ntrun = (int)g.truns.size() - rd.trun;
       }
       g.rot.push_back(rd);
     }
@@ -1215,6 +1307,7 @@ int fill_run(const BrkgaProblem* pb, const int32_t* pops, const int64_t* chrom_o
   run->S = pb->S;
   run->slot_words = pb->slot_words;
   run->slot_vac_off = pb->slot_vac_off;
+  run->task_max = pb->task_max;
   int64_t row = 0, item = 0, seq = 0, chrom = 0;
   for (int k = 0; k < pb->K; ++k) {
     const InstDev& id = pb->inst[k];
@@ -1318,7 +1411,7 @@ int brkga_problem_create_multi(const BrkgaProblemDesc* descs, int32_t K, BrkgaPr
   }
   Merged g;
   for (int k = 0; k < K; ++k) merge_instance(&descs[k], g);
-  if (g.maskbits.size() >= ((size_t)1 << 31) || g.runs.size() >= ((size_t)1 << 31)) return BRKGA_ERR_BAD_INSTANCE;
+  if (g.maskbits.size() >= ((size_t)1 << 31) || g.truns.size() >= ((size_t)1 << 31)) return BRKGA_ERR_BAD_INSTANCE;
   BrkgaProblem* pb = new BrkgaProblem();
   cudaGetDevice(&pb->device);
   pb->K = K;
@@ -1342,8 +1435,8 @@ int brkga_problem_create_multi(const BrkgaProblemDesc* descs, int32_t K, BrkgaPr
       (st = upload(pb, &pb->d_pt, g.pt)) || (st = upload(pb, &pb->d_pth, g.pth)) ||
       (st = upload(pb, &pb->d_area, g.area)) || (st = upload(pb, &pb->d_nrot, g.nrot)) ||
       (st = upload(pb, &pb->d_best, g.best)) || (st = upload(pb, &pb->d_rot, g.rot)) ||
-      (st = upload(pb, &pb->d_dens, g.dens)) || (st = upload(pb, &pb->d_run_off, g.run_off)) ||
-      (st = upload(pb, &pb->d_runs, g.runs)) || (st = upload(pb, &pb->d_maskbits, g.maskbits)) ||
+      (st = upload(pb, &pb->d_dens, g.dens)) || (st = upload(pb, &pb->d_truns, g.truns)) ||
+      (st = upload(pb, &pb->d_maskbits, g.maskbits)) ||
       (st = upload(pb, &pb->d_fits, g.fits)) || (st = upload(pb, &pb->d_newbin_ok, g.newbin_ok)) ||
       (st = upload(pb, &pb->d_bin_area, g.bin_area)) || (st = configure(pb, 0, -1))) {
     brkga_problem_destroy(pb);
@@ -1361,8 +1454,7 @@ int brkga_problem_create_multi(const BrkgaProblemDesc* descs, int32_t K, BrkgaPr
   tb.best_rot = pb->d_best;
   tb.rot = pb->d_rot;
   tb.dens = pb->d_dens;
-  tb.run_off = pb->d_run_off;
-  tb.runs = pb->d_runs;
+  tb.truns = pb->d_truns;
   tb.maskbits = pb->d_maskbits;
   tb.newbin_ok = pb->d_newbin_ok;
   tb.fits = pb->d_fits;
@@ -1387,22 +1479,28 @@ int brkga_problem_instances(const BrkgaProblem* pb, int32_t* K) {
   return BRKGA_OK;
 }
 
-int brkga_set_launch_config(BrkgaProblem* pb, int32_t ctas_per_sm, int32_t smem_plates) {
-  if (!pb || ctas_per_sm < 0 || ctas_per_sm > kMaxCtasPerSm || smem_plates < -1 || smem_plates > kMaxSmemPlates)
+int brkga_set_launch_config(BrkgaProblem* pb, int32_t ctas_per_sm, int32_t smem_plates, int32_t task_max) {
+  if (!pb || ctas_per_sm < 0 || ctas_per_sm > kMaxCtasPerSm || smem_plates < -1 || smem_plates > kMaxSmemPlates ||
+      task_max < -1 || task_max > kMaxTaskMax)
     return BRKGA_ERR_INVALID_ARGUMENT;
   DeviceGuard g(pb->device);
   const int old_ctas = pb->req_ctas, old_plates = pb->req_plates;
   const int st = configure(pb, ctas_per_sm, smem_plates);
-  if (st) configure(pb, old_ctas, old_plates);
-  return st;
+  if (st) {
+    configure(pb, old_ctas, old_plates);
+    return st;
+  }
+  pb->task_max = task_max < 0 ? kDefaultTaskMax : task_max;
+  return BRKGA_OK;
 }
 
 int brkga_get_launch_config(const BrkgaProblem* pb, int32_t* ctas_per_sm, int32_t* smem_plates,
-                            int32_t* resident_ctas) {
+                            int32_t* resident_ctas, int32_t* task_max) {
   if (!pb) return BRKGA_ERR_INVALID_ARGUMENT;
   if (ctas_per_sm) *ctas_per_sm = pb->ctas_per_sm;
   if (smem_plates) *smem_plates = pb->S;
   if (resident_ctas) *resident_ctas = pb->n_slots;
+  if (task_max) *task_max = pb->task_max;
   return BRKGA_OK;
 }
 

@@ -40,13 +40,14 @@ class _NativeProblem:
         self.handle = handle
 
     def launch_config(self):
-        """(CTAs per SM, plates per item in shared memory, resident CTAs) of the decode kernel."""
-        c, s, r = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
-        abi.check(self.lib.brkga_get_launch_config(self.handle, ctypes.byref(c), ctypes.byref(s), ctypes.byref(r)))
-        return c.value, s.value, r.value
+        """(CTAs per SM, plates per item in shared memory, resident CTAs, task_max) of the decode kernel."""
+        c, s, r, t = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        abi.check(self.lib.brkga_get_launch_config(self.handle, ctypes.byref(c), ctypes.byref(s), ctypes.byref(r),
+                                                   ctypes.byref(t)))
+        return c.value, s.value, r.value, t.value
 
-    def set_launch_config(self, ctas_per_sm: int, smem_plates: int):
-        abi.check(self.lib.brkga_set_launch_config(self.handle, int(ctas_per_sm), int(smem_plates)),
+    def set_launch_config(self, ctas_per_sm: int, smem_plates: int, task_max: int = -1):
+        abi.check(self.lib.brkga_set_launch_config(self.handle, int(ctas_per_sm), int(smem_plates), int(task_max)),
                   "brkga_set_launch_config")
 
     def close(self):
@@ -175,13 +176,13 @@ class DeviceDecoder:
         return nbytes.value
 
     def launch_config(self):
-        """(CTAs per SM, plates per item in shared memory, resident CTAs) of the decode kernel."""
+        """(CTAs per SM, plates per item in shared memory, resident CTAs, task_max) of the decode kernel."""
         return self.native.launch_config()
 
-    def set_launch_config(self, ctas_per_sm: int, smem_plates: int):
-        """Change the decode kernel's launch shape (0 / -1 = automatic) and
-        regrow the workspace when the new shape needs more."""
-        self.native.set_launch_config(ctas_per_sm, smem_plates)
+    def set_launch_config(self, ctas_per_sm: int, smem_plates: int, task_max: int = -1):
+        """Change the decode kernel's launch configuration (0 / -1 / -1 =
+        automatic) and regrow the workspace when the new shape needs more."""
+        self.native.set_launch_config(ctas_per_sm, smem_plates, task_max)
         need = self.workspace_bytes(self.max_pop)
         if need > self.ws_bytes:
             self.workspace = self.torch.empty(need, dtype=self.torch.uint8, device=self.device)
@@ -274,8 +275,8 @@ class MultiDecoder:
     def launch_config(self):
         return self.native.launch_config()
 
-    def set_launch_config(self, ctas_per_sm: int, smem_plates: int):
-        self.native.set_launch_config(ctas_per_sm, smem_plates)
+    def set_launch_config(self, ctas_per_sm: int, smem_plates: int, task_max: int = -1):
+        self.native.set_launch_config(ctas_per_sm, smem_plates, task_max)
         need = self.workspace_bytes(self.max_pops)
         if need > self.ws_bytes:
             self.workspace = self.torch.empty(need, dtype=self.torch.uint8, device=self.device)

@@ -206,18 +206,24 @@ int brkga_decode_multi_at(int32_t stage, const BrkgaProblem* problem, const floa
 
 /* Launch shape of the decode kernel (the autotuner's knobs; no reference
  * counterpart): ctas_per_sm resident CTAs of 4 warps per SM (1..32, 0 =
- * automatic) and smem_plates plates of each item kept in shared memory
- * (0..8, the rest in the global pool; -1 = as many as fit, at most 4).
- * A shape that cannot be resident is refused with BRKGA_ERR_INVALID_ARGUMENT
- * and the previous one kept.  The workspace size depends on the shape: query
+ * automatic), smem_plates plates of each item kept in shared memory (0..8,
+ * the rest in the global pool; -1 = as many as fit, at most 4), and task_max
+ * (0..8192, -1 = the default 512): a warp that tests 32 candidate rows deals
+ * the (candidate that passed the vacancy filter, 32-column output word) pairs
+ * across its lanes when there are at most task_max of them, else each lane
+ * tests its own candidate.  Results never depend on these knobs.  A shape that
+ * cannot be resident is refused with BRKGA_ERR_INVALID_ARGUMENT and the
+ * previous one kept.  The workspace size depends on the shape: query
  * brkga_workspace_bytes again after a change.  Not to be called while a
  * decode of this problem is being launched from another thread. */
-int brkga_set_launch_config(BrkgaProblem* problem, int32_t ctas_per_sm, int32_t smem_plates);
+int brkga_set_launch_config(BrkgaProblem* problem, int32_t ctas_per_sm, int32_t smem_plates,
+                            int32_t task_max);
 
-/* The shape in use: CTAs per SM, plates per item in shared memory, and the
- * decode kernel's grid (SMs x CTAs per SM); any output may be NULL. */
+/* The configuration in use: CTAs per SM, plates per item in shared memory,
+ * the decode kernel's grid (SMs x CTAs per SM) and task_max; any output may
+ * be NULL. */
 int brkga_get_launch_config(const BrkgaProblem* problem, int32_t* ctas_per_sm, int32_t* smem_plates,
-                            int32_t* resident_ctas);
+                            int32_t* resident_ctas, int32_t* task_max);
 
 /* Host-to-host evaluation, the drop-in for NativeFullDecoder::evaluate_batch
  * (full_native_decoder.py:563-641): copies h_chrom [P, 2N] float32 to the

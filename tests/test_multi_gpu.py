@@ -64,15 +64,16 @@ def test_uneven_instances_match_oracle(multi):
     _check(md, POPS, out, log, ref)
 
 
-@pytest.mark.parametrize("shape", [(1, 0), (2, 1), (4, -1), (8, 0), (0, 0), (0, -1)])
-def test_launch_shapes_give_identical_results(multi, shape):
+@pytest.mark.parametrize("cfg", [(1, 0, -1), (2, 1, 0), (4, -1, 64), (8, 0, 8192), (0, 0, 1), (0, -1, -1)])
+def test_launch_configs_give_identical_results(multi, cfg):
     torch, insts, packs, chroms, ref, md = multi
-    md.set_launch_config(*shape)
-    ctas, plates, grid = md.launch_config()
-    if shape[0]:
-        assert ctas == shape[0]
-    if shape[1] >= 0:
-        assert plates == shape[1]
+    md.set_launch_config(*cfg)
+    ctas, plates, grid, task_max = md.launch_config()
+    if cfg[0]:
+        assert ctas == cfg[0]
+    if cfg[1] >= 0:
+        assert plates == cfg[1]
+    assert task_max == (cfg[2] if cfg[2] >= 0 else 512)
     out, log = _run(torch, md, chroms, POPS)
     _check(md, POPS, out, log, ref)
     md.set_launch_config(0, -1)
