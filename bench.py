@@ -272,7 +272,7 @@ def run_ours(args):
                                  "and rotated mask, 4*(L*ceil(W/32)+h*ceil(w/32))"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": P * 2 * N * 4,
                     "d2h_bytes_per_step": P * 8, "matches_device_path": same},
-            "gpu_launches": 3 * args.steps,
+            "gpu_launches": 4 * args.steps,  # assign_sort, order_items, decode, reduce per step
             "kernel_share": statistics.mean(kern_ms) / statistics.mean(step_ms),
             "counters_last_step": {"tests": tests, "row_chunks": chunks, "plates": bins},
             "status": status,

@@ -1052,10 +1052,10 @@ class DeviceGuard {
 };
 
 // Shared-memory plate slots and resident CTAs per SM of the decode kernel.
-// ctas_req = 0 picks the shape automatically (aim at 8 resident items per
-// SM, fewer when one plate does not fit that share of shared memory; at most
-// 4 plates per item in shared memory); plates_req = -1 keeps as many plates
-// as fit (at most 4).  An explicit shape that cannot be resident is refused.
+// ctas_req = 0 picks the shape automatically (8 resident items per SM, at
+// most 4 plates per item in shared memory); plates_req = -1 keeps as many
+// plates as fit (at most 4).  An explicit shape that cannot be resident is
+// refused.
 int configure(BrkgaProblem* pb, int ctas_req, int plates_req) {
   cudaDeviceProp prop;
   if (cudaGetDeviceProperties(&prop, pb->device) != cudaSuccess) return BRKGA_ERR_CUDA;
@@ -1095,15 +1095,11 @@ int configure(BrkgaProblem* pb, int ctas_req, int plates_req) {
       ctas = 8;
       while (ctas > 1 && fit_for(ctas) < S) --ctas;
     } else {
-      for (ctas = 8; ctas >= 1; --ctas) {
-        S = fit_for(ctas);
-        if (S >= 1) break;
-      }
-      if (S < 1) {  // plates larger than shared memory: all of them in the global pool
-        S = 0;
-        ctas = 8;
-      }
-      S = std::min(S, 4);
+      // Resident warps matter far more than where the plates live (the pool
+      // stays in L2): 8 CTAs, and as many plates per item in shared memory
+      // as their share holds (none for plates above ~27 KB).
+      ctas = 8;
+      S = std::min(fit_for(ctas), 4);
     }
   } else {
     ctas = ctas_req;
