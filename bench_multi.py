@@ -76,7 +76,7 @@ def main():
     counters = md.counters()
 
     ga = MultiBRKGA(packs, num_generations=G, num_individuals=P, eliteCProb=0.7, seed=args.seed,
-                    launch_config=(shape[0], shape[1], shape[3]) if tune else None)
+                    launch_config=(shape[0], shape[1], shape[2], shape[4]) if tune else None)
     t0 = time.perf_counter()
     ga.prepare()
     prep_s = time.perf_counter() - t0
@@ -102,8 +102,8 @@ def main():
         "one_launch": {"rows": K * P, "ms": launch_ms, "decode_kernel_ms": kernel_ms,
                        "decodes_per_s": K * P / (launch_ms / 1000.0),
                        "placement_tests": counters[0], "plates": counters[2]},
-        "launch_config": {"ctas_per_sm": shape[0], "smem_plates": shape[1], "resident_ctas": shape[2],
-                          "task_max": shape[3]},
+        "launch_config": {"warps_per_item": shape[0], "ctas_per_sm": shape[1], "smem_plates": shape[2],
+                          "resident_ctas": shape[3], "task_max": shape[4]},
         "autotune": None if tune is None else {"table": tune["table"], "cached": tune["cached"]},
         "sample_exact": f"{n_ok}/{n_chk}",
         "parts": [i.nb_parts for i in insts], "machines": [i.nb_machines for i in insts],

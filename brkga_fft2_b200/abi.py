@@ -146,8 +146,8 @@ def load_library(path: str = LIB_PATH):
         "brkga_decode_multi_stage": (c_int, [c_i32, vp, vp, P(c_i32), vp, vp, vp, vp, c_sz, c_i64, vp]),
         "brkga_decode_multi_at": (c_int, [c_i32, vp, vp, P(c_i64), P(c_i32), vp, P(c_i64), vp, vp, vp, c_sz, c_i64,
                                           vp]),
-        "brkga_set_launch_config": (c_int, [vp, c_i32, c_i32, c_i32]),
-        "brkga_get_launch_config": (c_int, [vp, P(c_i32), P(c_i32), P(c_i32), P(c_i32)]),
+        "brkga_set_launch_config": (c_int, [vp, c_i32, c_i32, c_i32, c_i32]),
+        "brkga_get_launch_config": (c_int, [vp, c_i64, P(c_i32), P(c_i32), P(c_i32), P(c_i32), P(c_i32)]),
         "brkga_evaluate_host": (c_int, [vp, P(ctypes.c_float), c_i32, P(ctypes.c_double), vp]),
         "brkga_last_counters": (c_int, [vp, P(c_i64), P(c_i64), P(c_i64), P(c_i64)]),
     }

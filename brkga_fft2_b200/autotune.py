@@ -1,11 +1,14 @@
 """Launch-shape autotuner for the decode kernel.
 
-The decode kernel has three knobs (``brkga_set_launch_config``).  Two trade
-against each other: more resident CTAs per SM hide more latency, more plates
-per item in shared memory keep more collision searches off the global pool,
-and both draw on the same 228 KB of shared memory per SM, whose share per
-plate grows with the plate grid (a 500 x 500 plate is 36 KB as bit-packed
-rows, a 150 x 150 one 3.6 KB).  The third, ``task_max``, decides when a warp
+The decode kernel has four knobs (``brkga_set_launch_config``).  Warps per
+item (2 or 4) trade the latency of one (chromosome, machine) item against
+throughput: 4 finish an item sooner, 2 waste fewer lanes on speculative row
+chunks, so 2 win once the items fill several waves of resident CTAs.  More
+resident CTAs per SM hide more latency, more plates per item in shared
+memory keep more collision searches off the global pool, and both draw on
+the same 228 KB of shared memory per SM, whose share per plate grows with
+the plate grid (a 500 x 500 plate is 36 KB as bit-packed rows, a 150 x 150
+one 3.6 KB).  The fourth, ``task_max``, decides when a warp
 deals (candidate row, 32-column word) pairs of the exact collision test
 across its lanes instead of giving each lane one candidate row: dealing wins
 while the pairs are few, loses on wide plates with many surviving candidates
@@ -29,7 +32,9 @@ import numpy as np
 
 from . import abi
 
-DEFAULT_SHAPES: Tuple[Tuple[int, int], ...] = tuple((c, s) for c in (2, 4, 6, 8) for s in (0, 1, 2, 4))
+# (warps per item, CTAs per SM, plates per item in shared memory)
+DEFAULT_SHAPES: Tuple[Tuple[int, int, int], ...] = ((4, 8, 0), (4, 8, 1), (4, 8, 2), (4, 6, 1), (4, 6, 2),
+                                                    (2, 16, 0), (2, 16, 1), (2, 12, 1), (2, 12, 2), (2, 8, 2))
 DEFAULT_TASK_MAX: Tuple[int, ...] = (0, 64, 256, 1024, 8192)
 
 
@@ -58,17 +63,18 @@ def _time_decode(decoder, run, repeats: int) -> float:
     return float(np.median(times[1:]))
 
 
-def autotune(decoder, chrom, pops=None, shapes: Optional[Iterable[Tuple[int, int]]] = None,
+def autotune(decoder, chrom, pops=None, shapes: Optional[Iterable[Tuple[int, int, int]]] = None,
              task_max_values: Optional[Iterable[int]] = None, repeats: int = 2, cache_path: Optional[str] = None,
              key: Optional[str] = None) -> dict:
     """Pick the fastest decode-kernel configuration for ``decoder``.
 
     ``decoder`` is a ``DeviceDecoder`` (``chrom``: float32 CUDA [P, 2N]) or a
     ``MultiDecoder`` (``chrom``: the flat concatenated rows, ``pops``: rows per
-    instance).  Shapes that cannot be resident are skipped.  Returns
-    ``{"key", "config": (ctas_per_sm, smem_plates, task_max), "ms", "table":
-    [(ctas_per_sm, smem_plates, task_max, ms), ...], "cached"}`` and leaves the
-    decoder on the chosen configuration.
+    instance).  ``shapes`` are (warps per item, CTAs per SM, plates in shared
+    memory) triples; those that cannot be resident are skipped.  Returns
+    ``{"key", "config": (warps, ctas_per_sm, smem_plates, task_max), "ms",
+    "table": [(warps, ctas_per_sm, smem_plates, task_max, ms), ...],
+    "cached"}`` and leaves the decoder on the chosen configuration.
     """
     import torch
     packs = decoder.packs if hasattr(decoder, "packs") else [decoder.packed]
@@ -78,9 +84,9 @@ def autotune(decoder, chrom, pops=None, shapes: Optional[Iterable[Tuple[int, int
         with open(cache_path) as f:
             cache = json.load(f)
     if key in cache:
-        c, s, t = cache[key]["config"]
-        decoder.set_launch_config(c, s, t)
-        return {"key": key, "config": (c, s, t), "ms": cache[key]["ms"], "table": cache[key]["table"],
+        w, c, s, t = cache[key]["config"]
+        decoder.set_launch_config(w, c, s, t)
+        return {"key": key, "config": (w, c, s, t), "ms": cache[key]["ms"], "table": cache[key]["table"],
                 "cached": True}
 
     if pops is None:
@@ -92,31 +98,31 @@ def autotune(decoder, chrom, pops=None, shapes: Optional[Iterable[Tuple[int, int
     reference = []
     table = []
 
-    def trial(c, s, t):
+    def trial(w, c, s, t):
         try:
-            decoder.set_launch_config(c, s, t)
+            decoder.set_launch_config(w, c, s, t)
         except abi.BrkgaError:
             return
         ms = _time_decode(decoder, run, repeats)
         if not reference:
             reference.append(out.clone())
         elif not torch.equal(out, reference[0]):
-            raise RuntimeError(f"launch configuration {(c, s, t)} changed the makespans")
-        table.append((c, s, t, ms))
+            raise RuntimeError(f"launch configuration {(w, c, s, t)} changed the makespans")
+        table.append((w, c, s, t, ms))
 
-    for c, s in (shapes or DEFAULT_SHAPES):
-        trial(c, s, -1)
+    for w, c, s in (shapes or DEFAULT_SHAPES):
+        trial(w, c, s, -1)
     if not table:
         raise RuntimeError("no launch shape could be resident")
-    c, s, _, _ = min(table, key=lambda r: r[3])
+    w, c, s, _, _ = min(table, key=lambda r: r[4])
     for t in (task_max_values if task_max_values is not None else DEFAULT_TASK_MAX):
-        trial(c, s, t)
-    c, s, t, ms = min(table, key=lambda r: r[3])
-    decoder.set_launch_config(c, s, t)
-    t = decoder.launch_config()[3]
+        trial(w, c, s, t)
+    w, c, s, t, ms = min(table, key=lambda r: r[4])
+    decoder.set_launch_config(w, c, s, t)
+    t = decoder.launch_config()[4]
     if cache_path:
-        cache[key] = {"config": [c, s, t], "ms": ms, "table": table}
+        cache[key] = {"config": [w, c, s, t], "ms": ms, "table": table}
         os.makedirs(os.path.dirname(os.path.abspath(cache_path)), exist_ok=True)
         with open(cache_path, "w") as f:
             json.dump(cache, f, indent=1, sort_keys=True)
-    return {"key": key, "config": (c, s, t), "ms": ms, "table": table, "cached": False}
+    return {"key": key, "config": (w, c, s, t), "ms": ms, "table": table, "cached": False}

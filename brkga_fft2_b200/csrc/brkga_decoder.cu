@@ -50,7 +50,9 @@ namespace {
 constexpr int kMaxMachines = 255;
 constexpr int kMaxGenes = 8192;     // bitonic sort buffer: 8192 x 8 B = 64 KB shared memory
 constexpr int kMaxSide = 8191;      // 13-bit fields of the selection key
-constexpr int kDecodeThreads = 128; // 4 warps per item
+constexpr int kMaxItemWarps = 4;   // decode CTAs have 2 or 4 warps (one item per CTA)
+constexpr int kGreedyThreads = 128;
+constexpr int kResidentWarps = 32;  // automatic shape: 32 warps per SM (the register limit at 64 per thread)
 constexpr int kMaxInst = BRKGA_MAX_INSTANCES;
 constexpr int kMaxCtasPerSm = 32;
 constexpr int kMaxSmemPlates = 8;
@@ -447,7 +449,7 @@ struct SearchShared {
   unsigned long long best;
   int chunk, total, nr;
   int rlist[4];
-  unsigned char surv[kDecodeThreads / 32][32];  // per warp: lanes whose candidate passed the vacancy filter
+  unsigned char surv[kMaxItemWarps][32];  // per warp: lanes whose candidate passed the vacancy filter
 };
 
 // Best placement key of part type t (absolute) on one plate (kKeyNone if it
@@ -569,7 +571,7 @@ __device__ __forceinline__ void place_part(const Tables& tb, const MachDev& md, 
   const RotDev rd = tb.rot[t * 4 + r];
   const int sx = x & 31, wx = x >> 5, span = rd.mw + 1;
   const uint32_t* mb = tb.maskbits + rd.mask_base;
-  for (int idx = tid; idx < rd.h * span; idx += kDecodeThreads) {
+  for (int idx = tid; idx < rd.h * span; idx += blockDim.x) {
     const int i = idx / span, j = idx - i * span;
     const uint32_t lo = j > 0 ? __ldg(mb + i * rd.mw + j - 1) : 0u;
     const uint32_t hi = j < rd.mw ? __ldg(mb + i * rd.mw + j) : 0u;
@@ -577,7 +579,7 @@ __device__ __forceinline__ void place_part(const Tables& tb, const MachDev& md, 
     if (v) grid[(size_t)(ty + i) * md.RS + wx + j] |= v;
   }
   __syncthreads();
-  for (int i = tid; i < rd.h; i += kDecodeThreads)
+  for (int i = tid; i < rd.h; i += blockDim.x)
     vac[ty + i] = (uint16_t)max_zero_run(grid + (size_t)(ty + i) * md.RS, md.W, md.NW);
   if (tid == 0) {
     BinScal s = *scal;
@@ -596,8 +598,8 @@ __device__ __forceinline__ void place_part(const Tables& tb, const MachDev& md, 
 __device__ __forceinline__ void open_plate(const MachDev& md, uint32_t* grid, uint16_t* vac, BinScal* scal,
                                            int pool_index) {
   const int tid = threadIdx.x;
-  for (int i = tid; i < md.L * md.RS; i += kDecodeThreads) grid[i] = 0u;
-  for (int i = tid; i < md.L; i += kDecodeThreads) vac[i] = (uint16_t)md.W;
+  for (int i = tid; i < md.L * md.RS; i += blockDim.x) grid[i] = 0u;
+  for (int i = tid; i < md.L; i += blockDim.x) vac[i] = (uint16_t)md.W;
   if (tid == 0) {
     BinScal z;
     z.area = 0.0;
@@ -633,11 +635,11 @@ struct ItemCtx {
 
 // The tables go by value (every access has a fixed parameter offset); only
 // the per-launch instance array, which is searched, is a grid constant.
-#ifndef BRKGA_DECODE_MINB
-#define BRKGA_DECODE_MINB 8
-#endif
-__global__ void __launch_bounds__(kDecodeThreads, BRKGA_DECODE_MINB) decode_kernel(const Tables tb,
-                                                                                   const __grid_constant__ Run run) {
+// kThreads = 64 or 128 (2 or 4 warps per item); 32 resident warps per SM
+// cap the kernel at 64 registers, which it fits without spilling.
+template <int kThreads>
+__global__ void __launch_bounds__(kThreads, kResidentWarps * 32 / kThreads)
+    decode_kernel(const Tables tb, const __grid_constant__ Run run) {
   extern __shared__ __align__(16) uint32_t smem[];
   __shared__ SearchShared sh;
   __shared__ ItemCtx ctx;
@@ -680,13 +682,13 @@ __global__ void __launch_bounds__(kDecodeThreads, BRKGA_DECODE_MINB) decode_kern
     const int N = ctx.N;
     if (ctx.infeas) {  // any part too large for its machine: the whole chromosome scores 1e16
       if (lg)
-        for (int k = tid; k < N; k += kDecodeThreads) lg[k] = BrkgaPlacement{-1, -1, -1, -1, -1};
+        for (int k = tid; k < N; k += kThreads) lg[k] = BrkgaPlacement{-1, -1, -1, -1, -1};
       if (tid == 0) run.mk[item] = 0.0;
       __syncthreads();
       continue;
     }
     if (lg)
-      for (int k = n + tid; k < N; k += kDecodeThreads) lg[k] = BrkgaPlacement{-1, -1, -1, -1, -1};
+      for (int k = n + tid; k < N; k += kThreads) lg[k] = BrkgaPlacement{-1, -1, -1, -1, -1};
 
     int nb = 0;
     bool failed = false;
@@ -813,7 +815,7 @@ struct GreedyArgs {
   double* machine_makespan;  // [M]
 };
 
-__global__ void __launch_bounds__(kDecodeThreads) greedy_kernel(const __grid_constant__ Tables tb,
+__global__ void __launch_bounds__(kGreedyThreads) greedy_kernel(const __grid_constant__ Tables tb,
                                                                 const __grid_constant__ GreedyArgs g) {
   __shared__ SearchShared sh;
   __shared__ int s_fail;
@@ -822,7 +824,7 @@ __global__ void __launch_bounds__(kDecodeThreads) greedy_kernel(const __grid_con
   unsigned long long c_tests = 0, c_chunks = 0, c_bytes = 0;
   int nplates = 0;
   double cw = 0.0;  // current_worst_makespan
-  for (int m = tid; m < g.M; m += kDecodeThreads) g.machine_makespan[m] = 0.0;
+  for (int m = tid; m < g.M; m += kGreedyThreads) g.machine_makespan[m] = 0.0;
   __syncthreads();
   for (int k = 0; k < g.n; ++k) {
     const int gene = g.order[k];
@@ -929,6 +931,15 @@ struct LaunchCounts {
   int64_t rows = 0, items = 0, seq = 0;
 };
 
+// One launch shape of the decode kernel.
+struct Shape {
+  int warps = 4;     // per CTA (one item per CTA)
+  int ctas = 0;      // resident CTAs per SM
+  int S = 0;         // plates per item in shared memory
+  size_t smem = 0;   // dynamic shared memory per CTA
+  int n_slots = 0;   // resident CTAs on the GPU (the persistent grid)
+};
+
 }  // namespace
 
 // Fixed device scratch for brkga_decode_noalloc: every GPU that loads this
@@ -945,12 +956,12 @@ struct BrkgaProblem {
   int S2max = 1, Nmax = 0;
   int N = 0, M = 0, T = 0, mode = 0;  // instance 0 (the single-instance entry points)
   int sm_count = 0;
-  int req_ctas = 0, req_plates = -1;  // requested launch shape (0 / -1 = automatic)
+  int req_warps = 0, req_ctas = 0, req_plates = -1;  // requested launch shape (0 / 0 / -1 = automatic)
   int task_max = kDefaultTaskMax;
-  int ctas_per_sm = 0;
-  int S = 0, slot_words = 0, slot_vac_off = 0;
-  int n_slots = 0;
-  size_t decode_smem = 0;
+  Shape shape[2];      // 4 and 2 warps per item
+  int max_slots = 0;   // resident CTAs of the larger shape (per-CTA plate scalars in the workspace)
+  int min_S = 0;       // fewer plates in shared memory of the two shapes (pool sizing)
+  int slot_words = 0, slot_vac_off = 0;
   std::vector<MachDev> mach;
   std::vector<void*> allocations;
   Tables tb{};
@@ -1016,7 +1027,7 @@ Layout layout_of(const BrkgaProblem* pb, const LaunchCounts& lc, int64_t pool_bi
   l.off_mk = o = align_up(o, 256);
   o += (size_t)lc.items * sizeof(double);
   l.off_bins = o = align_up(o, 256);
-  o += (size_t)pb->n_slots * std::max(pb->Nmax, 1) * sizeof(BinScal);
+  o += (size_t)pb->max_slots * std::max(pb->Nmax, 1) * sizeof(BinScal);
   l.off_pool = o = align_up(o, 256);
   o += (size_t)pool_bins * pb->slot_words * sizeof(uint32_t);
   l.total = align_up(o, 256);
@@ -1024,7 +1035,7 @@ Layout layout_of(const BrkgaProblem* pb, const LaunchCounts& lc, int64_t pool_bi
 }
 
 int64_t default_pool_bins(const BrkgaProblem* pb, int64_t items) {
-  return std::max<int64_t>(256, items * (pb->S > 0 ? 2 : 4));
+  return std::max<int64_t>(256, items * (pb->min_S > 0 ? 2 : 4));
 }
 
 template <typename T>
@@ -1051,12 +1062,29 @@ class DeviceGuard {
   int prev_ = 0;
 };
 
-// Shared-memory plate slots and resident CTAs per SM of the decode kernel.
-// ctas_req = 0 picks the shape automatically (8 resident items per SM, at
-// most 4 plates per item in shared memory); plates_req = -1 keeps as many
-// plates as fit (at most 4).  An explicit shape that cannot be resident is
-// refused.
-int configure(BrkgaProblem* pb, int ctas_req, int plates_req) {
+template <int kThreads>
+int prepare_kernel(size_t dyn_max) {
+  return cudaFuncSetAttribute(decode_kernel<kThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_max) ==
+                 cudaSuccess
+             ? BRKGA_OK
+             : BRKGA_ERR_CUDA;
+}
+
+int occupancy(int warps, size_t smem, int* occ) {
+  const cudaError_t e = warps == 2 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, decode_kernel<64>, 64, smem)
+                                   : cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, decode_kernel<128>, 128, smem);
+  return e == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
+}
+
+// Launch shapes of the decode kernel, one per CTA size (4 and 2 warps per
+// item): resident CTAs per SM and plates per item kept in shared memory.
+// For the requested CTA size (warps_req), ctas_req = 0 picks the CTAs
+// automatically (32 resident warps per SM, the register limit) and
+// plates_req = -1 keeps as many plates as fit in their share (at most 4);
+// the other CTA size, or both when warps_req = 0, gets the automatic shape.
+// A requested shape that cannot be resident is refused.
+int configure(BrkgaProblem* pb, int warps_req, int ctas_req, int plates_req) {
+  if (warps_req == 0 && (ctas_req != 0 || plates_req != -1)) return BRKGA_ERR_INVALID_ARGUMENT;
   cudaDeviceProp prop;
   if (cudaGetDeviceProperties(&prop, pb->device) != cudaSuccess) return BRKGA_ERR_CUDA;
   pb->sm_count = prop.multiProcessorCount;
@@ -1068,15 +1096,17 @@ int configure(BrkgaProblem* pb, int ctas_req, int plates_req) {
   const int slot_vac_off = Lmax * RSmax;
   const int slot_words = (int)align_up((size_t)slot_vac_off + (size_t)(Lmax + 1) / 2, 4);
   const size_t slot_bytes = (size_t)slot_words * 4;
-  cudaFuncAttributes fa;
-  if (cudaFuncGetAttributes(&fa, decode_kernel) != cudaSuccess) return BRKGA_ERR_CUDA;
-  const size_t per_sm = prop.sharedMemPerMultiprocessor;
-  const size_t per_block_max = prop.sharedMemPerBlockOptin - fa.sharedSizeBytes;  // dynamic part
-  const size_t reserve = 1024 + fa.sharedSizeBytes;  // per-block system reservation + static shared variables
-  const int max_fit = (int)std::min<size_t>(kMaxSmemPlates, per_block_max / slot_bytes);
-  if (cudaFuncSetAttribute(decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)per_block_max) !=
-      cudaSuccess)
+  cudaFuncAttributes fa4, fa2;
+  if (cudaFuncGetAttributes(&fa4, decode_kernel<128>) != cudaSuccess ||
+      cudaFuncGetAttributes(&fa2, decode_kernel<64>) != cudaSuccess)
     return BRKGA_ERR_CUDA;
+  const size_t static_smem = std::max(fa4.sharedSizeBytes, fa2.sharedSizeBytes);
+  const size_t per_sm = prop.sharedMemPerMultiprocessor;
+  const size_t per_block_max = prop.sharedMemPerBlockOptin - static_smem;  // dynamic part
+  const size_t reserve = 1024 + static_smem;  // per-block system reservation + static shared variables
+  const int max_fit = (int)std::min<size_t>(kMaxSmemPlates, per_block_max / slot_bytes);
+  int st;
+  if ((st = prepare_kernel<128>(per_block_max)) || (st = prepare_kernel<64>(per_block_max))) return st;
   if (cudaFuncSetAttribute(assign_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxGenes * 8) !=
       cudaSuccess)
     return BRKGA_ERR_CUDA;
@@ -1088,39 +1118,59 @@ int configure(BrkgaProblem* pb, int ctas_req, int plates_req) {
     if (share <= reserve) return 0;
     return (int)std::min<size_t>((share - reserve) / slot_bytes, (size_t)max_fit);
   };
-  int S = 0, ctas = 0;
-  if (ctas_req == 0) {
-    if (plates_req >= 0) {
-      S = plates_req;
-      ctas = 8;
-      while (ctas > 1 && fit_for(ctas) < S) --ctas;
+  Shape shapes[2];
+  for (int v = 0; v < 2; ++v) {
+    const int warps = v == 0 ? 4 : 2;
+    const int auto_ctas = kResidentWarps / warps;
+    const bool req = warps_req == warps;
+    const int creq = req ? ctas_req : 0, preq = req ? plates_req : -1;
+    int S, ctas;
+    if (creq == 0) {
+      ctas = auto_ctas;
+      if (preq >= 0) {
+        S = preq;
+        while (ctas > 1 && fit_for(ctas) < S) --ctas;
+        if (fit_for(ctas) < S) return BRKGA_ERR_INVALID_ARGUMENT;
+      } else {
+        // Resident warps matter far more than where the plates live (the
+        // pool stays in L2): as many plates per item in shared memory as
+        // their share holds, none for large plates.
+        S = std::min(fit_for(ctas), 4);
+      }
     } else {
-      // Resident warps matter far more than where the plates live (the pool
-      // stays in L2): 8 CTAs, and as many plates per item in shared memory
-      // as their share holds (none for plates above ~27 KB).
-      ctas = 8;
-      S = std::min(fit_for(ctas), 4);
+      ctas = creq;
+      S = preq >= 0 ? preq : std::min(fit_for(ctas), 4);
     }
-  } else {
-    ctas = ctas_req;
-    S = plates_req >= 0 ? plates_req : std::min(fit_for(ctas), 4);
+    if (S > max_fit) return BRKGA_ERR_INVALID_ARGUMENT;
+    const size_t smem = (size_t)S * slot_bytes;
+    int occ = 0;
+    if ((st = occupancy(warps, smem, &occ))) return st;
+    if (occ < 1 || (creq > 0 && occ < creq)) return BRKGA_ERR_INVALID_ARGUMENT;
+    shapes[v].warps = warps;
+    shapes[v].S = S;
+    shapes[v].smem = smem;
+    shapes[v].ctas = std::max(1, std::min(occ, ctas));
+    shapes[v].n_slots = pb->sm_count * shapes[v].ctas;
   }
-  if (S > max_fit) return BRKGA_ERR_INVALID_ARGUMENT;
-  const size_t smem = (size_t)S * slot_bytes;
-  int occ = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, decode_kernel, kDecodeThreads, smem) != cudaSuccess)
-    return BRKGA_ERR_CUDA;
-  if (occ < 1 || (ctas_req > 0 && occ < ctas_req) || (ctas_req == 0 && plates_req >= 0 && fit_for(ctas) < S))
-    return BRKGA_ERR_INVALID_ARGUMENT;
   pb->slot_vac_off = slot_vac_off;
   pb->slot_words = slot_words;
-  pb->S = S;
-  pb->decode_smem = smem;
-  pb->ctas_per_sm = std::max(1, std::min(occ, ctas));
-  pb->n_slots = pb->sm_count * pb->ctas_per_sm;
+  pb->shape[0] = shapes[0];
+  pb->shape[1] = shapes[1];
+  pb->max_slots = std::max(shapes[0].n_slots, shapes[1].n_slots);
+  pb->min_S = std::min(shapes[0].S, shapes[1].S);
+  pb->req_warps = warps_req;
   pb->req_ctas = ctas_req;
   pb->req_plates = plates_req;
   return BRKGA_OK;
+}
+
+// The shape a launch of `items` items uses: the requested CTA size, else
+// 4 warps per item while the items fill at most three waves of resident
+// CTAs (per-item latency dominates), 2 warps beyond (throughput dominates).
+const Shape& pick_shape(const BrkgaProblem* pb, int64_t items) {
+  if (pb->req_warps == 4) return pb->shape[0];
+  if (pb->req_warps == 2) return pb->shape[1];
+  return items > 3 * (int64_t)pb->shape[0].n_slots ? pb->shape[1] : pb->shape[0];
 }
 
 int validate(const BrkgaProblemDesc* d) {
@@ -1300,7 +1350,7 @@ int fill_run(const BrkgaProblem* pb, const int32_t* pops, const int64_t* chrom_o
   run->binscal = reinterpret_cast<BinScal*>(ws + l.off_bins);
   run->pool = reinterpret_cast<uint32_t*>(ws + l.off_pool);
   run->pool_bins = pool_bins;
-  run->S = pb->S;
+  run->S = pick_shape(pb, lc.items).S;
   run->slot_words = pb->slot_words;
   run->slot_vac_off = pb->slot_vac_off;
   run->task_max = pb->task_max;
@@ -1331,8 +1381,10 @@ int launch(const BrkgaProblem* pb, int stage, const Run& run, cudaStream_t s) {
     order_items_kernel<<<1, 1024, (size_t)(pb->Nmax + 1) * sizeof(int), s>>>(pb->tb, run);
   }
   if (stage == 0 || stage == 2) {
-    const int grid = (int)std::min<int64_t>(pb->n_slots, run.n_items);
-    decode_kernel<<<grid, kDecodeThreads, pb->decode_smem, s>>>(pb->tb, run);
+    const Shape& sh = pick_shape(pb, run.n_items);
+    const int grid = (int)std::min<int64_t>(sh.n_slots, run.n_items);
+    if (sh.warps == 2) decode_kernel<64><<<grid, 64, sh.smem, s>>>(pb->tb, run);
+    else decode_kernel<128><<<grid, 128, sh.smem, s>>>(pb->tb, run);
   }
   if (stage == 0 || stage == 3) reduce_kernel<<<(run.n_rows + 255) / 256, 256, 0, s>>>(pb->tb, run);
   return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
@@ -1434,7 +1486,7 @@ int brkga_problem_create_multi(const BrkgaProblemDesc* descs, int32_t K, BrkgaPr
       (st = upload(pb, &pb->d_dens, g.dens)) || (st = upload(pb, &pb->d_truns, g.truns)) ||
       (st = upload(pb, &pb->d_maskbits, g.maskbits)) ||
       (st = upload(pb, &pb->d_fits, g.fits)) || (st = upload(pb, &pb->d_newbin_ok, g.newbin_ok)) ||
-      (st = upload(pb, &pb->d_bin_area, g.bin_area)) || (st = configure(pb, 0, -1))) {
+      (st = upload(pb, &pb->d_bin_area, g.bin_area)) || (st = configure(pb, 0, 0, -1))) {
     brkga_problem_destroy(pb);
     return st;
   }
@@ -1475,27 +1527,31 @@ int brkga_problem_instances(const BrkgaProblem* pb, int32_t* K) {
   return BRKGA_OK;
 }
 
-int brkga_set_launch_config(BrkgaProblem* pb, int32_t ctas_per_sm, int32_t smem_plates, int32_t task_max) {
-  if (!pb || ctas_per_sm < 0 || ctas_per_sm > kMaxCtasPerSm || smem_plates < -1 || smem_plates > kMaxSmemPlates ||
-      task_max < -1 || task_max > kMaxTaskMax)
+int brkga_set_launch_config(BrkgaProblem* pb, int32_t warps_per_item, int32_t ctas_per_sm, int32_t smem_plates,
+                            int32_t task_max) {
+  if (!pb || (warps_per_item != 0 && warps_per_item != 2 && warps_per_item != 4) || ctas_per_sm < 0 ||
+      ctas_per_sm > kMaxCtasPerSm || smem_plates < -1 || smem_plates > kMaxSmemPlates || task_max < -1 ||
+      task_max > kMaxTaskMax)
     return BRKGA_ERR_INVALID_ARGUMENT;
   DeviceGuard g(pb->device);
-  const int old_ctas = pb->req_ctas, old_plates = pb->req_plates;
-  const int st = configure(pb, ctas_per_sm, smem_plates);
+  const int old_warps = pb->req_warps, old_ctas = pb->req_ctas, old_plates = pb->req_plates;
+  const int st = configure(pb, warps_per_item, ctas_per_sm, smem_plates);
   if (st) {
-    configure(pb, old_ctas, old_plates);
+    configure(pb, old_warps, old_ctas, old_plates);
     return st;
   }
   pb->task_max = task_max < 0 ? kDefaultTaskMax : task_max;
   return BRKGA_OK;
 }
 
-int brkga_get_launch_config(const BrkgaProblem* pb, int32_t* ctas_per_sm, int32_t* smem_plates,
-                            int32_t* resident_ctas, int32_t* task_max) {
-  if (!pb) return BRKGA_ERR_INVALID_ARGUMENT;
-  if (ctas_per_sm) *ctas_per_sm = pb->ctas_per_sm;
-  if (smem_plates) *smem_plates = pb->S;
-  if (resident_ctas) *resident_ctas = pb->n_slots;
+int brkga_get_launch_config(const BrkgaProblem* pb, int64_t items, int32_t* warps_per_item, int32_t* ctas_per_sm,
+                            int32_t* smem_plates, int32_t* resident_ctas, int32_t* task_max) {
+  if (!pb || items < 0) return BRKGA_ERR_INVALID_ARGUMENT;
+  const Shape& sh = pick_shape(pb, items);
+  if (warps_per_item) *warps_per_item = sh.warps;
+  if (ctas_per_sm) *ctas_per_sm = sh.ctas;
+  if (smem_plates) *smem_plates = sh.S;
+  if (resident_ctas) *resident_ctas = sh.n_slots;
   if (task_max) *task_max = pb->task_max;
   return BRKGA_OK;
 }
@@ -1717,7 +1773,7 @@ int brkga_initial_solution_host(BrkgaProblem* pb, const int32_t* h_order, int32_
     g.plate_machine = reinterpret_cast<int32_t*>(d + off_pm);
     g.plate_index = reinterpret_cast<int32_t*>(d + off_pi);
     g.machine_makespan = reinterpret_cast<double*>(d + off_mk);
-    greedy_kernel<<<1, kDecodeThreads>>>(pb->tb, g);
+    greedy_kernel<<<1, kGreedyThreads>>>(pb->tb, g);
     int32_t status = 0;
     if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess ||
         cudaMemcpy(&status, g.status, 4, cudaMemcpyDeviceToHost) != cudaSuccess) {

@@ -39,16 +39,18 @@ class _NativeProblem:
             abi.check(st, "brkga_problem_create")
         self.handle = handle
 
-    def launch_config(self):
-        """(CTAs per SM, plates per item in shared memory, resident CTAs, task_max) of the decode kernel."""
-        c, s, r, t = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
-        abi.check(self.lib.brkga_get_launch_config(self.handle, ctypes.byref(c), ctypes.byref(s), ctypes.byref(r),
-                                                   ctypes.byref(t)))
-        return c.value, s.value, r.value, t.value
+    def launch_config(self, items: int = 0):
+        """(warps per item, CTAs per SM, plates per item in shared memory, resident CTAs, task_max)
+        of a decode launch of ``items`` (chromosome, machine) items."""
+        w, c, s, r, t = (ctypes.c_int32() for _ in range(5))
+        abi.check(self.lib.brkga_get_launch_config(self.handle, int(items), ctypes.byref(w), ctypes.byref(c),
+                                                   ctypes.byref(s), ctypes.byref(r), ctypes.byref(t)))
+        return w.value, c.value, s.value, r.value, t.value
 
-    def set_launch_config(self, ctas_per_sm: int, smem_plates: int, task_max: int = -1):
-        abi.check(self.lib.brkga_set_launch_config(self.handle, int(ctas_per_sm), int(smem_plates), int(task_max)),
-                  "brkga_set_launch_config")
+    def set_launch_config(self, warps_per_item: int = 0, ctas_per_sm: int = 0, smem_plates: int = -1,
+                          task_max: int = -1):
+        abi.check(self.lib.brkga_set_launch_config(self.handle, int(warps_per_item), int(ctas_per_sm),
+                                                   int(smem_plates), int(task_max)), "brkga_set_launch_config")
 
     def close(self):
         if getattr(self, "handle", None) is not None and self.handle.value:
@@ -175,14 +177,16 @@ class DeviceDecoder:
         abi.check(self.lib.brkga_workspace_bytes(self.native.handle, int(P), self.pool_bins, ctypes.byref(nbytes)))
         return nbytes.value
 
-    def launch_config(self):
-        """(CTAs per SM, plates per item in shared memory, resident CTAs, task_max) of the decode kernel."""
-        return self.native.launch_config()
+    def launch_config(self, items: Optional[int] = None):
+        """(warps per item, CTAs per SM, plates per item in shared memory, resident CTAs, task_max) of a
+        decode launch of ``items`` items (default: a full population, ``max_pop`` x machines)."""
+        return self.native.launch_config(self.max_pop * self.packed.n_machines if items is None else items)
 
-    def set_launch_config(self, ctas_per_sm: int, smem_plates: int, task_max: int = -1):
-        """Change the decode kernel's launch configuration (0 / -1 / -1 =
-        automatic) and regrow the workspace when the new shape needs more."""
-        self.native.set_launch_config(ctas_per_sm, smem_plates, task_max)
+    def set_launch_config(self, warps_per_item: int = 0, ctas_per_sm: int = 0, smem_plates: int = -1,
+                          task_max: int = -1):
+        """Change the decode kernel's launch configuration (defaults: automatic)
+        and regrow the workspace when the new shape needs more."""
+        self.native.set_launch_config(warps_per_item, ctas_per_sm, smem_plates, task_max)
         need = self.workspace_bytes(self.max_pop)
         if need > self.ws_bytes:
             self.workspace = self.torch.empty(need, dtype=self.torch.uint8, device=self.device)
@@ -272,11 +276,15 @@ class MultiDecoder:
                   "brkga_workspace_bytes_multi")
         return nbytes.value
 
-    def launch_config(self):
-        return self.native.launch_config()
+    def launch_config(self, items: Optional[int] = None):
+        """Launch configuration for ``items`` items (default: every instance at ``max_pops``)."""
+        if items is None:
+            items = int(sum(int(p) * m for p, m in zip(self.max_pops, self.n_machines)))
+        return self.native.launch_config(items)
 
-    def set_launch_config(self, ctas_per_sm: int, smem_plates: int, task_max: int = -1):
-        self.native.set_launch_config(ctas_per_sm, smem_plates, task_max)
+    def set_launch_config(self, warps_per_item: int = 0, ctas_per_sm: int = 0, smem_plates: int = -1,
+                          task_max: int = -1):
+        self.native.set_launch_config(warps_per_item, ctas_per_sm, smem_plates, task_max)
         need = self.workspace_bytes(self.max_pops)
         if need > self.ws_bytes:
             self.workspace = self.torch.empty(need, dtype=self.torch.uint8, device=self.device)

@@ -204,26 +204,36 @@ int brkga_decode_multi_at(int32_t stage, const BrkgaProblem* problem, const floa
                           const int64_t* makespan_offsets, BrkgaPlacement* d_log, int32_t* d_status,
                           void* d_ws, size_t ws_bytes, int64_t pool_bins, void* stream);
 
-/* Launch shape of the decode kernel (the autotuner's knobs; no reference
- * counterpart): ctas_per_sm resident CTAs of 4 warps per SM (1..32, 0 =
- * automatic), smem_plates plates of each item kept in shared memory (0..8,
- * the rest in the global pool; -1 = as many as fit, at most 4), and task_max
- * (0..8192, -1 = the default 512): a warp that tests 32 candidate rows deals
- * the (candidate that passed the vacancy filter, 32-column output word) pairs
- * across its lanes when there are at most task_max of them, else each lane
- * tests its own candidate.  Results never depend on these knobs.  A shape that
- * cannot be resident is refused with BRKGA_ERR_INVALID_ARGUMENT and the
- * previous one kept.  The workspace size depends on the shape: query
- * brkga_workspace_bytes again after a change.  Not to be called while a
- * decode of this problem is being launched from another thread. */
-int brkga_set_launch_config(BrkgaProblem* problem, int32_t ctas_per_sm, int32_t smem_plates,
-                            int32_t task_max);
+/* Launch configuration of the decode kernel (the autotuner's knobs; no
+ * reference counterpart).  Results never depend on it.
+ *   warps_per_item  2 or 4 warps per CTA, one (chromosome, machine) item per
+ *                   CTA; 0 = automatic per launch (4 while the items fill at
+ *                   most three waves of resident CTAs, where the latency of
+ *                   one item dominates; 2 beyond, where throughput does)
+ *   ctas_per_sm     resident CTAs per SM for that size (1..32; 0 = 32
+ *                   resident warps per SM, the register limit)
+ *   smem_plates     plates of each item kept in shared memory (0..8, the
+ *                   rest in the global pool; -1 = as many as fit, at most 4)
+ *   task_max        0..8192, -1 = the default 512: a warp that tests 32
+ *                   candidate rows deals the (candidate that passed the
+ *                   vacancy filter, 32-column output word) pairs across its
+ *                   lanes when there are at most task_max of them, else each
+ *                   lane tests its own candidate
+ * ctas_per_sm and smem_plates need an explicit warps_per_item (with 0 they
+ * must be 0 and -1).  A shape that cannot be resident is refused with
+ * BRKGA_ERR_INVALID_ARGUMENT and the previous configuration kept.  The
+ * workspace size depends on the configuration: query brkga_workspace_bytes
+ * again after a change.  Not to be called while a decode of this problem is
+ * being launched from another thread. */
+int brkga_set_launch_config(BrkgaProblem* problem, int32_t warps_per_item, int32_t ctas_per_sm,
+                            int32_t smem_plates, int32_t task_max);
 
-/* The configuration in use: CTAs per SM, plates per item in shared memory,
- * the decode kernel's grid (SMs x CTAs per SM) and task_max; any output may
- * be NULL. */
-int brkga_get_launch_config(const BrkgaProblem* problem, int32_t* ctas_per_sm, int32_t* smem_plates,
-                            int32_t* resident_ctas, int32_t* task_max);
+/* The configuration a launch of `items` (chromosome, machine) items uses:
+ * warps per item, CTAs per SM, plates per item in shared memory, the decode
+ * kernel's grid (SMs x CTAs per SM) and task_max; any output may be NULL. */
+int brkga_get_launch_config(const BrkgaProblem* problem, int64_t items, int32_t* warps_per_item,
+                            int32_t* ctas_per_sm, int32_t* smem_plates, int32_t* resident_ctas,
+                            int32_t* task_max);
 
 /* Host-to-host evaluation, the drop-in for NativeFullDecoder::evaluate_batch
  * (full_native_decoder.py:563-641): copies h_chrom [P, 2N] float32 to the

@@ -99,5 +99,5 @@ def test_multi_instance_arguments(lib):
     n = ctypes.c_size_t()
     assert lib.brkga_workspace_bytes_multi(None, abi.ptr(pops, ctypes.c_int32), 0, ctypes.byref(n)) == \
         abi.ERR_INVALID_ARGUMENT
-    assert lib.brkga_set_launch_config(None, 1, 0, -1) == abi.ERR_INVALID_ARGUMENT
-    assert lib.brkga_get_launch_config(None, None, None, None, None) == abi.ERR_INVALID_ARGUMENT
+    assert lib.brkga_set_launch_config(None, 4, 1, 0, -1) == abi.ERR_INVALID_ARGUMENT
+    assert lib.brkga_get_launch_config(None, 0, None, None, None, None, None) == abi.ERR_INVALID_ARGUMENT

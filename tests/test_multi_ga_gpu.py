@@ -64,17 +64,19 @@ def test_autotune_picks_a_shape_and_keeps_results(torch, tmp_path):
     md = MultiDecoder(packs, max_pops=pops)
     flat = torch.from_numpy(np.concatenate([c.reshape(-1) for c in chroms])).cuda()
     cache = str(tmp_path / "tune.json")
-    shapes = [(2, 0), (4, 1), (8, 0), (0, -1), (32, 8)]  # the last cannot be resident and is skipped
+    shapes = [(4, 2, 0), (4, 4, 1), (2, 16, 0), (0, 0, -1), (4, 32, 8)]  # the last cannot be resident
     res = autotune(md, flat, pops, shapes=shapes, task_max_values=(0, 256), cache_path=cache)
     assert not res["cached"] and len(res["table"]) == 6
-    assert res["config"] in [(c, s, t if t >= 0 else 512) for c, s, t, _ in res["table"]]
-    c, s, _, t = md.launch_config()
-    assert t == res["config"][2]
+    assert res["config"] in [(w, c, s, t if t >= 0 else 512) for w, c, s, t, _ in res["table"]]
+    w, c, s, _, t = md.launch_config()
+    assert t == res["config"][3]
     if res["config"][0]:
-        assert c == res["config"][0]
+        assert w == res["config"][0]
+    if res["config"][1]:
+        assert c == res["config"][1]
     np.testing.assert_array_equal(md.decode_concat(flat, pops).cpu().numpy(), ref)
-    md.set_launch_config(0, -1)
+    md.set_launch_config()
     again = autotune(md, flat, pops, shapes=shapes, cache_path=cache)
     assert again["cached"] and again["config"] == res["config"]
-    assert md.launch_config()[3] == res["config"][2]
+    assert md.launch_config()[4] == res["config"][3]
     np.testing.assert_array_equal(md.decode_concat(flat, pops).cpu().numpy(), ref)

@@ -64,27 +64,44 @@ def test_uneven_instances_match_oracle(multi):
     _check(md, POPS, out, log, ref)
 
 
-@pytest.mark.parametrize("cfg", [(1, 0, -1), (2, 1, 0), (4, -1, 64), (8, 0, 8192), (0, 0, 1), (0, -1, -1)])
+CONFIGS = [(4, 1, 0, -1), (4, 2, 1, 0), (2, 4, -1, 64), (4, 8, 0, 8192), (2, 16, 0, 1), (0, 0, -1, -1),
+           (2, 0, -1, -1), (4, 0, 2, -1)]
+
+
+@pytest.mark.parametrize("cfg", CONFIGS)
 def test_launch_configs_give_identical_results(multi, cfg):
     torch, insts, packs, chroms, ref, md = multi
     md.set_launch_config(*cfg)
-    ctas, plates, grid, task_max = md.launch_config()
+    warps, ctas, plates, grid, task_max = md.launch_config()
     if cfg[0]:
-        assert ctas == cfg[0]
-    if cfg[1] >= 0:
-        assert plates == cfg[1]
-    assert task_max == (cfg[2] if cfg[2] >= 0 else 512)
+        assert warps == cfg[0]
+    if cfg[1]:
+        assert ctas == cfg[1]
+    if cfg[2] >= 0:
+        assert plates == cfg[2]
+    assert task_max == (cfg[3] if cfg[3] >= 0 else 512)
     out, log = _run(torch, md, chroms, POPS)
     _check(md, POPS, out, log, ref)
-    md.set_launch_config(0, -1)
+    md.set_launch_config()
+
+
+def test_automatic_warps_follow_item_count(multi):
+    torch, insts, packs, chroms, ref, md = multi
+    md.set_launch_config()
+    w_small, _, _, slots4, _ = md.launch_config(items=1)
+    assert w_small == 4
+    assert md.launch_config(items=3 * slots4)[0] == 4
+    assert md.launch_config(items=3 * slots4 + 1)[0] == 2
 
 
 def test_unresident_shape_is_refused(multi):
     torch, insts, packs, chroms, ref, md = multi
     before = md.launch_config()
     with pytest.raises(abi.BrkgaError) as e:
-        md.set_launch_config(32, 8)  # 32 CTAs with 8 plates each cannot share one SM
+        md.set_launch_config(4, 32, 8)  # 32 CTAs with 8 plates each cannot share one SM
     assert e.value.status == abi.ERR_INVALID_ARGUMENT
+    with pytest.raises(abi.BrkgaError):
+        md.set_launch_config(0, 8, 0)  # a CTA count needs an explicit CTA size
     assert md.launch_config() == before
 
 
