@@ -125,6 +125,7 @@ def load_library(path: str = LIB_PATH):
         "brkga_ga_gather": (c_int, [vp, vp, c_i32, c_i32, vp, vp]),
         "brkga_ga_screen_stats": (c_int, [vp, vp, vp, vp, c_i32, vp, vp, c_i32, vp, vp]),
         "brkga_ga_track": (c_int, [vp, vp, c_i32, c_i32, vp, vp, c_i32, vp, vp, vp]),
+        "brkga_ga_audit": (c_int, [vp, vp, vp, c_i32, c_i32, vp, c_i32, vp, vp, vp]),
         "brkga_gemm_bf16": (c_int, [vp, c_i32, vp, c_i32, vp, c_i32, c_i32, c_i32, c_i32, vp, vp]),
         "brkga_surrogate_create": (c_int, [vp, c_i32, c_i32, ctypes.c_uint64, P(vp)]),
         "brkga_surrogate_destroy": (None, [vp]),

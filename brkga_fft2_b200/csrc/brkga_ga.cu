@@ -24,7 +24,9 @@
 
 namespace {
 
-constexpr int kMaxRank = 8192;  // single-CTA bitonic sort: 8192 x 12 B in shared memory
+constexpr int kMaxRank = 8192;         // single-CTA bitonic sort: 8192 x 12 B in shared memory
+constexpr int kMaxRankCount = 65536;   // larger populations: rank by counting (P^2 key comparisons)
+constexpr int kRankTile = 2048;
 
 enum Tag : uint32_t { kTagInit = 0, kTagMutant = 1, kTagMask = 2, kTagParents = 3 };
 
@@ -106,6 +108,31 @@ __global__ void rank_kernel(const double* fit, int P, int S2, int32_t* order) {
   for (int i = tid; i < P; i += nt) order[i] = idx[i];
 }
 
+// Rank by counting for populations above the single-CTA sort: the rank of row
+// i is the number of rows j with (key_j, j) < (key_i, i), the keys of all rows
+// streamed through shared memory tile by tile (every thread reads the same
+// entry: broadcast).  Same order as rank_kernel; O(P^2) comparisons, about
+// 0.1 ms at P = 20,000.
+__global__ void rank_count_kernel(const double* fit, int P, int32_t* order) {
+  __shared__ unsigned long long tile[kRankTile];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned long long ki = i < P ? ordered_f64(fit[i]) : 0ull;
+  int rank = 0;
+  for (int base = 0; base < P; base += kRankTile) {
+    const int n = min(kRankTile, P - base);
+    __syncthreads();
+    for (int t = threadIdx.x; t < n; t += blockDim.x) tile[t] = ordered_f64(fit[base + t]);
+    __syncthreads();
+    if (i < P) {
+      for (int t = 0; t < n; ++t) {
+        const unsigned long long kj = tile[t];
+        rank += (kj < ki) | ((kj == ki) & (base + t < i));
+      }
+    }
+  }
+  if (i < P) order[rank] = i;
+}
+
 // One thread per (row, 4-key block) of the new population.
 __global__ void breed_kernel(const float* pop, const double* fit, const int32_t* order, int P, int out_rows, int K,
                              int ne, int nm, float rho, uint32_t k0, uint32_t k1, const long long* generation,
@@ -145,6 +172,22 @@ __global__ void gather_rows_kernel(const float* src, const int32_t* idx, int n, 
     const int r = (int)(i / K), k = (int)(i - (long long)r * K);
     dst[i] = src[(size_t)idx[r] * K + k];
   }
+}
+
+// Audit sample: rows idx[0..n) of the population and their makespans into
+// slot g = *generation of the audit arrays (nothing when g >= slots).
+__global__ void audit_kernel(const float* pop, const double* fit, const int32_t* idx, int n, int K,
+                             const long long* generation, int slots, float* audit_pop, double* audit_fit) {
+  const long long g = *generation;
+  if (g < 0 || g >= slots) return;
+  const long long total = (long long)n * K;
+  float* dst = audit_pop + (size_t)g * n * K;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(i / K), k = (int)(i - (long long)r * K);
+    dst[i] = pop[(size_t)idx[r] * K + k];
+  }
+  if (blockIdx.x == 0)
+    for (int r = threadIdx.x; r < n; r += blockDim.x) audit_fit[(size_t)g * n + r] = fit[idx[r]];
 }
 
 // Surrogate quality on the rows decoded this generation: Spearman correlation
@@ -295,8 +338,12 @@ int brkga_ga_init_population(float* d_pop, int32_t P, int32_t n_keys, uint64_t s
 }
 
 int brkga_ga_rank(const double* d_fitness, int32_t P, int32_t* d_order, void* stream) {
-  if (P < 0 || P > kMaxRank || (P > 0 && (!d_fitness || !d_order))) return BRKGA_ERR_INVALID_ARGUMENT;
+  if (P < 0 || P > kMaxRankCount || (P > 0 && (!d_fitness || !d_order))) return BRKGA_ERR_INVALID_ARGUMENT;
   if (P == 0) return BRKGA_OK;
+  if (P > kMaxRank) {
+    rank_count_kernel<<<(P + 255) / 256, 256, 0, (cudaStream_t)stream>>>(d_fitness, P, d_order);
+    return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
+  }
   int S2 = 1;
   while (S2 < P) S2 <<= 1;
   const size_t smem = (size_t)S2 * (sizeof(unsigned long long) + sizeof(int));
@@ -345,6 +392,19 @@ int brkga_ga_gather(const float* d_src, const int32_t* d_index, int32_t n, int32
   if (n == 0) return BRKGA_OK;
   gather_rows_kernel<<<grid_for((long long)n * n_keys), 256, 0, (cudaStream_t)stream>>>(d_src, d_index, n, n_keys,
                                                                                       d_dst);
+  return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
+}
+
+int brkga_ga_audit(const float* d_pop, const double* d_fitness, const int32_t* d_index, int32_t n, int32_t n_keys,
+                   const int64_t* d_generation, int32_t slots, float* d_audit_pop, double* d_audit_fit,
+                   void* stream) {
+  if (n < 0 || n_keys < 1 || slots < 0 ||
+      (n > 0 && (!d_pop || !d_fitness || !d_index || !d_generation || !d_audit_pop || !d_audit_fit)))
+    return BRKGA_ERR_INVALID_ARGUMENT;
+  if (n == 0 || slots == 0) return BRKGA_OK;
+  audit_kernel<<<grid_for((long long)n * n_keys), 256, 0, (cudaStream_t)stream>>>(
+      d_pop, d_fitness, d_index, n, n_keys, reinterpret_cast<const long long*>(d_generation), slots, d_audit_pop,
+      d_audit_fit);
   return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
 }
 

@@ -10,6 +10,12 @@ decoded rows are logged for every generation (``history['spearman']``,
 the last ``check_every`` generations stays below ``spearman_threshold``
 (the surrogate keeps learning from plain generations meanwhile).
 
+With ``audit_fraction > 0`` every generation also copies an evenly spaced
+sample of the rows it decoded (that fraction of them), with their exact
+makespans, into ``audit`` = (chromosomes [G+1, n, 2N], makespans [G+1, n]),
+so a run can be checked against an independent decoder afterwards without
+stopping the graph replays.
+
 ``DeviceBRKGA`` mirrors ``BRKGA_alg3.BRKGA`` (``BRKGA_alg3.py:23-281``): the
 same constructor parameters (``num_generations``, ``num_individuals``,
 ``num_elites``, ``num_mutants``, ``eliteCProb``, ``initialSol``), ``fit()``,
@@ -32,6 +38,8 @@ from . import abi
 from .evaluator import DeviceDecoder
 from .problem import THRESH_F32, PackedProblem, pack_problem
 
+MAX_RANK = 65536  # brkga_ga_rank
+
 
 class DeviceBRKGA:
     def __init__(self, problem_data, nbParts, nbMachines, thresholds, instanceParts, initialSol=None,
@@ -41,7 +49,7 @@ class DeviceBRKGA:
                  packed: Optional[PackedProblem] = None, device=None, screening: bool = False,
                  oversample: int = 5, train_steps: int = 8, train_batch: int = 512, lr: float = 1e-3,
                  spearman_threshold: float = 0.3, check_every: int = 5, warmup_generations: int = 5,
-                 buffer_capacity: int = 200_000, target: Optional[float] = None):
+                 buffer_capacity: int = 200_000, target: Optional[float] = None, audit_fraction: float = 0.0):
         import torch
         del collision_backend, eval_mode, eval_workers, eval_chunksize
         self.torch = torch
@@ -58,8 +66,8 @@ class DeviceBRKGA:
         self.initialSol = None if initialSol is None else np.asarray(initialSol, np.float32)
         if not (1 <= self.num_elites and self.num_elites + self.num_mutants <= self.num_individuals):
             raise ValueError("need 1 <= num_elites and num_elites + num_mutants <= num_individuals")
-        if self.num_individuals > 8192:
-            raise ValueError("num_individuals must be <= 8192 (single-CTA rank)")
+        if self.num_individuals > MAX_RANK:
+            raise ValueError(f"num_individuals must be <= {MAX_RANK} (device rank)")
         self.packed = packed if packed is not None else pack_problem(
             problem_data, nbParts, nbMachines, thresholds, instanceParts, threshold_mode)
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
@@ -82,6 +90,15 @@ class DeviceBRKGA:
         self._graphs = {}
         self._prepared = False
         self.target = target
+        # audit sample: evenly spaced rows among those decoded every generation, kept with their makespans
+        self.audit = None
+        n_dec = P - self.num_elites
+        self.n_audit = min(n_dec, max(1, int(np.ceil(audit_fraction * n_dec)))) if audit_fraction > 0 and n_dec else 0
+        if self.n_audit:
+            idx = self.num_elites + (np.arange(self.n_audit) * n_dec) // self.n_audit
+            self.audit_index = torch.from_numpy(idx.astype(np.int32)).to(dev)
+            self.audit_pop = torch.zeros(self.num_generations + 1, self.n_audit, K, dtype=torch.float32, device=dev)
+            self.audit_fit = torch.zeros(self.num_generations + 1, self.n_audit, dtype=torch.float64, device=dev)
         self.screening = bool(screening)
         if self.screening:
             from .surrogate import Surrogate
@@ -92,8 +109,8 @@ class DeviceBRKGA:
             self.warmup_generations = int(warmup_generations)
             rows = P - self.num_elites
             self.pool_rows = self.num_elites + self.oversample * rows
-            if self.pool_rows - self.num_elites > 8192:
-                raise ValueError("oversampled pool too large for the single-CTA rank (8192 rows)")
+            if self.pool_rows - self.num_elites > MAX_RANK:
+                raise ValueError(f"oversampled pool too large for the device rank ({MAX_RANK} rows)")
             self.pool = torch.zeros(self.pool_rows, K, dtype=torch.float32, device=dev)
             self.pool_fit = torch.zeros(self.pool_rows, dtype=torch.float64, device=dev)
             self.pred = torch.zeros(self.pool_rows - self.num_elites, dtype=torch.float64, device=dev)
@@ -115,6 +132,12 @@ class DeviceBRKGA:
         return ctypes.c_void_p(self.torch.cuda.current_stream(self.device).cuda_stream)
 
     def _track(self, cur):
+        if self.n_audit:
+            abi.check(self.lib.brkga_ga_audit(self._ptr(self.pop[cur]), self._ptr(self.fitness_buf[cur]),
+                                              self._ptr(self.audit_index), self.n_audit, self.num_gene,
+                                              self._ptr(self.generation), self.num_generations + 1,
+                                              self._ptr(self.audit_pop), self._ptr(self.audit_fit), self._stream()),
+                      "brkga_ga_audit")
         abi.check(self.lib.brkga_ga_track(self._ptr(self.fitness_buf[cur]), self._ptr(self.pop[cur]),
                                           self.num_individuals, self.num_gene, self._ptr(self.generation),
                                           self._ptr(self.history_dev), self.num_generations + 1,
@@ -298,6 +321,8 @@ class DeviceBRKGA:
             self.solution = self.best_sol.cpu().numpy()
             self.used_bins = int(np.floor(self.best_fitness))
             self.population = self.pop[cur].cpu().numpy()
+            if self.n_audit:
+                self.audit = (self.audit_pop[:G + 1].cpu().numpy(), self.audit_fit[:G + 1].cpu().numpy())
             self.fitness = self.fitness_buf[cur].cpu().numpy()
             self.wall_time = wall
             if verbose:

@@ -25,6 +25,7 @@ import numpy as np
 
 from . import abi
 from .evaluator import MultiDecoder
+from .ga import MAX_RANK
 
 
 def _per_instance(v, K, name):
@@ -52,8 +53,8 @@ class MultiBRKGA:
               else [int(round(0.15 * p)) for p in self.P])
         self.ne, self.nm = [int(v) for v in ne], [int(v) for v in nm]
         for P, e, m in zip(self.P, self.ne, self.nm):
-            if not (1 <= e and e + m <= P <= 8192):
-                raise ValueError("need 1 <= num_elites, num_elites + num_mutants <= num_individuals <= 8192")
+            if not (1 <= e and e + m <= P <= MAX_RANK):
+                raise ValueError(f"need 1 <= num_elites, num_elites + num_mutants <= num_individuals <= {MAX_RANK}")
         self.rho = float(eliteCProb)
         self.seed = int(seed)
         self.use_graph = bool(use_graph)

@@ -276,7 +276,8 @@ int brkga_ga_init_population(float* d_pop, int32_t P, int32_t n_keys, uint64_t s
                              void* stream);
 
 /* d_order[P] = indices sorting d_fitness ascending, ties by index; NaN last.
- * P <= 8192.  Replaces partition (BRKGA_alg3.py:178-186).  For P > 4096 the
+ * P <= 65536 (a single-CTA sort up to 8192, ranking by counting above).
+ * Replaces partition (BRKGA_alg3.py:178-186).  For 4096 < P <= 8192 the
  * first call on a device sets a kernel attribute, so make it outside graph capture. */
 int brkga_ga_rank(const double* d_fitness, int32_t P, int32_t* d_order, void* stream);
 
@@ -309,6 +310,15 @@ int brkga_ga_gather(const float* d_src, const int32_t* d_index, int32_t n, int32
 int brkga_ga_screen_stats(const double* d_pred, const double* d_exact, const int32_t* d_order_pred,
                           const int32_t* d_order_exact, int32_t n, const int64_t* d_generation, double* d_stats,
                           int32_t stats_len, int32_t* d_scratch, void* stream);
+
+/* Copy rows d_index[0..n) of d_pop [P, n_keys] and their d_fitness into slot
+ * g = *d_generation of d_audit_pop [slots, n, n_keys] and d_audit_fit
+ * [slots, n] (nothing when g >= slots): a sample of every generation's
+ * exact makespans kept for verification after the run (no reference
+ * counterpart). */
+int brkga_ga_audit(const float* d_pop, const double* d_fitness, const int32_t* d_index, int32_t n,
+                   int32_t n_keys, const int64_t* d_generation, int32_t slots, float* d_audit_pop,
+                   double* d_audit_fit, void* stream);
 
 /* After a population is scored: history[2g] = min, history[2g+1] = mean of
  * d_fitness for g = *d_generation (BRKGA_alg3.py:224-227,255-262); copies the

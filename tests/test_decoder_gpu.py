@@ -54,7 +54,8 @@ def test_fingerprint_strings(torch_cuda):
         assert [f"{v:.6f}" for v in ms[ms < 1e15]] == [f"{v:.6f}" for v in z["fingerprint"]], name
 
 
-@pytest.mark.parametrize("maker,P,seed", [(instances.p50m2, 100, 11), (instances.p100m4, 64, 12)])
+@pytest.mark.parametrize("maker,P,seed", [(instances.p50m2, 100, 11), (instances.p100m4, 64, 12),
+                                          (instances.p200m6, 24, 13), (instances.p400m8, 8, 14)])
 def test_benchmark_workloads_vs_oracle(maker, P, seed, torch_cuda):
     from brkga_fft2_b200.evaluator import B200DecoderEvaluator
     inst = maker(0)

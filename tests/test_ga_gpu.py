@@ -50,6 +50,28 @@ def test_kernels_match_oracle(torch):
     np.testing.assert_array_equal(nfit.cpu().numpy()[:ne], rfit[:ne])
 
 
+@pytest.mark.parametrize("P", [8192, 8193, 20000, 65536])
+def test_rank_large_populations(torch, P):
+    """Above 8192 rows the rank counts instead of sorting; same order (ties by index, NaN last)."""
+    lib = abi.load_library()
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    rng = np.random.default_rng(P)
+    fit_h = np.round(rng.random(P) * 300)  # many ties
+    fit_h[rng.choice(P, 5, replace=False)] = np.nan
+    fit_h[rng.choice(P, 5, replace=False)] = -0.0
+    fit = torch.from_numpy(fit_h).cuda()
+    order = torch.full((P,), -1, dtype=torch.int32, device="cuda")
+    assert lib.brkga_ga_rank(_p(fit), P, _p(order), s) == 0
+    np.testing.assert_array_equal(order.cpu().numpy(), go.rank(fit_h))
+
+
+def test_rank_refuses_beyond_limit(torch):
+    lib = abi.load_library()
+    fit = torch.zeros(65537, dtype=torch.float64, device="cuda")
+    order = torch.zeros(65537, dtype=torch.int32, device="cuda")
+    assert lib.brkga_ga_rank(_p(fit), 65537, _p(order), None) == abi.ERR_INVALID_ARGUMENT
+
+
 @pytest.mark.parametrize("use_graph", [False, True])
 def test_ga_run_matches_oracle(torch, use_graph):
     from brkga_fft2_b200.ga import DeviceBRKGA
@@ -99,3 +121,24 @@ def test_screened_ga_reports_exact_makespans(torch):
     assert "screen" in ga.history["mode"]
     assert np.isfinite(ga.history["spearman"][1:]).all() and np.isfinite(ga.history["mae"][1:]).all()
     assert (np.diff(ga.history["min"]) <= 0).all()
+
+
+@pytest.mark.parametrize("maker,P,G,frac", [(instances.p50m2, 200, 12, 0.02), (instances.p400m8, 48, 2, 0.01)])
+def test_audit_sample_of_every_generation_is_exact(torch, maker, P, G, frac):
+    """The audit sample (1-2 % of the rows decoded in every generation, screening on)
+    matches the oracle bit for bit, generation by generation."""
+    from brkga_fft2_b200.ga import DeviceBRKGA
+    from oracle import oracle_decode
+    inst = maker(0)
+    pk = pack_problem(inst.problem_data, inst.nb_parts, inst.nb_machines, inst.thresholds, inst.instance_parts)
+    ne = max(1, P // 10)
+    ga = DeviceBRKGA(None, inst.nb_parts, inst.nb_machines, inst.thresholds, inst.instance_parts,
+                     num_generations=G, num_individuals=P, num_elites=ne, num_mutants=P // 6, packed=pk, seed=5,
+                     screening=True, oversample=3, warmup_generations=1, check_every=1, spearman_threshold=-1.0,
+                     audit_fraction=frac)
+    ga.fit()
+    chrom, fit = ga.audit
+    assert chrom.shape[:2] == (G + 1, ga.n_audit) and ga.n_audit >= 1
+    ref = oracle_decode(pk, chrom.reshape(-1, chrom.shape[-1]), n_threads=8).reshape(fit.shape)
+    np.testing.assert_array_equal(fit, ref)
+    assert "screen" in ga.history["mode"]
