@@ -224,19 +224,38 @@ __global__ void relu_backward_kernel(float* dH, const float* Z, int B, int H, __
 }
 
 // out[h] = sum_b A[b, h] * (scale ? scale[b] : 1) * (mask ? (mask[b, h] > 0) : 1) * (colscale ? colscale[h] : 1)
-__global__ void col_reduce_kernel(const float* A, const float* scale, const float* mask, const float* colscale,
-                                  int B, int H, float* out) {
-  const int h = blockIdx.x * blockDim.x + threadIdx.x;
-  if (h >= H) return;
+// 32 columns per CTA (threadIdx.x, coalesced rows), the rows split over
+// kColRows thread rows and summed in shared memory in a fixed order, so the
+// result does not depend on scheduling.
+constexpr int kColRows = 16;
+__global__ void __launch_bounds__(32 * kColRows) col_reduce_kernel(const float* A, const float* scale,
+                                                                   const float* mask, const float* colscale, int B,
+                                                                   int H, float* out) {
+  __shared__ float part[kColRows][33];
+  const int h = blockIdx.x * 32 + threadIdx.x;
   float s = 0.f;
-  for (int b = 0; b < B; ++b) {
-    const size_t i = (size_t)b * H + h;
-    float v = A ? A[i] : 1.f;
-    if (scale) v *= scale[b];
-    if (mask && !(mask[i] > 0.f)) v = 0.f;
-    s += v;
+  if (h < H) {
+    for (int b = threadIdx.y; b < B; b += kColRows) {
+      const size_t i = (size_t)b * H + h;
+      float v = A ? A[i] : 1.f;
+      if (scale) v *= scale[b];
+      if (mask && !(mask[i] > 0.f)) v = 0.f;
+      s += v;
+    }
   }
-  out[h] = colscale ? s * colscale[h] : s;
+  part[threadIdx.y][threadIdx.x] = s;
+  __syncthreads();
+  if (threadIdx.y == 0 && h < H) {
+    float t = 0.f;
+#pragma unroll
+    for (int y = 0; y < kColRows; ++y) t += part[y][threadIdx.x];
+    out[h] = colscale ? t * colscale[h] : t;
+  }
+}
+
+void col_reduce(const float* A, const float* scale, const float* mask, const float* colscale, int B, int H,
+                float* out, cudaStream_t st) {
+  col_reduce_kernel<<<(H + 31) / 32, dim3(32, kColRows), 0, st>>>(A, scale, mask, colscale, B, H, out);
 }
 
 // Adam (Kingma & Ba); the step count t is read from device memory so graph replays stay correct
@@ -454,13 +473,34 @@ int dalloc(BrkgaSurrogate* s, T** p, size_t n) {
   return BRKGA_OK;
 }
 
+// The GEMM's two-stage tiles exceed the default 48 KB of shared memory: opt
+// in once per device (at surrogate creation or the first brkga_gemm_bf16,
+// so never inside a stream capture).
+int prepare_gemm() {
+  static int ready[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return BRKGA_ERR_CUDA;
+  if (ready[dev]) return BRKGA_OK;
+  if (cudaFuncSetAttribute(umma::gemm_bf16_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           umma::gemm_smem_bytes<128>()) != cudaSuccess ||
+      cudaFuncSetAttribute(umma::gemm_bf16_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           umma::gemm_smem_bytes<64>()) != cudaSuccess)
+    return BRKGA_ERR_CUDA;
+  ready[dev] = 1;
+  return BRKGA_OK;
+}
+
+// 128 x 128 tiles when they alone fill the GPU twice over, else 128 x 64
+// (these GEMMs are small: more CTAs matter more than tile reuse).
 int gemm(const __nv_bfloat16* A, int lda, const __nv_bfloat16* B, int ldb, float* C, int ldc, int M, int N, int K,
          int* err, cudaStream_t st) {
   if (M % 128 || K % 64 || N % 64) return BRKGA_ERR_INVALID_ARGUMENT;
-  if (N % 128 == 0) {
-    umma::gemm_bf16_kernel<128><<<dim3(M / 128, N / 128), 128, 0, st>>>(A, lda, B, ldb, C, ldc, K, err);
+  if (N % 128 == 0 && (long long)(M / 128) * (N / 128) >= 2 * 148) {
+    umma::gemm_bf16_kernel<128><<<dim3(M / 128, N / 128), 128, umma::gemm_smem_bytes<128>(), st>>>(A, lda, B, ldb,
+                                                                                                  C, ldc, K, err);
   } else {
-    umma::gemm_bf16_kernel<64><<<dim3(M / 128, N / 64), 128, 0, st>>>(A, lda, B, ldb, C, ldc, K, err);
+    umma::gemm_bf16_kernel<64><<<dim3(M / 128, N / 64), 128, umma::gemm_smem_bytes<64>(), st>>>(A, lda, B, ldb, C,
+                                                                                               ldc, K, err);
   }
   return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
 }
@@ -538,6 +578,8 @@ int brkga_gemm_bf16(const void* d_A, int32_t lda, const void* d_B, int32_t ldb, 
       ldb % 8 || ldc % 4)
     return BRKGA_ERR_INVALID_ARGUMENT;
   if (M == 0 || N == 0 || K == 0) return BRKGA_OK;
+  const int st = prepare_gemm();
+  if (st) return st;
   return gemm(static_cast<const __nv_bfloat16*>(d_A), lda, static_cast<const __nv_bfloat16*>(d_B), ldb, d_C, ldc, M,
               N, K, d_err, static_cast<cudaStream_t>(stream));
 }
@@ -579,7 +621,8 @@ int brkga_surrogate_create(const BrkgaProblem* problem, int32_t max_batch, int32
     s->inv_pth = mh > 0 ? (float)(1.0 / mh) : 1.f;
   }
   if (cudaFuncSetAttribute(features_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxGenes * 8) !=
-      cudaSuccess) {
+          cudaSuccess ||
+      prepare_gemm() != BRKGA_OK) {
     delete s;
     return BRKGA_ERR_CUDA;
   }
@@ -681,15 +724,15 @@ static int gradients(BrkgaSurrogate* s, int B, cudaStream_t st) {
   const int I = s->in_pad;
   loss_grad_dev_kernel<<<(B + 255) / 256, 256, 0, st>>>(s->y, s->t, s->n_valid, B, s->dy, s->loss);
   // output layer
-  col_reduce_kernel<<<(kH2 + 127) / 128, 128, 0, st>>>(s->Z2, s->dy, nullptr, nullptr, B, kH2, s->gw3);
-  col_reduce_kernel<<<1, 32, 0, st>>>(nullptr, s->dy, nullptr, nullptr, B, 1, s->gb3);
+  col_reduce(s->Z2, s->dy, nullptr, nullptr, B, kH2, s->gw3, st);
+  col_reduce(nullptr, s->dy, nullptr, nullptr, B, 1, s->gb3, st);
   out_backward_kernel<<<grid_for((long long)B * kH2), 256, 0, st>>>(s->Z2, s->dy, s->w3, B, kH2, s->dZ2b, s->dZ2Tb);
-  col_reduce_kernel<<<(kH2 + 127) / 128, 128, 0, st>>>(nullptr, s->dy, s->Z2, s->w3, B, kH2, s->gb2);
+  col_reduce(nullptr, s->dy, s->Z2, s->w3, B, kH2, s->gb2, st);
   // layer 2: dW2 = dZ2^T H1, dH1 = dZ2 W2
   if ((r = gemm(s->dZ2Tb, B, s->H1Tb, B, s->gW2, kH1, kH2, kH1, B, s->err, st))) return r;
   if ((r = gemm(s->dZ2b, kH2, s->W2Tb, kH2, s->dH1, kH1, B, kH1, kH2, s->err, st))) return r;
   relu_backward_kernel<<<grid_for((long long)B * kH1), 256, 0, st>>>(s->dH1, s->Z1, B, kH1, s->dZ1Tb);
-  col_reduce_kernel<<<(kH1 + 127) / 128, 128, 0, st>>>(s->dH1, nullptr, nullptr, nullptr, B, kH1, s->gb1);
+  col_reduce(s->dH1, nullptr, nullptr, nullptr, B, kH1, s->gb1, st);
   // layer 1: dW1 = dZ1^T X
   if ((r = gemm(s->dZ1Tb, B, s->XT, B, s->gW1, I, kH1, I, B, s->err, st))) return r;
   return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;

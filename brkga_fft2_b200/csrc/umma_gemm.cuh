@@ -5,7 +5,8 @@
 //   M % 128 == 0, N % BN == 0 (BN = 64 or 128), K % 64 == 0 (callers pad with zeros).
 //
 // One CTA of 128 threads per 128 x BN output tile.  Per 64-wide K step the
-// threads stage the A and B tiles in shared memory in the canonical K-major
+// threads stage the A and B tiles (two stages in dynamic shared memory, so
+// staging overlaps the previous step's MMAs) in the canonical K-major
 // "interleaved" layout (8 x 16-byte core matrices; core (row block, k chunk)
 // at (row_block * 8 + k_chunk) * 128 bytes, so the descriptor's leading byte
 // offset — next k chunk — is 128 B and its stride byte offset — next 8-row
@@ -82,20 +83,33 @@ __device__ __forceinline__ bool wait_parity(uint64_t* bar, uint32_t parity) {
   return false;
 }
 
+// Dynamic shared memory of gemm_bf16_kernel<BN>: two stages of A and B tiles.
+template <int BN>
+constexpr int gemm_smem_bytes() {
+  return 2 * (kTileM * kTileK + BN * kTileK) * 2;
+}
+
+// Two stages: while the tensor cores multiply stage kt, the threads stage
+// kt + 1 into the other buffer (after the MMAs of kt - 1, which read it,
+// have signalled their mbarrier).
 template <int BN>
 __global__ void __launch_bounds__(128) gemm_bf16_kernel(const __nv_bfloat16* __restrict__ A, int lda,
                                                         const __nv_bfloat16* __restrict__ B, int ldb,
                                                         float* __restrict__ C, int ldc, int K, int* err) {
-  static_assert(BN == 64 || BN == 128, "BN must be 64 or 128 (static shared memory <= 48 KB)");
-  constexpr int kCols = BN < 32 ? 32 : BN;  // tensor-memory columns (power of two >= 32)
-  __shared__ __align__(1024) uint4 sA[kTileM * kTileK / 8];
-  __shared__ __align__(1024) uint4 sB[BN * kTileK / 8];
-  __shared__ __align__(8) uint64_t bar;
+  static_assert(BN == 64 || BN == 128, "BN must be 64 or 128");
+  constexpr int kCols = BN;                    // tensor-memory columns (power of two >= 32)
+  constexpr int kAWords = kTileM * kTileK / 8;  // uint4 per A stage
+  constexpr int kBWords = BN * kTileK / 8;
+  extern __shared__ __align__(1024) uint4 smem_tiles[];
+  __shared__ __align__(8) uint64_t bar[2];
   __shared__ uint32_t tmem_base;
   __shared__ int s_fail, s_fail_kt;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int m0 = blockIdx.x * kTileM, n0 = blockIdx.y * BN;
+  // stage b: A tile at b * (kAWords + kBWords), B tile right after it
+  auto tileA = [&](int b) { return smem_tiles + b * (kAWords + kBWords); };
+  auto tileB = [&](int b) { return smem_tiles + b * (kAWords + kBWords) + kAWords; };
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
@@ -105,7 +119,8 @@ __global__ void __launch_bounds__(128) gemm_bf16_kernel(const __nv_bfloat16* __r
   }
   if (tid == 0) {
     s_fail = 0;
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar)) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar[0])) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar[1])) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -114,24 +129,30 @@ __global__ void __launch_bounds__(128) gemm_bf16_kernel(const __nv_bfloat16* __r
   const uint32_t tmem = tmem_base;
   constexpr uint32_t idesc = instr_desc_bf16(kTileM, BN);
 
-  const int ksteps = K / kTileK;
-  for (int kt = 0; kt < ksteps; ++kt) {
-    // stage A: 128 rows x 8 chunks of 8 bf16; chunk (r, c) -> core ((r/8)*8 + c), row r%8
+  // stage a 128 x 64 A tile and a BN x 64 B tile: chunk (r, c) of 8 bf16 -> core ((r/8)*8 + c), row r%8
+  auto stage = [&](int buf, int kt) {
     for (int i = tid; i < kTileM * 8; i += 128) {
       const int r = i >> 3, c = i & 7;
-      sA[((r >> 3) * 8 + c) * 8 + (r & 7)] =
+      tileA(buf)[((r >> 3) * 8 + c) * 8 + (r & 7)] =
           *reinterpret_cast<const uint4*>(A + (size_t)(m0 + r) * lda + kt * kTileK + c * 8);
     }
     for (int i = tid; i < BN * 8; i += 128) {
       const int r = i >> 3, c = i & 7;
-      sB[((r >> 3) * 8 + c) * 8 + (r & 7)] =
+      tileB(buf)[((r >> 3) * 8 + c) * 8 + (r & 7)] =
           *reinterpret_cast<const uint4*>(B + (size_t)(n0 + r) * ldb + kt * kTileK + c * 8);
     }
+  };
+
+  const int ksteps = K / kTileK;
+  stage(0, 0);
+  int last = -1;  // last k step whose MMAs were committed
+  for (int kt = 0; kt < ksteps; ++kt) {
+    const int buf = kt & 1;
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
     if (tid == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+      const uint32_t a0 = smem_u32(tileA(buf)), b0 = smem_u32(tileB(buf));
 #pragma unroll
       for (int s = 0; s < kTileK / 16; ++s) {
         // K = 16 is two 8-wide chunks: chunk 2s at +256*s bytes, the next one +128 B (LBO)
@@ -139,18 +160,34 @@ __global__ void __launch_bounds__(128) gemm_bf16_kernel(const __nv_bfloat16* __r
         const uint64_t bd = smem_desc(b0 + 256u * s, 128u, 1024u);
         mma_bf16(tmem, ad, bd, idesc, (kt > 0 || s > 0) ? 1u : 0u);
       }
-      commit_to(&bar);
+      commit_to(&bar[buf]);
     }
-    __syncwarp();
-    if (!wait_parity(&bar, (uint32_t)(kt & 1))) {
+    last = kt;
+    if (kt + 1 < ksteps) {
+      if (kt >= 1) {  // the other buffer was read by the MMAs of kt - 1
+        if (!wait_parity(&bar[buf ^ 1], (uint32_t)(((kt - 1) >> 1) & 1))) {
+          if (lane == 0) {
+            atomicExch(&s_fail, 1);
+            s_fail_kt = kt;
+          }
+        }
+        __syncthreads();
+        if (s_fail) break;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      }
+      stage(buf ^ 1, kt + 1);
+    }
+  }
+  // the MMAs of one thread complete in order: the last commit covers them all
+  if (!s_fail && last >= 0) {
+    if (!wait_parity(&bar[last & 1], (uint32_t)((last >> 1) & 1))) {
       if (lane == 0) {
         atomicExch(&s_fail, 1);
-        s_fail_kt = kt;
+        s_fail_kt = last;
       }
     }
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     __syncthreads();
-    if (s_fail) break;
   }
 
   if (!s_fail) {
@@ -177,8 +214,8 @@ __global__ void __launch_bounds__(128) gemm_bf16_kernel(const __nv_bfloat16* __r
     }
   } else if (tid == 0) {
     atomicExch(err, 3 /* BRKGA_ERR_CUDA */);
-    // let any MMA still in flight finish before the tensor memory is released
-    wait_parity(&bar, (uint32_t)(s_fail_kt & 1));
+    // let the MMAs still in flight finish before the tensor memory is released
+    if (last >= 0) wait_parity(&bar[last & 1], (uint32_t)((last >> 1) & 1));
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
