@@ -5,8 +5,8 @@
 //   M % 128 == 0, N % BN == 0 (BN = 64 or 128), K % 64 == 0 (callers pad with zeros).
 //
 // One CTA of 128 threads per 128 x BN output tile.  Per 64-wide K step the
-// threads stage the A and B tiles (two stages in dynamic shared memory, so
-// staging overlaps the previous step's MMAs) in the canonical K-major
+// threads copy the A and B tiles with cp.async (six buffers in dynamic shared
+// memory: four steps of copies in flight, two of MMAs) in the canonical K-major
 // "interleaved" layout (8 x 16-byte core matrices; core (row block, k chunk)
 // at (row_block * 8 + k_chunk) * 128 bytes, so the descriptor's leading byte
 // offset — next k chunk — is 128 B and its stride byte offset — next 8-row
@@ -83,15 +83,29 @@ __device__ __forceinline__ bool wait_parity(uint64_t* bar, uint32_t parity) {
   return false;
 }
 
-// Dynamic shared memory of gemm_bf16_kernel<BN>: two stages of A and B tiles.
+constexpr int kStages = 6;  // shared-memory buffers
+constexpr int kAhead = 4;   // K steps of copies in flight; the MMAs of kStages - kAhead steps may still run
+
+// Dynamic shared memory of gemm_bf16_kernel<BN>: kStages stages of A and B tiles.
 template <int BN>
 constexpr int gemm_smem_bytes() {
-  return 2 * (kTileM * kTileK + BN * kTileK) * 2;
+  return kStages * (kTileM * kTileK + BN * kTileK) * 2;
 }
 
-// Two stages: while the tensor cores multiply stage kt, the threads stage
-// kt + 1 into the other buffer (after the MMAs of kt - 1, which read it,
-// have signalled their mbarrier).
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem_dst)), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Pipeline: the threads keep kAhead K steps of tiles in flight as
+// asynchronous copies (cp.async, straight into shared memory) while one
+// thread issues the MMAs of the oldest complete step; a buffer is refilled
+// only after the MMAs that read it (kStages - kAhead steps earlier) have
+// signalled their mbarrier, so the MMAs of the last steps keep running.
 template <int BN>
 __global__ void __launch_bounds__(128) gemm_bf16_kernel(const __nv_bfloat16* __restrict__ A, int lda,
                                                         const __nv_bfloat16* __restrict__ B, int ldb,
@@ -101,9 +115,9 @@ __global__ void __launch_bounds__(128) gemm_bf16_kernel(const __nv_bfloat16* __r
   constexpr int kAWords = kTileM * kTileK / 8;  // uint4 per A stage
   constexpr int kBWords = BN * kTileK / 8;
   extern __shared__ __align__(1024) uint4 smem_tiles[];
-  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ __align__(8) uint64_t bar[kStages];
   __shared__ uint32_t tmem_base;
-  __shared__ int s_fail, s_fail_kt;
+  __shared__ int s_fail;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int m0 = blockIdx.x * kTileM, n0 = blockIdx.y * BN;
@@ -119,8 +133,8 @@ __global__ void __launch_bounds__(128) gemm_bf16_kernel(const __nv_bfloat16* __r
   }
   if (tid == 0) {
     s_fail = 0;
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar[0])) : "memory");
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar[1])) : "memory");
+    for (int b = 0; b < kStages; ++b)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar[b])) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -129,25 +143,31 @@ __global__ void __launch_bounds__(128) gemm_bf16_kernel(const __nv_bfloat16* __r
   const uint32_t tmem = tmem_base;
   constexpr uint32_t idesc = instr_desc_bf16(kTileM, BN);
 
-  // stage a 128 x 64 A tile and a BN x 64 B tile: chunk (r, c) of 8 bf16 -> core ((r/8)*8 + c), row r%8
+  // copy a 128 x 64 A tile and a BN x 64 B tile of step kt into stage buf:
+  // chunk (r, c) of 8 bf16 -> core ((r/8)*8 + c), row r%8
   auto stage = [&](int buf, int kt) {
-    for (int i = tid; i < kTileM * 8; i += 128) {
-      const int r = i >> 3, c = i & 7;
-      tileA(buf)[((r >> 3) * 8 + c) * 8 + (r & 7)] =
-          *reinterpret_cast<const uint4*>(A + (size_t)(m0 + r) * lda + kt * kTileK + c * 8);
+#pragma unroll
+    for (int j = 0; j < kTileM * 8 / 128; ++j) {
+      const int i = tid + 128 * j, r = i >> 3, c = i & 7;
+      cp_async16(tileA(buf) + ((r >> 3) * 8 + c) * 8 + (r & 7), A + (size_t)(m0 + r) * lda + kt * kTileK + c * 8);
     }
-    for (int i = tid; i < BN * 8; i += 128) {
-      const int r = i >> 3, c = i & 7;
-      tileB(buf)[((r >> 3) * 8 + c) * 8 + (r & 7)] =
-          *reinterpret_cast<const uint4*>(B + (size_t)(n0 + r) * ldb + kt * kTileK + c * 8);
+#pragma unroll
+    for (int j = 0; j < BN * 8 / 128; ++j) {
+      const int i = tid + 128 * j, r = i >> 3, c = i & 7;
+      cp_async16(tileB(buf) + ((r >> 3) * 8 + c) * 8 + (r & 7), B + (size_t)(n0 + r) * ldb + kt * kTileK + c * 8);
     }
   };
 
   const int ksteps = K / kTileK;
-  stage(0, 0);
+#pragma unroll
+  for (int p = 0; p < kAhead; ++p) {
+    if (p < ksteps) stage(p, p);
+    cp_async_commit();  // one group per step, empty ones included, so the group count stays uniform
+  }
   int last = -1;  // last k step whose MMAs were committed
   for (int kt = 0; kt < ksteps; ++kt) {
-    const int buf = kt & 1;
+    const int buf = kt % kStages;
+    cp_async_wait<kAhead - 1>();  // this thread's copies of step kt have landed
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
     if (tid == 0) {
@@ -163,28 +183,26 @@ __global__ void __launch_bounds__(128) gemm_bf16_kernel(const __nv_bfloat16* __r
       commit_to(&bar[buf]);
     }
     last = kt;
-    if (kt + 1 < ksteps) {
-      if (kt >= 1) {  // the other buffer was read by the MMAs of kt - 1
-        if (!wait_parity(&bar[buf ^ 1], (uint32_t)(((kt - 1) >> 1) & 1))) {
-          if (lane == 0) {
-            atomicExch(&s_fail, 1);
-            s_fail_kt = kt;
-          }
+    const int nk = kt + kAhead;  // the step to prefetch, into the buffer of step kt - (kStages - kAhead)
+    constexpr int kLag = kStages - kAhead;
+    if (nk < ksteps) {
+      if (kt >= kLag) {
+        const int pb = (kt - kLag) % kStages;
+        if (!wait_parity(&bar[pb], (uint32_t)(((kt - kLag) / kStages) & 1))) {
+          if (lane == 0) atomicExch(&s_fail, 1);
         }
         __syncthreads();
         if (s_fail) break;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       }
-      stage(buf ^ 1, kt + 1);
+      stage(nk % kStages, nk);
     }
+    cp_async_commit();
   }
   // the MMAs of one thread complete in order: the last commit covers them all
   if (!s_fail && last >= 0) {
-    if (!wait_parity(&bar[last & 1], (uint32_t)((last >> 1) & 1))) {
-      if (lane == 0) {
-        atomicExch(&s_fail, 1);
-        s_fail_kt = last;
-      }
+    if (!wait_parity(&bar[last % kStages], (uint32_t)((last / kStages) & 1))) {
+      if (lane == 0) atomicExch(&s_fail, 1);
     }
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     __syncthreads();
@@ -215,8 +233,9 @@ __global__ void __launch_bounds__(128) gemm_bf16_kernel(const __nv_bfloat16* __r
   } else if (tid == 0) {
     atomicExch(err, 3 /* BRKGA_ERR_CUDA */);
     // let the MMAs still in flight finish before the tensor memory is released
-    if (last >= 0) wait_parity(&bar[last & 1], (uint32_t)((last >> 1) & 1));
+    if (last >= 0) wait_parity(&bar[last % kStages], (uint32_t)((last / kStages) & 1));
   }
+  asm volatile("cp.async.wait_all;" ::: "memory");  // no copy may land after the CTA is gone
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0) {
