@@ -63,7 +63,7 @@ constexpr unsigned kFull = 0xFFFFFFFFu;
 
 struct RotDev {
   int h, w, mw;      // rows, columns, 32-bit words per mask row
-  int dens_row;      // first entry in dens[] (h entries)
+  int vt;            // first entry in vtest[]: h (row << 16 | longest run of the row), collision-test order
   int trun, ntrun;   // runs of ones of all rows in test order: truns[trun .. trun + ntrun)
   int mask_base;     // first word in maskbits[] (h * mw words)
   int imax, dmax;    // row with the longest run of ones and that length
@@ -102,7 +102,7 @@ struct Tables {
   const int32_t* nrot;
   const int32_t* best_rot;
   const RotDev* rot;        // [absolute type * 4 + rotation]
-  const uint16_t* dens;
+  const uint32_t* vtest;
   const uint2* truns;       // (start | length << 16, row) per run of ones
   const uint32_t* maskbits;
   const uint8_t* newbin_ok;
@@ -229,30 +229,36 @@ __device__ __forceinline__ uint32_t blocked(const uint32_t* row, int p0, int d) 
 
 // Necessary condition for the rotation to fit with its top row at ty: every
 // plate row it covers has a free run at least as long as the mask row's
-// longest run (numba_utils.py:50-94).  Widest row first, then bottom to top,
-// BRKGA_VAC_ILP rows per step so their loads overlap.
+// longest run (numba_utils.py:50-94).  Rows in the collision-test order
+// (widest row first, then coarse to fine from the bottom), BRKGA_VAC_ILP rows
+// per step so their loads overlap.
 __device__ __forceinline__ bool vacancy_ok(const uint16_t* vac, int ty, const RotDev& rd,
-                                           const uint16_t* dens) {
-  if (vac[ty + rd.imax] < rd.dmax) return false;
-  const uint16_t* d = dens + rd.dens_row;
-  const uint16_t* v = vac + ty;
-  int i = rd.h - 1;
-  for (; i >= BRKGA_VAC_ILP - 1; i -= BRKGA_VAC_ILP) {
+                                           const uint32_t* vtest) {
+  const uint32_t* v = vtest + rd.vt;
+  const uint16_t* row = vac + ty;
+  const int h = rd.h;
+  int i = 0;
+  for (; i + BRKGA_VAC_ILP <= h; i += BRKGA_VAC_ILP) {
     bool bad = false;
 #pragma unroll
-    for (int u = 0; u < BRKGA_VAC_ILP; ++u) bad |= v[i - u] < __ldg(d + i - u);
+    for (int u = 0; u < BRKGA_VAC_ILP; ++u) {
+      const uint32_t e = __ldg(v + i + u);
+      bad |= row[e >> 16] < (e & 0xFFFFu);
+    }
     if (bad) return false;
   }
-  for (; i >= 0; --i)
-    if (v[i] < __ldg(d + i)) return false;
+  for (; i < h; ++i) {
+    const uint32_t e = __ldg(v + i);
+    if (row[e >> 16] < (e & 0xFFFFu)) return false;
+  }
   return true;
 }
 
 // The bits of F (candidate columns base .. base + 31) at which the rotation
 // fits with its top row at plate row g0: every run of ones of the mask, in
-// test order (widest row, then bottom to top: plates fill from the bottom, so
-// those rows reject a blocked candidate soonest), clears the columns it would
-// overlap; BRKGA_TEST_ILP independent runs per step, stop when F is empty.
+// collision-test order (widest row, then the rows coarse to fine from the
+// bottom), clears the columns it would overlap; BRKGA_TEST_ILP independent
+// runs per step, stop when F is empty.
 __device__ __forceinline__ uint32_t word_free(const uint32_t* g0, int RS, int base, uint32_t F, const RotDev& rd,
                                               const uint2* truns) {
   const uint2* e = truns + rd.trun;
@@ -505,7 +511,7 @@ __device__ __forceinline__ unsigned long long search_plate(const Tables& tb, con
     // filter take part in the exact test of the others, and the first pair
     // with a free column is the bottom-most candidate's leftmost x.
     // Otherwise each lane tests its own candidate's words left to right.
-    const bool pass = ty >= 0 && vacancy_ok(vac, ty, rd, tb.dens);
+    const bool pass = ty >= 0 && vacancy_ok(vac, ty, rd, tb.vtest);
     const unsigned S = __ballot_sync(kFull, pass);
     if (!S) continue;
     const int nx = md.W - rd.w + 1, nwo = (nx + 31) >> 5;
@@ -975,7 +981,7 @@ struct BrkgaProblem {
   int32_t* d_nrot = nullptr;
   int32_t* d_best = nullptr;
   RotDev* d_rot = nullptr;
-  uint16_t* d_dens = nullptr;
+  uint32_t* d_vtest = nullptr;
   uint2* d_truns = nullptr;
   uint32_t* d_maskbits = nullptr;
   uint8_t* d_fits = nullptr;
@@ -1221,7 +1227,7 @@ struct Merged {
   std::vector<int32_t> gene_type, nrot, best;
   std::vector<double> thr, pt, pth, area, bin_area;
   std::vector<RotDev> rot;
-  std::vector<uint16_t> dens;
+  std::vector<uint32_t> vtest;
   std::vector<uint2> truns;
   std::vector<uint32_t> maskbits;
   std::vector<uint8_t> fits, newbin_ok;
@@ -1251,11 +1257,11 @@ void merge_instance(const BrkgaProblemDesc* d, Merged& g) {
         rd.h = h;
         rd.w = w;
         rd.mw = (w + 31) / 32;
-        rd.dens_row = (int)g.dens.size();
         rd.mask_base = (int)g.maskbits.size();
         rd.imax = 0;
         rd.dmax = 0;
         std::vector<std::vector<uint32_t>> row_runs(h);
+        std::vector<int> dens(h, 0);
         for (int i = 0; i < h; ++i) {
           int best = 0, j = 0;
           while (j < w) {
@@ -1268,7 +1274,7 @@ void merge_instance(const BrkgaProblemDesc* d, Merged& g) {
               ++j;
             }
           }
-          g.dens.push_back((uint16_t)best);
+          dens[i] = best;
           if (best > rd.dmax) {
             rd.dmax = best;
             rd.imax = i;
@@ -1280,13 +1286,27 @@ void merge_instance(const BrkgaProblemDesc* d, Merged& g) {
             g.maskbits.push_back(v);
           }
         }
-        // collision-test order: the widest row, then the others bottom to top
-        // (plates fill from the bottom, so those rows reject soonest)
+        // collision-test order: the widest row, then the rows coarse to fine
+        // from the bottom (every 16th, then every 8th, 4th, 2nd, the rest).
+        // Plates fill from the bottom, so low rows reject a blocked candidate
+        // soonest; spreading the first tests over the part's height catches
+        // a collision higher up without walking every row below it.
         rd.trun = (int)g.truns.size();
-        for (int ii = -1; ii < h; ++ii) {
-          const int i = ii < 0 ? rd.imax : h - 1 - ii;
-          if (ii >= 0 && i == rd.imax) continue;
-          for (uint32_t r : row_runs[i]) g.truns.push_back(make_uint2(r, (unsigned)i));
+        {
+          std::vector<int> order;
+          std::vector<char> used(h, 0);
+          order.push_back(rd.imax);
+          used[rd.imax] = 1;
+          for (int st = 16; st >= 1; st >>= 1)
+            for (int i = h - 1; i >= 0; i -= st)
+              if (!used[i]) {
+                order.push_back(i);
+                used[i] = 1;
+              }
+          for (int i : order)
+            for (uint32_t r : row_runs[i]) g.truns.push_back(make_uint2(r, (unsigned)i));
+          rd.vt = (int)g.vtest.size();
+          for (int i : order) g.vtest.push_back(((uint32_t)i << 16) | (uint32_t)dens[i]);
         }
         rd.ntrun = (int)g.truns.size() - rd.trun;
       }
@@ -1483,7 +1503,7 @@ int brkga_problem_create_multi(const BrkgaProblemDesc* descs, int32_t K, BrkgaPr
       (st = upload(pb, &pb->d_pt, g.pt)) || (st = upload(pb, &pb->d_pth, g.pth)) ||
       (st = upload(pb, &pb->d_area, g.area)) || (st = upload(pb, &pb->d_nrot, g.nrot)) ||
       (st = upload(pb, &pb->d_best, g.best)) || (st = upload(pb, &pb->d_rot, g.rot)) ||
-      (st = upload(pb, &pb->d_dens, g.dens)) || (st = upload(pb, &pb->d_truns, g.truns)) ||
+      (st = upload(pb, &pb->d_vtest, g.vtest)) || (st = upload(pb, &pb->d_truns, g.truns)) ||
       (st = upload(pb, &pb->d_maskbits, g.maskbits)) ||
       (st = upload(pb, &pb->d_fits, g.fits)) || (st = upload(pb, &pb->d_newbin_ok, g.newbin_ok)) ||
       (st = upload(pb, &pb->d_bin_area, g.bin_area)) || (st = configure(pb, 0, 0, -1))) {
@@ -1501,7 +1521,7 @@ int brkga_problem_create_multi(const BrkgaProblemDesc* descs, int32_t K, BrkgaPr
   tb.nrot = pb->d_nrot;
   tb.best_rot = pb->d_best;
   tb.rot = pb->d_rot;
-  tb.dens = pb->d_dens;
+  tb.vtest = pb->d_vtest;
   tb.truns = pb->d_truns;
   tb.maskbits = pb->d_maskbits;
   tb.newbin_ok = pb->d_newbin_ok;
