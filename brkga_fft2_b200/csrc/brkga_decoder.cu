@@ -56,7 +56,7 @@ constexpr int kResidentWarps = 32;  // automatic shape: 32 warps per SM (the reg
 constexpr int kMaxInst = BRKGA_MAX_INSTANCES;
 constexpr int kMaxCtasPerSm = 32;
 constexpr int kMaxSmemPlates = 8;
-constexpr int kDefaultTaskMax = 512;
+constexpr int kDefaultTaskMax = 8192;
 constexpr int kMaxTaskMax = 32 * 256;  // 32 candidates x the output words of the widest plate
 constexpr unsigned long long kKeyNone = ~0ull;
 constexpr unsigned kFull = 0xFFFFFFFFu;

@@ -214,7 +214,7 @@ int brkga_decode_multi_at(int32_t stage, const BrkgaProblem* problem, const floa
  *                   resident warps per SM, the register limit)
  *   smem_plates     plates of each item kept in shared memory (0..8, the
  *                   rest in the global pool; -1 = as many as fit, at most 4)
- *   task_max        0..8192, -1 = the default 512: a warp that tests 32
+ *   task_max        0..8192, -1 = the default 8192: a warp that tests 32
  *                   candidate rows deals the (candidate that passed the
  *                   vacancy filter, 32-column output word) pairs across its
  *                   lanes when there are at most task_max of them, else each

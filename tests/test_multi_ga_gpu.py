@@ -67,7 +67,7 @@ def test_autotune_picks_a_shape_and_keeps_results(torch, tmp_path):
     shapes = [(4, 2, 0), (4, 4, 1), (2, 16, 0), (0, 0, -1), (4, 32, 8)]  # the last cannot be resident
     res = autotune(md, flat, pops, shapes=shapes, task_max_values=(0, 256), cache_path=cache)
     assert not res["cached"] and len(res["table"]) == 6
-    assert res["config"] in [(w, c, s, t if t >= 0 else 512) for w, c, s, t, _ in res["table"]]
+    assert res["config"] in [(w, c, s, t if t >= 0 else 8192) for w, c, s, t, _ in res["table"]]
     w, c, s, _, t = md.launch_config()
     assert t == res["config"][3]
     if res["config"][0]:

@@ -79,7 +79,7 @@ def test_launch_configs_give_identical_results(multi, cfg):
         assert ctas == cfg[1]
     if cfg[2] >= 0:
         assert plates == cfg[2]
-    assert task_max == (cfg[3] if cfg[3] >= 0 else 512)
+    assert task_max == (cfg[3] if cfg[3] >= 0 else 8192)
     out, log = _run(torch, md, chroms, POPS)
     _check(md, POPS, out, log, ref)
     md.set_launch_config()
