@@ -227,16 +227,19 @@ __device__ __forceinline__ uint32_t blocked(const uint32_t* row, int p0, int d) 
 #define BRKGA_VAC_ILP 4
 #endif
 
-// Necessary condition for the rotation to fit with its top row at ty: every
-// plate row it covers has a free run at least as long as the mask row's
-// longest run (numba_utils.py:50-94).  Rows in the collision-test order
-// (widest row first, then coarse to fine from the bottom), BRKGA_VAC_ILP rows
-// per step so their loads overlap.
+// Necessary condition for the rotation to fit with its top row at ty: the
+// plate rows it covers have free runs at least as long as the mask rows'
+// longest runs (numba_utils.py:50-94).  The first kVacRows rows of the
+// collision-test order (widest row, then coarse to fine from the bottom)
+// are checked, BRKGA_VAC_ILP per step so their loads overlap: a candidate
+// that fails the filter fails within them almost always, and one that slips
+// through is rejected by the exact test.
+constexpr int kVacRows = 32;
 __device__ __forceinline__ bool vacancy_ok(const uint16_t* vac, int ty, const RotDev& rd,
                                            const uint32_t* vtest) {
   const uint32_t* v = vtest + rd.vt;
   const uint16_t* row = vac + ty;
-  const int h = rd.h;
+  const int h = min(rd.h, kVacRows);
   int i = 0;
   for (; i + BRKGA_VAC_ILP <= h; i += BRKGA_VAC_ILP) {
     bool bad = false;
