@@ -20,18 +20,21 @@
 //      gene) 64-bit keys in shared memory -> per-(chromosome, machine) part
 //      order (placement.py:118-135).  order_items_kernel then sorts the
 //      (chromosome, machine) items of all instances by part count.
-//   2. decode_kernel       persistent CTAs of 4 warps pulling items, longest
-//      first, from a device counter.  A plate is L rows of ceil(W/32)+2
-//      32-bit words (bit x of a row = cell x); the first S plates of an item
-//      live in shared memory, further ones in a global pool.  For each part:
-//      first-fit over plates (area filter, then the collision search), else a
-//      new plate with the best rotation at (0, L-1).  The collision search
-//      splits (rotation, 32 candidate rows) chunks over the warps; a lane
-//      tests one candidate top row: vacancy filter, then the exact
-//      run-dilation test word by word, giving the leftmost free x.  Results
-//      are merged with a 64-bit lexicographic key (newLen, -y, x, rotation)
-//      by atomicMin in shared memory, which is the reference's rotation rule
-//      (binClassNew.py:101-117) — see key_of().
+//   2. decode_kernel       persistent CTAs of 2 or 4 warps (the launch
+//      shape), one (chromosome, machine) item at a time, longest first, from
+//      a device counter.  A plate is L rows of ceil(W/32)+2 32-bit words (bit
+//      x of a row = cell x); the first S plates of an item live in shared
+//      memory, further ones in a global pool.  For each part: first-fit over
+//      plates (area filter, then the collision search), else a new plate with
+//      the best rotation at (0, L-1).  The collision search splits (rotation,
+//      32 candidate rows) chunks over the warps; a lane runs the vacancy
+//      filter of one candidate top row, then the (surviving candidate,
+//      32-column word) pairs are dealt to the lanes for the exact
+//      run-dilation test, mask rows coarse to fine from the bottom; the first
+//      pair with a free column gives the bottom-most candidate and its
+//      leftmost x.  Results are merged with a 64-bit lexicographic key
+//      (newLen, -y, x, rotation) by atomicMin in shared memory, which is the
+//      reference's rotation rule (binClassNew.py:101-117) — see key_of().
 //   3. reduce_kernel       max over machines, 1e16 for infeasible chromosomes.
 
 #include <cuda_runtime.h>
