@@ -2,7 +2,7 @@
 """Surrogate screening benchmark: time for the screened GPU GA to reach the
 best makespan the plain GPU GA finds in its first G generations.
 
-    python bench_ga.py [--workload P200M6] [--pop 1000] [--generations 200] [--seeds 1]
+    python bench_ga.py [--workload P200M6] [--pop 1000] [--generations 200] [--seeds 3]
 
 Both runs use the same instance, GA parameters (elites ceil(0.1 pop), mutants
 ceil(0.15 pop), rho 0.7 as BRKGA_alg3.py:618) and decoder; each generation is
@@ -29,7 +29,7 @@ def main():
     ap.add_argument("--workload", default="P200M6")
     ap.add_argument("--pop", type=int, default=1000)
     ap.add_argument("--generations", type=int, default=200)
-    ap.add_argument("--seeds", type=int, default=1)
+    ap.add_argument("--seeds", type=int, default=3)
     ap.add_argument("--oversample", type=int, default=5)
     ap.add_argument("--train-steps", type=int, default=8)
     args = ap.parse_args()
