@@ -1100,12 +1100,14 @@ int configure(BrkgaProblem* pb, int warps_req, int ctas_req, int plates_req) {
   cudaDeviceProp prop;
   if (cudaGetDeviceProperties(&prop, pb->device) != cudaSuccess) return BRKGA_ERR_CUDA;
   pb->sm_count = prop.multiProcessorCount;
-  int Lmax = 0, RSmax = 0;
+  // A plate of machine m uses its own L x RS words, then L vacancy entries:
+  // a slot holds the largest plate of any machine (not Lmax x RSmax, which
+  // for a tall plate beside a wide one is far more than either needs).
+  int Lmax = 0, slot_vac_off = 0;
   for (const MachDev& m : pb->mach) {
     Lmax = std::max(Lmax, m.L);
-    RSmax = std::max(RSmax, m.RS);
+    slot_vac_off = std::max(slot_vac_off, m.L * m.RS);
   }
-  const int slot_vac_off = Lmax * RSmax;
   const int slot_words = (int)align_up((size_t)slot_vac_off + (size_t)(Lmax + 1) / 2, 4);
   const size_t slot_bytes = (size_t)slot_words * 4;
   cudaFuncAttributes fa4, fa2;
