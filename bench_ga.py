@@ -3,13 +3,23 @@
 best makespan the plain GPU GA finds in its first G generations.
 
     python bench_ga.py [--workload P200M6] [--pop 1000] [--generations 200] [--seeds 3]
+                       [--screened-limit 2.0]
 
 Both runs use the same instance, GA parameters (elites ceil(0.1 pop), mutants
 ceil(0.15 pop), rho 0.7 as BRKGA_alg3.py:618) and decoder; each generation is
 a CUDA-graph replay, timed with CUDA events on the GPU timeline.  The screened
 run breeds an oversampled pool and decodes exactly only the best-predicted
-rows; every makespan either run reports comes from the exact decoder.
-Prints one JSON line.
+rows; every makespan either run reports comes from the exact decoder.  The
+screened run stops at the target or after screened-limit x generations; a run
+that never reaches the target has ratio Infinity.
+
+``ratio`` is the metric as specified: the screened run's time to the plain
+run's 200-generation best over the plain run's time for all 200 generations.
+When the plain run finds that best early and then stalls, a run identical to
+it (screening never on: the screened GA then replays the plain GA exactly)
+scores the same early fraction.  ``ratio_vs_plain_hit`` therefore divides by
+the time at which the plain run itself first reached that makespan: below 1
+only when screening got there sooner.  Prints one JSON line.
 """
 from __future__ import annotations
 
@@ -31,7 +41,14 @@ def main():
     ap.add_argument("--generations", type=int, default=200)
     ap.add_argument("--seeds", type=int, default=3)
     ap.add_argument("--oversample", type=int, default=5)
-    ap.add_argument("--train-steps", type=int, default=8)
+    ap.add_argument("--train-steps", default="8",
+                    help="surrogate training steps per generation; a comma list runs one screened GA per value "
+                         "against the same plain run")
+    ap.add_argument("--explore", default="0",
+                    help="share of the decoded rows spread over the lower-ranked pool; a comma list runs one "
+                         "screened GA per value (and per training budget)")
+    ap.add_argument("--screened-limit", type=float, default=2.0,
+                    help="the screened run may use up to this many times the plain run's generations")
     args = ap.parse_args()
     import torch
     from brkga_fft2_b200 import build, instances, pack_problem
@@ -41,6 +58,7 @@ def main():
     pk = pack_problem(inst.problem_data, inst.nb_parts, inst.nb_machines, inst.thresholds, inst.instance_parts)
     P = args.pop
     ne, nm = math.ceil(0.1 * P), math.ceil(0.15 * P)
+    variants = [(int(t), float(x)) for t in str(args.train_steps).split(",") for x in str(args.explore).split(",")]
     runs = []
     for seed in range(args.seeds):
         plain = DeviceBRKGA(None, inst.nb_parts, inst.nb_machines, inst.thresholds, inst.instance_parts,
@@ -49,28 +67,52 @@ def main():
         plain.fit()
         target = plain.best_fitness
         t_plain = plain.history["time"][-1]
-        scr = DeviceBRKGA(None, inst.nb_parts, inst.nb_machines, inst.thresholds, inst.instance_parts,
-                          num_generations=args.generations, num_individuals=P, num_elites=ne, num_mutants=nm,
-                          eliteCProb=0.7, seed=seed, packed=pk, screening=True, oversample=args.oversample,
-                          train_steps=args.train_steps, target=target)
-        scr.fit()
-        mins = np.array(scr.history["min"])
-        hit = np.flatnonzero(mins <= target)
-        t_scr = scr.history["time"][int(hit[0])] if hit.size else float("inf")
-        # best makespan of each run at the plain run's wall time
-        sp = np.array(scr.history["spearman"][1:])
-        runs.append({"seed": seed, "target": target, "plain_s": t_plain, "plain_gen_ms": 1000 * t_plain / args.generations,
-                     "screened_s": t_scr, "screened_generations": int(hit[0]) if hit.size else None,
-                     "screened_best": float(mins.min()), "ratio": t_scr / t_plain,
-                     "screened_gen_ms": 1000 * scr.history["time"][-1] / max(len(mins) - 1, 1),
-                     "screen_fraction": float(np.mean([m == "screen" for m in scr.history["mode"][1:]])),
-                     "spearman_median": float(np.nanmedian(sp)) if np.isfinite(sp).any() else None,
-                     "mae_median": float(np.nanmedian(scr.history["mae"][1:]))})
+        p_hit = int(np.flatnonzero(np.array(plain.history["min"]) <= target)[0])
+        t_plain_hit = plain.history["time"][p_hit]
+        del plain
         torch.cuda.empty_cache()
-    ratios = [r["ratio"] for r in runs]
+        for ts, ex in variants:
+            runs.append(screened_run(args, inst, pk, P, ne, nm, seed, ts, ex, target, t_plain, p_hit, t_plain_hit))
+            torch.cuda.empty_cache()
+    by_variant = {}
+    for ts, ex in variants:
+        rs = [r for r in runs if (r["train_steps"], r["explore"]) == (ts, ex)]
+        by_variant[f"train_steps={ts},explore={ex:g}"] = {
+            "ratio_median": float(np.median([r["ratio"] for r in rs])),
+            "ratio_vs_plain_hit_median": float(np.median([r["ratio_vs_plain_hit"] for r in rs])),
+            "reached": sum(math.isfinite(r["ratio"]) for r in rs)}
+    first = by_variant[f"train_steps={variants[0][0]},explore={variants[0][1]:g}"]
     print(json.dumps({"metric": "time to plain-GA best makespan, screened vs plain", "workload": args.workload,
                       "pop": P, "generations": args.generations, "oversample": args.oversample,
-                      "ratio_median": float(np.median(ratios)), "runs": runs}))
+                      "screened_limit": args.screened_limit, "train_steps": variants[0][0],
+                      "explore": variants[0][1], "reached": first["reached"], "ratio_median": first["ratio_median"],
+                      "ratio_vs_plain_hit_median": first["ratio_vs_plain_hit_median"],
+                      "by_variant": by_variant, "runs": runs}))
+
+
+def screened_run(args, inst, pk, P, ne, nm, seed, train_steps, explore, target, t_plain, p_hit, t_plain_hit):
+    """One screened GA against the plain run's target; a dict for the JSON line."""
+    from brkga_fft2_b200.ga import DeviceBRKGA
+    scr = DeviceBRKGA(None, inst.nb_parts, inst.nb_machines, inst.thresholds, inst.instance_parts,
+                      num_generations=max(1, int(round(args.generations * args.screened_limit))),
+                      num_individuals=P, num_elites=ne, num_mutants=nm,
+                      eliteCProb=0.7, seed=seed, packed=pk, screening=True, oversample=args.oversample,
+                      train_steps=train_steps, explore=explore, target=target)
+    scr.fit()
+    mins = np.array(scr.history["min"])
+    hit = np.flatnonzero(mins <= target)
+    t_scr = scr.history["time"][int(hit[0])] if hit.size else float("inf")
+    sp = np.array(scr.history["spearman"][1:])
+    return {"seed": seed, "train_steps": train_steps, "explore": explore, "target": target, "plain_s": t_plain,
+            "plain_gen_ms": 1000 * t_plain / args.generations,
+            "screened_s": t_scr, "screened_generations": int(hit[0]) if hit.size else None,
+            "screened_best": float(mins.min()), "ratio": t_scr / t_plain,
+            "plain_hit_generation": p_hit, "plain_hit_s": t_plain_hit,
+            "ratio_vs_plain_hit": t_scr / t_plain_hit if t_plain_hit > 0 else float("inf"),
+            "screened_gen_ms": 1000 * scr.history["time"][-1] / max(len(mins) - 1, 1),
+            "screen_fraction": float(np.mean([m == "screen" for m in scr.history["mode"][1:]])),
+            "spearman_median": float(np.nanmedian(sp)) if np.isfinite(sp).any() else None,
+            "mae_median": float(np.nanmedian(scr.history["mae"][1:]))}
 
 
 if __name__ == "__main__":

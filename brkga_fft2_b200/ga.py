@@ -8,7 +8,10 @@ exact makespans.  Its Spearman correlation and mean absolute error on the
 decoded rows are logged for every generation (``history['spearman']``,
 ``history['mae']``), and screening is switched off while the mean Spearman of
 the last ``check_every`` generations stays below ``spearman_threshold``
-(the surrogate keeps learning from plain generations meanwhile).
+(the surrogate keeps learning from plain generations meanwhile).  With
+``explore > 0`` that share of the decoded rows is not the surrogate's top but
+spread evenly over the rest of the ranked pool, which keeps lower-ranked
+offspring in the population.
 
 With ``audit_fraction > 0`` every generation also copies an evenly spaced
 sample of the rows it decoded (that fraction of them), with their exact
@@ -49,7 +52,8 @@ class DeviceBRKGA:
                  packed: Optional[PackedProblem] = None, device=None, screening: bool = False,
                  oversample: int = 5, train_steps: int = 8, train_batch: int = 512, lr: float = 1e-3,
                  spearman_threshold: float = 0.3, check_every: int = 5, warmup_generations: int = 5,
-                 buffer_capacity: int = 200_000, target: Optional[float] = None, audit_fraction: float = 0.0):
+                 buffer_capacity: int = 200_000, target: Optional[float] = None, audit_fraction: float = 0.0,
+                 explore: float = 0.0):
         import torch
         del collision_backend, eval_mode, eval_workers, eval_chunksize
         self.torch = torch
@@ -122,6 +126,16 @@ class DeviceBRKGA:
             self.stats_dev = torch.full((self.num_generations + 1, 2), float("nan"), dtype=torch.float64, device=dev)
             self.surrogate = Surrogate(self.decoder.native, max_batch=max(self.train_batch, 1024),
                                        buffer_capacity=buffer_capacity, seed=self.seed ^ 0x5EED)
+            # exploration: that share of the decoded rows is spread evenly over the
+            # pool's lower-ranked candidates instead of taken from its top
+            cand = self.pool_rows - self.num_elites
+            self.n_explore = min(rows, max(0, int(round(float(explore) * rows))))
+            if self.n_explore:
+                top = rows - self.n_explore
+                sel = np.arange(rows, dtype=np.int64)
+                sel[top:] = top + (np.arange(self.n_explore) * (cand - top)) // self.n_explore
+                self.sel_idx = torch.from_numpy(sel).to(dev)
+                self.order_sel = torch.zeros(rows, dtype=torch.int32, device=dev)
 
     # ---- kernels of one generation ------------------------------------------------
     @staticmethod
@@ -206,7 +220,11 @@ class DeviceBRKGA:
         cand = self.pool_rows - ne
         self.surrogate.predict(self.pool[ne:], out=self.pred)
         self._rank(self.pred, cand, self.order_pool)
-        abi.check(self.lib.brkga_ga_gather(self._ptr(self.pool[ne:]), self._ptr(self.order_pool), rows, K,
+        order = self.order_pool
+        if self.n_explore:
+            self.torch.index_select(self.order_pool, 0, self.sel_idx, out=self.order_sel)
+            order = self.order_sel
+        abi.check(self.lib.brkga_ga_gather(self._ptr(self.pool[ne:]), self._ptr(order), rows, K,
                                            self._ptr(self.pop[nxt][ne:]), self._stream()), "brkga_ga_gather")
         self.pop[nxt][:ne].copy_(self.pool[:ne])
         self.fitness_buf[nxt][:ne].copy_(self.pool_fit[:ne])
