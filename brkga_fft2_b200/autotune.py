@@ -1,9 +1,12 @@
 """Launch-shape autotuner for the decode kernel.
 
 The decode kernel has four knobs (``brkga_set_launch_config``).  Warps per
-item (2 or 4) trade the latency of one (chromosome, machine) item against
+item (1, 2 or 4) trade the latency of one (chromosome, machine) item against
 throughput: 4 finish an item sooner, 2 waste fewer lanes on speculative row
-chunks, so 2 win once the items fill several waves of resident CTAs.  More
+chunks, so 2 win once the items fill several waves of resident CTAs, and 1
+(no CTA barrier at all) wins by a few per cent only when they fill some 20
+waves (measured: 64 uneven instances x 256 chromosomes, 52,000 items, 43.8
+against 46.5 ms).  More
 resident CTAs per SM hide more latency, more plates per item in shared
 memory keep more collision searches off the global pool, and both draw on
 the same 228 KB of shared memory per SM, whose share per plate grows with
@@ -34,7 +37,8 @@ from . import abi
 
 # (warps per item, CTAs per SM, plates per item in shared memory)
 DEFAULT_SHAPES: Tuple[Tuple[int, int, int], ...] = ((4, 8, 0), (4, 8, 1), (4, 8, 2), (4, 6, 1), (4, 6, 2),
-                                                    (2, 16, 0), (2, 16, 1), (2, 12, 1), (2, 12, 2), (2, 8, 2))
+                                                    (2, 16, 0), (2, 16, 1), (2, 12, 1), (2, 12, 2), (2, 8, 2),
+                                                    (1, 32, 0))
 DEFAULT_TASK_MAX: Tuple[int, ...] = (0, 64, 256, 1024, 8192)
 
 

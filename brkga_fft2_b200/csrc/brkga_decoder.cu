@@ -20,7 +20,7 @@
 //      gene) 64-bit keys in shared memory -> per-(chromosome, machine) part
 //      order (placement.py:118-135).  order_items_kernel then sorts the
 //      (chromosome, machine) items of all instances by part count.
-//   2. decode_kernel       persistent CTAs of 2 or 4 warps (the launch
+//   2. decode_kernel       persistent CTAs of 1, 2 or 4 warps (the launch
 //      shape), one (chromosome, machine) item at a time, longest first, from
 //      a device counter.  A plate is L rows of ceil(W/32)+2 32-bit words (bit
 //      x of a row = cell x); the first S plates of an item live in shared
@@ -53,7 +53,7 @@ namespace {
 constexpr int kMaxMachines = 255;
 constexpr int kMaxGenes = 8192;     // bitonic sort buffer: 8192 x 8 B = 64 KB shared memory
 constexpr int kMaxSide = 8191;      // 13-bit fields of the selection key
-constexpr int kMaxItemWarps = 4;   // decode CTAs have 2 or 4 warps (one item per CTA)
+constexpr int kMaxItemWarps = 4;   // decode CTAs have 1, 2 or 4 warps (one item per CTA)
 constexpr int kGreedyThreads = 128;
 constexpr int kResidentWarps = 32;  // automatic shape: 32 warps per SM (the register limit at 64 per thread)
 constexpr int kMaxInst = BRKGA_MAX_INSTANCES;
@@ -647,8 +647,8 @@ struct ItemCtx {
 
 // The tables go by value (every access has a fixed parameter offset); only
 // the per-launch instance array, which is searched, is a grid constant.
-// kThreads = 64 or 128 (2 or 4 warps per item); 32 resident warps per SM
-// cap the kernel at 64 registers, which it fits without spilling.
+// kThreads = 32, 64 or 128 (1, 2 or 4 warps per item); 32 resident warps
+// per SM cap the kernel at 64 registers, which it fits without spilling.
 template <int kThreads>
 __global__ void __launch_bounds__(kThreads, kResidentWarps * 32 / kThreads)
     decode_kernel(const Tables tb, const __grid_constant__ Run run) {
@@ -970,9 +970,9 @@ struct BrkgaProblem {
   int sm_count = 0;
   int req_warps = 0, req_ctas = 0, req_plates = -1;  // requested launch shape (0 / 0 / -1 = automatic)
   int task_max = kDefaultTaskMax;
-  Shape shape[2];      // 4 and 2 warps per item
-  int max_slots = 0;   // resident CTAs of the larger shape (per-CTA plate scalars in the workspace)
-  int min_S = 0;       // fewer plates in shared memory of the two shapes (pool sizing)
+  Shape shape[3];      // 4, 2 and 1 warps per item
+  int max_slots = 0;   // resident CTAs of the largest usable shape (per-CTA plate scalars in the workspace)
+  int min_S = 0;       // fewest plates in shared memory of the usable shapes (pool sizing)
   int slot_words = 0, slot_vac_off = 0;
   std::vector<MachDev> mach;
   std::vector<void*> allocations;
@@ -1083,12 +1083,14 @@ int prepare_kernel(size_t dyn_max) {
 }
 
 int occupancy(int warps, size_t smem, int* occ) {
-  const cudaError_t e = warps == 2 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, decode_kernel<64>, 64, smem)
-                                   : cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, decode_kernel<128>, 128, smem);
+  const cudaError_t e =
+      warps == 1   ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, decode_kernel<32>, 32, smem)
+      : warps == 2 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, decode_kernel<64>, 64, smem)
+                   : cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, decode_kernel<128>, 128, smem);
   return e == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
 }
 
-// Launch shapes of the decode kernel, one per CTA size (4 and 2 warps per
+// Launch shapes of the decode kernel, one per CTA size (4, 2 and 1 warps per
 // item): resident CTAs per SM and plates per item kept in shared memory.
 // For the requested CTA size (warps_req), ctas_req = 0 picks the CTAs
 // automatically (32 resident warps per SM, the register limit) and
@@ -1110,17 +1112,20 @@ int configure(BrkgaProblem* pb, int warps_req, int ctas_req, int plates_req) {
   }
   const int slot_words = (int)align_up((size_t)slot_vac_off + (size_t)(Lmax + 1) / 2, 4);
   const size_t slot_bytes = (size_t)slot_words * 4;
-  cudaFuncAttributes fa4, fa2;
+  cudaFuncAttributes fa4, fa2, fa1;
   if (cudaFuncGetAttributes(&fa4, decode_kernel<128>) != cudaSuccess ||
-      cudaFuncGetAttributes(&fa2, decode_kernel<64>) != cudaSuccess)
+      cudaFuncGetAttributes(&fa2, decode_kernel<64>) != cudaSuccess ||
+      cudaFuncGetAttributes(&fa1, decode_kernel<32>) != cudaSuccess)
     return BRKGA_ERR_CUDA;
-  const size_t static_smem = std::max(fa4.sharedSizeBytes, fa2.sharedSizeBytes);
+  const size_t static_smem = std::max({fa4.sharedSizeBytes, fa2.sharedSizeBytes, fa1.sharedSizeBytes});
   const size_t per_sm = prop.sharedMemPerMultiprocessor;
   const size_t per_block_max = prop.sharedMemPerBlockOptin - static_smem;  // dynamic part
   const size_t reserve = 1024 + static_smem;  // per-block system reservation + static shared variables
   const int max_fit = (int)std::min<size_t>(kMaxSmemPlates, per_block_max / slot_bytes);
   int st;
-  if ((st = prepare_kernel<128>(per_block_max)) || (st = prepare_kernel<64>(per_block_max))) return st;
+  if ((st = prepare_kernel<128>(per_block_max)) || (st = prepare_kernel<64>(per_block_max)) ||
+      (st = prepare_kernel<32>(per_block_max)))
+    return st;
   if (cudaFuncSetAttribute(assign_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxGenes * 8) !=
       cudaSuccess)
     return BRKGA_ERR_CUDA;
@@ -1132,9 +1137,9 @@ int configure(BrkgaProblem* pb, int warps_req, int ctas_req, int plates_req) {
     if (share <= reserve) return 0;
     return (int)std::min<size_t>((share - reserve) / slot_bytes, (size_t)max_fit);
   };
-  Shape shapes[2];
-  for (int v = 0; v < 2; ++v) {
-    const int warps = v == 0 ? 4 : 2;
+  Shape shapes[3];
+  for (int v = 0; v < 3; ++v) {
+    const int warps = 4 >> v;
     const int auto_ctas = kResidentWarps / warps;
     const bool req = warps_req == warps;
     const int creq = req ? ctas_req : 0, preq = req ? plates_req : -1;
@@ -1168,10 +1173,16 @@ int configure(BrkgaProblem* pb, int warps_req, int ctas_req, int plates_req) {
   }
   pb->slot_vac_off = slot_vac_off;
   pb->slot_words = slot_words;
-  pb->shape[0] = shapes[0];
-  pb->shape[1] = shapes[1];
-  pb->max_slots = std::max(shapes[0].n_slots, shapes[1].n_slots);
-  pb->min_S = std::min(shapes[0].S, shapes[1].S);
+  for (int v = 0; v < 3; ++v) pb->shape[v] = shapes[v];
+  // The automatic choice uses the 4- and 2-warp shapes; the 1-warp shape only
+  // when requested, so its 32 CTAs per SM size the per-CTA scratch only then.
+  const int usable = warps_req == 1 ? 3 : 2;
+  pb->max_slots = 0;
+  pb->min_S = shapes[0].S;
+  for (int v = 0; v < usable; ++v) {
+    pb->max_slots = std::max(pb->max_slots, shapes[v].n_slots);
+    pb->min_S = std::min(pb->min_S, shapes[v].S);
+  }
   pb->req_warps = warps_req;
   pb->req_ctas = ctas_req;
   pb->req_plates = plates_req;
@@ -1184,6 +1195,7 @@ int configure(BrkgaProblem* pb, int warps_req, int ctas_req, int plates_req) {
 const Shape& pick_shape(const BrkgaProblem* pb, int64_t items) {
   if (pb->req_warps == 4) return pb->shape[0];
   if (pb->req_warps == 2) return pb->shape[1];
+  if (pb->req_warps == 1) return pb->shape[2];
   return items > 3 * (int64_t)pb->shape[0].n_slots ? pb->shape[1] : pb->shape[0];
 }
 
@@ -1411,7 +1423,8 @@ int launch(const BrkgaProblem* pb, int stage, const Run& run, cudaStream_t s) {
   if (stage == 0 || stage == 2) {
     const Shape& sh = pick_shape(pb, run.n_items);
     const int grid = (int)std::min<int64_t>(sh.n_slots, run.n_items);
-    if (sh.warps == 2) decode_kernel<64><<<grid, 64, sh.smem, s>>>(pb->tb, run);
+    if (sh.warps == 1) decode_kernel<32><<<grid, 32, sh.smem, s>>>(pb->tb, run);
+    else if (sh.warps == 2) decode_kernel<64><<<grid, 64, sh.smem, s>>>(pb->tb, run);
     else decode_kernel<128><<<grid, 128, sh.smem, s>>>(pb->tb, run);
   }
   if (stage == 0 || stage == 3) reduce_kernel<<<(run.n_rows + 255) / 256, 256, 0, s>>>(pb->tb, run);
@@ -1557,7 +1570,8 @@ int brkga_problem_instances(const BrkgaProblem* pb, int32_t* K) {
 
 int brkga_set_launch_config(BrkgaProblem* pb, int32_t warps_per_item, int32_t ctas_per_sm, int32_t smem_plates,
                             int32_t task_max) {
-  if (!pb || (warps_per_item != 0 && warps_per_item != 2 && warps_per_item != 4) || ctas_per_sm < 0 ||
+  if (!pb || (warps_per_item != 0 && warps_per_item != 1 && warps_per_item != 2 && warps_per_item != 4) ||
+      ctas_per_sm < 0 ||
       ctas_per_sm > kMaxCtasPerSm || smem_plates < -1 || smem_plates > kMaxSmemPlates || task_max < -1 ||
       task_max > kMaxTaskMax)
     return BRKGA_ERR_INVALID_ARGUMENT;

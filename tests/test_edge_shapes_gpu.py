@@ -4,7 +4,7 @@ and on the full-size large-stress population, bit for bit against the oracle.
 Edge instances: every row, makespans and placements, in both threshold modes,
 with adversarial keys (ties, signed zeros, machine keys on the float32
 thresholds), under launch shapes that take every path of the plate search —
-2- and 4-warp CTAs, plates in shared memory and in the global pool, the
+1-, 2- and 4-warp CTAs, plates in shared memory and in the global pool, the
 (candidate, word) pairs dealt across lanes and, with task_max 0, each lane
 testing its own candidate.  Full size: P400M8 (400 parts up to 240x240
 cells, 8 plates of 600x600) at population 4096 in one launch — every 8th row
@@ -22,7 +22,7 @@ from tests.test_placement_check_cpu import special_keys
 pytestmark = pytest.mark.gpu
 
 # (warps per item, CTAs per SM, plates in shared memory, task_max); 0 / -1 = automatic
-SHAPES = [(0, 0, -1, -1), (2, 0, -1, -1), (4, 0, 0, 0), (4, 1, -1, 64)]
+SHAPES = [(0, 0, -1, -1), (2, 0, -1, -1), (4, 0, 0, 0), (4, 1, -1, 64), (1, 0, -1, -1)]
 
 
 @pytest.fixture(scope="module")

@@ -65,7 +65,7 @@ def test_uneven_instances_match_oracle(multi):
 
 
 CONFIGS = [(4, 1, 0, -1), (4, 2, 1, 0), (2, 4, -1, 64), (4, 8, 0, 8192), (2, 16, 0, 1), (0, 0, -1, -1),
-           (2, 0, -1, -1), (4, 0, 2, -1)]
+           (2, 0, -1, -1), (4, 0, 2, -1), (1, 0, -1, -1), (1, 4, 1, 64), (1, 32, 0, 0)]
 
 
 @pytest.mark.parametrize("cfg", CONFIGS)
