@@ -301,6 +301,26 @@ __device__ __forceinline__ int first_free_x(const uint32_t* grid, int RS, int W,
   return -1;
 }
 
+// Longest run of ones in x, branch-free: p_s marks the starts of runs of at
+// least s ones (s = 1, 2, 4, 8, 16); descending, cur marks the starts of runs
+// of at least n + s ones when cur & (p_s >> n) is not empty.
+__device__ __forceinline__ int longest_ones(uint32_t x) {
+  if (x == 0xFFFFFFFFu) return 32;
+  const uint32_t p1 = x, p2 = p1 & (p1 >> 1), p4 = p2 & (p2 >> 2), p8 = p4 & (p4 >> 4), p16 = p8 & (p8 >> 8);
+  const uint32_t p[5] = {p16, p8, p4, p2, p1};
+  uint32_t cur = 0xFFFFFFFFu;
+  int n = 0;
+#pragma unroll
+  for (int i = 0; i < 5; ++i) {
+    const uint32_t c = cur & (p[i] >> n);
+    if (c) {
+      cur = c;
+      n += 16 >> i;
+    }
+  }
+  return n;
+}
+
 // longest run of empty cells in a plate row (numba_utils.py:160-188)
 __device__ int max_zero_run(const uint32_t* row, int W, int NW) {
   int run = 0, best = 0;
@@ -316,15 +336,7 @@ __device__ int max_zero_run(const uint32_t* row, int W, int NW) {
     run += tz;
     best = max(best, run);
     const int hb = 31 - __clz(v);
-    if (hb > tz + 1) {
-      uint32_t zi = ~v & ((1u << hb) - 1u) & ~((2u << tz) - 1u);
-      int n = 0;
-      while (zi) {
-        zi &= zi >> 1;
-        ++n;
-      }
-      best = max(best, n);
-    }
+    if (hb > tz + 1) best = max(best, longest_ones(~v & ((1u << hb) - 1u) & ~((2u << tz) - 1u)));
     run = __clz(v);
   }
   return max(best, run);
@@ -461,14 +473,16 @@ struct SearchShared {
   unsigned long long best;
   int chunk, total, nr;
   int rlist[4];
+  int rh[4];  // heights of the rotations in rlist
   unsigned char surv[kMaxItemWarps][32];  // per warp: lanes whose candidate passed the vacancy filter
 };
 
 // Best placement key of part type t (absolute) on one plate (kKeyNone if it
-// does not fit): the four warps pull (rotation, 32 candidate top rows) chunks
-// from a shared counter (rotations interleaved, bottom rows first), skip
-// chunks that cannot beat the best key found so far, and merge with
-// atomicMin.  Called by all threads of the CTA; contains __syncthreads.
+// does not fit): the CTA's warps pull (rotation, 32 candidate top rows)
+// chunks from a shared counter (rotations interleaved, bottom rows first),
+// skip chunks that cannot beat the best key found so far, stop once no
+// rotation can at the current level, and merge with atomicMin.  Called by
+// all threads of the CTA; contains __syncthreads.
 __device__ __forceinline__ unsigned long long search_plate(const Tables& tb, const MachDev& md,
                                                            const uint32_t* grid, const uint16_t* vac, int enc,
                                                            int t, int task_max, SearchShared& sh,
@@ -482,6 +496,7 @@ __device__ __forceinline__ unsigned long long search_plate(const Tables& tb, con
     for (int r = 0; r < nrot; ++r) {
       const RotDev rd = tb.rot[t * 4 + r];
       if (rd.h <= md.L && rd.w <= md.W) {  // numba_utils.py:82-84
+        sh.rh[nr] = rd.h;
         sh.rlist[nr++] = r;
         hmin = min(hmin, rd.h);
         c_bytes += 4ull * ((unsigned long long)md.L * md.NW + (unsigned long long)rd.h * rd.mw);
@@ -508,7 +523,18 @@ __device__ __forceinline__ unsigned long long search_plate(const Tables& tb, con
     unsigned long long cur = 0;
     if (lane == 0) cur = *(volatile unsigned long long*)&sh.best;
     cur = __shfl_sync(kFull, cur, 0);
-    if (key_of(max(enc, md.L - ty_hi), ty_hi + rd.h - 1, 0, r) >= cur) continue;
+    if (key_of(max(enc, md.L - ty_hi), ty_hi + rd.h - 1, 0, r) >= cur) {
+      // The best key a chunk can give only grows with its level, and the best
+      // found only shrinks: when no rotation can beat it at this level, no
+      // later chunk (same level or higher) can, and the warp is done.
+      bool beat = false;
+      for (int j = 0; j < nr; ++j) {
+        const int tyj = md.L - sh.rh[j] - 32 * level;
+        beat |= tyj >= 0 && key_of(max(enc, md.L - tyj), tyj + sh.rh[j] - 1, 0, sh.rlist[j]) < cur;
+      }
+      if (!beat) break;
+      continue;
+    }
     const int ty = ty_hi - lane;
     if (lane == 0) ++c_chunks;
     // Vacancy filter one candidate per lane.  Then, when there are few enough
