@@ -27,7 +27,8 @@
 //      memory, further ones in a global pool.  For each part: first-fit over
 //      plates (area filter, then the collision search), else a new plate with
 //      the best rotation at (0, L-1).  The collision search splits (rotation,
-//      32 candidate rows) chunks over the warps; a lane runs the vacancy
+//      32 candidate rows) chunks over the warps, skipping chunks that cannot
+//      beat the best position found so far; a lane runs the vacancy
 //      filter of one candidate top row, then the (surviving candidate,
 //      32-column word) pairs are dealt to the lanes for the exact
 //      run-dilation test, mask rows coarse to fine from the bottom; the first
@@ -223,18 +224,14 @@ __device__ __forceinline__ uint32_t blocked(const uint32_t* row, int p0, int d) 
   return res;
 }
 
-#ifndef BRKGA_TEST_ILP
-#define BRKGA_TEST_ILP 2
-#endif
-#ifndef BRKGA_VAC_ILP
-#define BRKGA_VAC_ILP 4
-#endif
+constexpr int kTestIlp = 2;  // independent run dilations per step of the exact test
+constexpr int kVacIlp = 4;   // vacancy rows compared per step of the filter
 
 // Necessary condition for the rotation to fit with its top row at ty: the
 // plate rows it covers have free runs at least as long as the mask rows'
 // longest runs (numba_utils.py:50-94).  The first kVacRows rows of the
 // collision-test order (widest row, then coarse to fine from the bottom)
-// are checked, BRKGA_VAC_ILP per step so their loads overlap: a candidate
+// are checked, kVacIlp per step so their loads overlap: a candidate
 // that fails the filter fails within them almost always, and one that slips
 // through is rejected by the exact test.
 constexpr int kVacRows = 32;
@@ -244,10 +241,10 @@ __device__ __forceinline__ bool vacancy_ok(const uint16_t* vac, int ty, const Ro
   const uint16_t* row = vac + ty;
   const int h = min(rd.h, kVacRows);
   int i = 0;
-  for (; i + BRKGA_VAC_ILP <= h; i += BRKGA_VAC_ILP) {
+  for (; i + kVacIlp <= h; i += kVacIlp) {
     bool bad = false;
 #pragma unroll
-    for (int u = 0; u < BRKGA_VAC_ILP; ++u) {
+    for (int u = 0; u < kVacIlp; ++u) {
       const uint32_t e = __ldg(v + i + u);
       bad |= row[e >> 16] < (e & 0xFFFFu);
     }
@@ -263,17 +260,17 @@ __device__ __forceinline__ bool vacancy_ok(const uint16_t* vac, int ty, const Ro
 // The bits of F (candidate columns base .. base + 31) at which the rotation
 // fits with its top row at plate row g0: every run of ones of the mask, in
 // collision-test order (widest row, then the rows coarse to fine from the
-// bottom), clears the columns it would overlap; BRKGA_TEST_ILP independent
+// bottom), clears the columns it would overlap; kTestIlp independent
 // runs per step, stop when F is empty.
 __device__ __forceinline__ uint32_t word_free(const uint32_t* g0, int RS, int base, uint32_t F, const RotDev& rd,
                                               const uint2* truns) {
   const uint2* e = truns + rd.trun;
   const int n = rd.ntrun;
   int q = 0;
-  for (; q + BRKGA_TEST_ILP <= n && F; q += BRKGA_TEST_ILP) {
+  for (; q + kTestIlp <= n && F; q += kTestIlp) {
     uint32_t bl = 0u;
 #pragma unroll
-    for (int u = 0; u < BRKGA_TEST_ILP; ++u) {
+    for (int u = 0; u < kTestIlp; ++u) {
       const uint2 r = __ldg(e + q + u);
       bl |= blocked(g0 + (int)r.y * RS, base + (int)(r.x & 0xFFFFu), (int)(r.x >> 16));
     }
