@@ -10,7 +10,9 @@ host-to-host entry point ``brkga_evaluate_host`` of the C ABI.
 ``DeviceDecoder`` decodes populations that are already on the GPU (torch
 tensors), stream-ordered and without host synchronisation, through
 ``brkga_decode`` with a preallocated workspace — the form the GA loop and the
-throughput benchmark use.
+throughput benchmark use.  ``MultiDecoder`` does the same for several
+independent instances (own parts, machines and plate sizes) in one launch of
+each kernel, through ``brkga_decode_multi(_at)``.
 """
 from __future__ import annotations
 
