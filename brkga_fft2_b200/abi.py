@@ -23,6 +23,7 @@ ERR_WORKSPACE = 4
 ERR_CAPACITY = 5
 ERR_NEW_BIN_UNFIT = 6
 ERR_NO_DEVICE = 7
+ERR_INTERNAL = 8
 
 STATUS_NAMES = {
     OK: "ok",
@@ -33,6 +34,7 @@ STATUS_NAMES = {
     ERR_CAPACITY: "bin pool exhausted",
     ERR_NEW_BIN_UNFIT: "new plate received a rotation that does not fit",
     ERR_NO_DEVICE: "no CUDA device",
+    ERR_INTERNAL: "device consistency check failed",
 }
 
 

@@ -31,9 +31,11 @@
 //      beat the best position found so far; a lane runs the vacancy
 //      filter of one candidate top row, then the (surviving candidate,
 //      32-column word) pairs are dealt to the lanes for the exact
-//      run-dilation test, mask rows coarse to fine from the bottom; the first
-//      pair with a free column gives the bottom-most candidate and its
-//      leftmost x.  Results are merged with a 64-bit lexicographic key
+//      run-dilation test, mask rows coarse to fine from the bottom: each lane
+//      walks the first runs of its pair alone, the pairs still open are
+//      finished in order by the whole warp (a lane per run, results ANDed);
+//      the first pair with a free column gives the bottom-most candidate and
+//      its leftmost x.  Results are merged with a 64-bit lexicographic key
 //      (newLen, -y, x, rotation) by atomicMin in shared memory, which is the
 //      reference's rotation rule (binClassNew.py:101-117) — see key_of().
 //   3. reduce_kernel       max over machines, 1e16 for infeasible chromosomes.
@@ -226,6 +228,10 @@ __device__ __forceinline__ uint32_t blocked(const uint32_t* row, int p0, int d) 
 
 constexpr int kTestIlp = 2;  // independent run dilations per step of the exact test
 constexpr int kVacIlp = 4;   // vacancy rows compared per step of the filter
+// Runs a lane walks alone before the pairs still open share the warp: a
+// sixth of the rotation's runs, between 8 and 20 (measured best on the
+// 50- to 400-part workloads).
+__device__ __forceinline__ int solo_runs(int n_runs) { return min(n_runs, min(20, max(8, n_runs / 6))); }
 
 // Necessary condition for the rotation to fit with its top row at ty: the
 // plate rows it covers have free runs at least as long as the mask rows'
@@ -341,6 +347,21 @@ __device__ int max_zero_run(const uint32_t* row, int W, int NW) {
 
 __device__ __forceinline__ void raise_status(int32_t* status, int code) {
   atomicCAS(status, 0, code);
+}
+
+// blocked() with the plate row and the words it reads checked first: a run
+// whose access would leave the plate raises BRKGA_ERR_INTERNAL and blocks
+// every column instead of being read.  The checks never fire on consistent
+// tables; they keep the exact test's cooperative phase in bounds whatever
+// the values its lanes exchange.
+__device__ __forceinline__ uint32_t blocked_checked(const uint32_t* grid, int row, int L, int RS, int p0, int d,
+                                                    int32_t* status) {
+  const int whi = ((d <= 32 ? p0 + 32 : p0 + d) >> 5) + 1;
+  if (row < 0 || row >= L || p0 < 0 || d < 1 || whi >= RS) {
+    raise_status(status, BRKGA_ERR_INTERNAL);
+    return kFull;
+  }
+  return blocked(grid + (size_t)row * RS, p0, d);
 }
 
 
@@ -482,7 +503,7 @@ struct SearchShared {
 // all threads of the CTA; contains __syncthreads.
 __device__ __forceinline__ unsigned long long search_plate(const Tables& tb, const MachDev& md,
                                                            const uint32_t* grid, const uint16_t* vac, int enc,
-                                                           int t, int task_max, SearchShared& sh,
+                                                           int t, int task_max, int32_t* status, SearchShared& sh,
                                                            unsigned long long& c_tests,
                                                            unsigned long long& c_chunks,
                                                            unsigned long long& c_bytes) {
@@ -535,10 +556,12 @@ __device__ __forceinline__ unsigned long long search_plate(const Tables& tb, con
     const int ty = ty_hi - lane;
     if (lane == 0) ++c_chunks;
     // Vacancy filter one candidate per lane.  Then, when there are few enough
-    // (survivor, output word) pairs, they are dealt to the lanes, bottom-most
-    // survivor and leftmost word first, so lanes whose candidate failed the
-    // filter take part in the exact test of the others, and the first pair
-    // with a free column is the bottom-most candidate's leftmost x.
+    // (survivor, output word) pairs, they are dealt to the lanes in rounds of
+    // 32, bottom-most survivor and leftmost word first, so lanes whose
+    // candidate failed the filter take part in the exact test of the others;
+    // in a round each lane first walks a few runs of its pair alone, then the
+    // pairs still open are finished by the whole warp in order, and the first
+    // pair with a free column is the bottom-most candidate's leftmost x.
     // Otherwise each lane tests its own candidate's words left to right.
     const bool pass = ty >= 0 && vacancy_ok(vac, ty, rd, tb.vtest);
     const unsigned S = __ballot_sync(kFull, pass);
@@ -550,26 +573,69 @@ __device__ __forceinline__ unsigned long long search_plate(const Tables& tb, con
       if (pass) surv[__popc(S & ((1u << lane) - 1u))] = (unsigned char)lane;
       __syncwarp();
       const uint32_t Flast = (nx & 31) ? ((1u << (nx & 31)) - 1u) : kFull;
+      const uint2* runs = tb.truns + rd.trun;
+      const int n_runs = rd.ntrun, qsolo = solo_runs(n_runs);
       for (int t0 = 0; t0 < ntask; t0 += 32) {
+        // Solo phase: each lane walks the first runs of its own pair, two per
+        // step; most blocked words close within them.
         const int t = t0 + lane;
         uint32_t F = 0u;
-        int k = 0, sl = 0;
+        int k = 0, sl = 0, q = 0;
         if (t < ntask) {
           const int si = t / nwo;
           k = t - si * nwo;
           sl = surv[si];
-          F = word_free(grid + (size_t)(ty_hi - sl) * md.RS, md.RS, k << 5, k == nwo - 1 ? Flast : kFull, rd,
-                        tb.truns);
+          F = k == nwo - 1 ? Flast : kFull;
+          const int row0 = ty_hi - sl, base = k << 5;
+          for (; q < qsolo && F; q += 2) {
+            const uint2 e0 = __ldg(runs + q);
+            uint32_t bl = blocked_checked(grid, row0 + (int)e0.y, md.L, md.RS, base + (int)(e0.x & 0xFFFFu),
+                                          (int)(e0.x >> 16), status);
+            if (q + 1 < qsolo) {
+              const uint2 e1 = __ldg(runs + q + 1);
+              bl |= blocked_checked(grid, row0 + (int)e1.y, md.L, md.RS, base + (int)(e1.x & 0xFFFFu),
+                                    (int)(e1.x >> 16), status);
+            }
+            F &= ~bl;
+          }
+          q = min(q, qsolo);
         }
-        const unsigned fm = __ballot_sync(kFull, F != 0u);
-        if (fm) {
-          const int l = __ffs(fm) - 1;
-          const uint32_t Fb = __shfl_sync(kFull, F, l);
-          const int kb = __shfl_sync(kFull, k, l);
-          const int slb = __shfl_sync(kFull, sl, l);
+        // Shared phase: a pair with runs left and columns open is walked by the
+        // whole warp, in task order, up to the first pair already proven free
+        // (pairs after it cannot win): every lane takes every 32nd remaining
+        // run on its own, then the lanes AND their open columns.  The first
+        // pair that stays free is the bottom-most candidate's leftmost x.
+        const unsigned open = __ballot_sync(kFull, F != 0u && q < n_runs);
+        const unsigned done_free = __ballot_sync(kFull, F != 0u && q >= n_runs);
+        unsigned rem = open & (done_free ? ((done_free & (0u - done_free)) - 1u) : kFull);
+        int win = done_free ? __ffs(done_free) - 1 : -1;
+        uint32_t Fw = __shfl_sync(kFull, F, win < 0 ? 0 : win);
+        while (rem) {
+          const int l = __ffs(rem) - 1;
+          rem &= rem - 1u;
+          uint32_t Fp = __shfl_sync(kFull, F, l);
+          const int ql = __shfl_sync(kFull, q, l);
+          const int kl = __shfl_sync(kFull, k, l);
+          const int sll = __shfl_sync(kFull, sl, l);
+          const int row0 = ty_hi - sll, base = kl << 5;
+          for (int qq = ql + lane; qq < n_runs && Fp; qq += 32) {
+            const uint2 e = __ldg(runs + qq);
+            Fp &= ~blocked_checked(grid, row0 + (int)e.y, md.L, md.RS, base + (int)(e.x & 0xFFFFu), (int)(e.x >> 16),
+                                   status);
+          }
+          for (int o = 1; o < 32; o <<= 1) Fp &= __shfl_xor_sync(kFull, Fp, o);
+          if (Fp) {
+            win = l;
+            Fw = Fp;
+            break;
+          }
+        }
+        if (win >= 0) {
+          const int kb = __shfl_sync(kFull, k, win);
+          const int slb = __shfl_sync(kFull, sl, win);
           if (lane == 0) {
             const int tyb = ty_hi - slb;
-            atomicMin(&sh.best, key_of(max(enc, md.L - tyb), tyb + rd.h - 1, (kb << 5) + __ffs(Fb) - 1, r));
+            atomicMin(&sh.best, key_of(max(enc, md.L - tyb), tyb + rd.h - 1, (kb << 5) + __ffs(Fw) - 1, r));
           }
           break;
         }
@@ -740,7 +806,8 @@ __global__ void __launch_bounds__(kThreads, kResidentWarps * 32 / kThreads)
         const uint32_t* grid = b < run.S ? smem + (size_t)b * run.slot_words
                                          : run.pool + (size_t)bs[b].pool * run.slot_words;
         const uint16_t* vac = reinterpret_cast<const uint16_t*>(grid + run.slot_vac_off);
-        key = search_plate(tb, md, grid, vac, bs[b].enc, t, run.task_max, sh, c_tests, c_chunks, c_bytes);
+        key = search_plate(tb, md, grid, vac, bs[b].enc, t, run.task_max, run.status, sh, c_tests, c_chunks,
+                           c_bytes);
         if (key != kKeyNone) {
           pb = b;
           break;
@@ -888,7 +955,7 @@ __global__ void __launch_bounds__(kGreedyThreads) greedy_kernel(const __grid_con
         const uint32_t* grid = g.pool + (size_t)bs[b].pool * g.slot_words;
         const unsigned long long key =
             search_plate(tb, md, grid, reinterpret_cast<const uint16_t*>(grid + g.slot_vac_off), bs[b].enc, t,
-                         kDefaultTaskMax, sh, c_tests, c_chunks, c_bytes);
+                         kDefaultTaskMax, g.status, sh, c_tests, c_chunks, c_bytes);
         if (key == kKeyNone) continue;
         const double bpth = bs[b].pth;
         const double cand2 = bpth < pthm ? ((mm - bpth) + pthm) + ptm : mm + ptm;  // :486-489
@@ -1489,6 +1556,7 @@ const char* brkga_status_string(int status) {
     case BRKGA_ERR_CAPACITY: return "bin pool exhausted";
     case BRKGA_ERR_NEW_BIN_UNFIT: return "new plate received a rotation that does not fit";
     case BRKGA_ERR_NO_DEVICE: return "no CUDA device";
+    case BRKGA_ERR_INTERNAL: return "device consistency check failed";
     default: return "unknown status";
   }
 }

@@ -46,7 +46,10 @@ typedef enum BrkgaStatus {
   BRKGA_ERR_CAPACITY = 5,         /* device bin pool exhausted (retry with more)      */
   BRKGA_ERR_NEW_BIN_UNFIT = 6,    /* a new plate got a best_rotation that does not fit;
                                      the reference raises in numpy slicing here      */
-  BRKGA_ERR_NO_DEVICE = 7
+  BRKGA_ERR_NO_DEVICE = 7,
+  BRKGA_ERR_INTERNAL = 8          /* a device-side consistency check failed: an access
+                                     would have left a plate; the access was skipped
+                                     and the makespans of the launch are not valid */
 } BrkgaStatus;
 
 /* Host description of one instance.  All arrays are read during
