@@ -5,8 +5,8 @@ item (1, 2 or 4) trade the latency of one (chromosome, machine) item against
 throughput: 4 finish an item sooner, 2 waste fewer lanes on speculative row
 chunks, so 2 win once the items fill several waves of resident CTAs, and 1
 (no CTA barrier at all) wins by a few per cent only when they fill some 20
-waves (measured: 64 uneven instances x 256 chromosomes, 52,000 items, 43.8
-against 46.5 ms).  More
+waves (measured: 64 uneven instances x 256 chromosomes, 52,000 items, 33.0
+against 35.4 ms); the automatic choice follows these tiers.  More
 resident CTAs per SM hide more latency, more plates per item in shared
 memory keep more collision searches off the global pool, and both draw on
 the same 228 KB of shared memory per SM, whose share per plate grows with

@@ -1061,8 +1061,7 @@ struct BrkgaProblem {
   int req_warps = 0, req_ctas = 0, req_plates = -1;  // requested launch shape (0 / 0 / -1 = automatic)
   int task_max = kDefaultTaskMax;
   Shape shape[3];      // 4, 2 and 1 warps per item
-  int max_slots = 0;   // resident CTAs of the largest usable shape (per-CTA plate scalars in the workspace)
-  int min_S = 0;       // fewest plates in shared memory of the usable shapes (pool sizing)
+  int min_S = 0;       // fewest plates in shared memory of the three shapes (pool sizing)
   int slot_words = 0, slot_vac_off = 0;
   std::vector<MachDev> mach;
   std::vector<void*> allocations;
@@ -1113,6 +1112,31 @@ int counts_of(const BrkgaProblem* pb, const int32_t* pops, LaunchCounts* lc) {
   return BRKGA_OK;
 }
 
+// The shape a launch of `items` items uses: the requested CTA size, else
+// 4 warps per item while the items fill at most three waves of resident
+// 4-warp CTAs (per-item latency dominates), 2 warps up to sixteen waves of
+// 2-warp CTAs, 1 warp beyond (throughput dominates; no CTA barriers).
+const Shape& pick_shape(const BrkgaProblem* pb, int64_t items) {
+  if (pb->req_warps == 4) return pb->shape[0];
+  if (pb->req_warps == 2) return pb->shape[1];
+  if (pb->req_warps == 1) return pb->shape[2];
+  if (items <= 3 * (int64_t)pb->shape[0].n_slots) return pb->shape[0];
+  if (items <= 16 * (int64_t)pb->shape[1].n_slots) return pb->shape[1];
+  return pb->shape[2];
+}
+
+// CTAs whose plate scalars the workspace of a launch of `items` items holds:
+// the most resident CTAs of any shape a launch of at most `items` items can
+// use, so that a workspace sized for the largest population serves every
+// smaller launch too.
+int scratch_slots(const BrkgaProblem* pb, int64_t items) {
+  if (pb->req_warps) return pick_shape(pb, items).n_slots;
+  int n = pb->shape[0].n_slots;
+  if (items > 3 * (int64_t)pb->shape[0].n_slots) n = std::max(n, pb->shape[1].n_slots);
+  if (items > 16 * (int64_t)pb->shape[1].n_slots) n = std::max(n, pb->shape[2].n_slots);
+  return n;
+}
+
 Layout layout_of(const BrkgaProblem* pb, const LaunchCounts& lc, int64_t pool_bins) {
   Layout l;
   size_t o = 0;
@@ -1129,7 +1153,7 @@ Layout layout_of(const BrkgaProblem* pb, const LaunchCounts& lc, int64_t pool_bi
   l.off_mk = o = align_up(o, 256);
   o += (size_t)lc.items * sizeof(double);
   l.off_bins = o = align_up(o, 256);
-  o += (size_t)pb->max_slots * std::max(pb->Nmax, 1) * sizeof(BinScal);
+  o += (size_t)scratch_slots(pb, lc.items) * std::max(pb->Nmax, 1) * sizeof(BinScal);
   l.off_pool = o = align_up(o, 256);
   o += (size_t)pool_bins * pb->slot_words * sizeof(uint32_t);
   l.total = align_up(o, 256);
@@ -1263,30 +1287,15 @@ int configure(BrkgaProblem* pb, int warps_req, int ctas_req, int plates_req) {
   }
   pb->slot_vac_off = slot_vac_off;
   pb->slot_words = slot_words;
-  for (int v = 0; v < 3; ++v) pb->shape[v] = shapes[v];
-  // The automatic choice uses the 4- and 2-warp shapes; the 1-warp shape only
-  // when requested, so its 32 CTAs per SM size the per-CTA scratch only then.
-  const int usable = warps_req == 1 ? 3 : 2;
-  pb->max_slots = 0;
   pb->min_S = shapes[0].S;
-  for (int v = 0; v < usable; ++v) {
-    pb->max_slots = std::max(pb->max_slots, shapes[v].n_slots);
+  for (int v = 0; v < 3; ++v) {
+    pb->shape[v] = shapes[v];
     pb->min_S = std::min(pb->min_S, shapes[v].S);
   }
   pb->req_warps = warps_req;
   pb->req_ctas = ctas_req;
   pb->req_plates = plates_req;
   return BRKGA_OK;
-}
-
-// The shape a launch of `items` items uses: the requested CTA size, else
-// 4 warps per item while the items fill at most three waves of resident
-// CTAs (per-item latency dominates), 2 warps beyond (throughput dominates).
-const Shape& pick_shape(const BrkgaProblem* pb, int64_t items) {
-  if (pb->req_warps == 4) return pb->shape[0];
-  if (pb->req_warps == 2) return pb->shape[1];
-  if (pb->req_warps == 1) return pb->shape[2];
-  return items > 3 * (int64_t)pb->shape[0].n_slots ? pb->shape[1] : pb->shape[0];
 }
 
 int validate(const BrkgaProblemDesc* d) {

@@ -211,9 +211,9 @@ int brkga_decode_multi_at(int32_t stage, const BrkgaProblem* problem, const floa
  * reference counterpart).  Results never depend on it.
  *   warps_per_item  1, 2 or 4 warps per CTA, one (chromosome, machine) item
  *                   per CTA; 0 = automatic per launch (4 while the items fill
- *                   at most three waves of resident CTAs, where the latency
- *                   of one item dominates; 2 beyond, where throughput does;
- *                   1 only when requested)
+ *                   at most three waves of resident 4-warp CTAs, where the
+ *                   latency of one item dominates; 2 up to sixteen waves of
+ *                   2-warp CTAs; 1 beyond, where throughput does)
  *   ctas_per_sm     resident CTAs per SM for that size (1..32; 0 = 32
  *                   resident warps per SM, the register limit)
  *   smem_plates     plates of each item kept in shared memory (0..8, the

@@ -91,7 +91,10 @@ def test_automatic_warps_follow_item_count(multi):
     w_small, _, _, slots4, _ = md.launch_config(items=1)
     assert w_small == 4
     assert md.launch_config(items=3 * slots4)[0] == 4
-    assert md.launch_config(items=3 * slots4 + 1)[0] == 2
+    w2, _, _, slots2, _ = md.launch_config(items=3 * slots4 + 1)
+    assert w2 == 2
+    assert md.launch_config(items=16 * slots2)[0] == 2
+    assert md.launch_config(items=16 * slots2 + 1)[0] == 1
 
 
 def test_unresident_shape_is_refused(multi):
