@@ -520,6 +520,20 @@ __device__ __forceinline__ unsigned long long search_plate(const Tables& tb, con
         c_bytes += 4ull * ((unsigned long long)md.L * md.NW + (unsigned long long)rd.h * rd.mw);
       }
     }
+    // With fewer than four warps a level's chunks are taken one after another:
+    // the shortest rotation first has the smallest best-case key and prunes
+    // the others sooner (measured 4.5 % off the 2-warp P200M6 launch; with
+    // four warps every rotation of a level starts at once and the order only
+    // cost time).
+    if (blockDim.x < 128)
+      for (int i = 1; i < nr; ++i)
+        for (int j = i; j > 0 && sh.rh[j] < sh.rh[j - 1]; --j) {
+          const int th = sh.rh[j], tr = sh.rlist[j];
+          sh.rh[j] = sh.rh[j - 1];
+          sh.rlist[j] = sh.rlist[j - 1];
+          sh.rh[j - 1] = th;
+          sh.rlist[j - 1] = tr;
+        }
     sh.nr = nr;
     sh.total = nr ? nr * ((md.L - hmin + 1 + 31) >> 5) : 0;
     sh.best = kKeyNone;
