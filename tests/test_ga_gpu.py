@@ -2,6 +2,7 @@
 populations, fitness, history and best solution; CUDA-graph replay equals
 eager execution."""
 import ctypes
+import os
 
 import numpy as np
 import pytest
@@ -126,10 +127,12 @@ def test_screened_ga_reports_exact_makespans(torch, explore):
     assert (np.diff(ga.history["min"]) <= 0).all()
 
 
-@pytest.mark.parametrize("maker,P,G,frac", [(instances.p50m2, 200, 12, 0.02), (instances.p400m8, 48, 2, 0.01)])
+@pytest.mark.parametrize("maker,P,G,frac", [(instances.p50m2, 200, 12, 0.02), (instances.p400m8, 48, 2, 0.01),
+                                             (instances.p400m8, 4096, 3, 0.01)])
 def test_audit_sample_of_every_generation_is_exact(torch, maker, P, G, frac):
     """The audit sample (1-2 % of the rows decoded in every generation, screening on)
-    matches the oracle bit for bit, generation by generation."""
+    matches the oracle bit for bit, generation by generation — at the
+    large-stress size too (P400M8, population 4096: 37 rows a generation)."""
     from brkga_fft2_b200.ga import DeviceBRKGA
     from oracle import oracle_decode
     inst = maker(0)
@@ -142,6 +145,7 @@ def test_audit_sample_of_every_generation_is_exact(torch, maker, P, G, frac):
     ga.fit()
     chrom, fit = ga.audit
     assert chrom.shape[:2] == (G + 1, ga.n_audit) and ga.n_audit >= 1
-    ref = oracle_decode(pk, chrom.reshape(-1, chrom.shape[-1]), n_threads=8).reshape(fit.shape)
+    ref = oracle_decode(pk, chrom.reshape(-1, chrom.shape[-1]), n_threads=min(16, os.cpu_count() or 1)
+                        ).reshape(fit.shape)
     np.testing.assert_array_equal(fit, ref)
     assert "screen" in ga.history["mode"]
