@@ -162,3 +162,18 @@ def test_single_machine_and_nan_keys(torch_cuda):
     ch2[::3, 12 + 2] = np.nan
     ch2[1::4, 5] = np.nan
     np.testing.assert_array_equal(np.asarray(ev2.evaluate_batch(ch2)), oracle_decode(ev2.packed, ch2))
+
+
+def test_audit_output_from_the_device_log(torch_cuda):
+    """Plates rebuilt from the CUDA decoder's log equal the reference's own plate
+    dumps (P50M2-0 chromosome 462), and the solution record's machines rebuild
+    the makespan."""
+    from brkga_fft2_b200 import audit
+    from tests.test_audit_cpu import reference_plates
+    ev, z = evaluator_for("real_P50M2-0", torch_cuda)
+    ms, log = ev.evaluate_batch(z["chromosomes"], return_log=True)
+    plates = audit.plates_from_log(ev.packed, log[0])
+    for k, grid in reference_plates(z).items():
+        assert (plates[k] == grid).all(), k
+    rec = audit.solution_record(ev.packed, z["chromosomes"][0], ms[0], log[0], instance="P50M2-0")
+    assert max(m["makespan"] for m in rec["machines"].values()) == rec["makespan"] == round(ms[0], 6)
