@@ -267,6 +267,7 @@ def run_ours(args):
                          "frac": achieved / hbm_peak, "traffic": profile_traffic(),
                          "kernel": "decode_kernel", "kernel_ms": statistics.mean(kern_ms),
                          "algorithmic_bytes_per_launch": scan, "tests_per_launch": tests,
+                         "placement_tests_per_s": tests / kern_avg_s,
                          "peak_source": peak_kind,
                          "note": "algorithmic bytes = per placement test one read of the bit-packed plate "
                                  "and rotated mask, 4*(L*ceil(W/32)+h*ceil(w/32))"},
