@@ -18,6 +18,7 @@ host cores instead (the reference itself is Python and cannot be shipped).
 from __future__ import annotations
 
 import argparse
+import datetime
 import json
 import os
 import statistics
@@ -87,7 +88,9 @@ def cpu_rate(packed, n_parts, seconds, threads, seed=12345):
 
 
 class ClockSampler:
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    """nvidia-smi clock and throttle-reason samples (every 20 ms, timestamped)
+    around the timed region; only the samples taken inside it are reported."""
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -95,16 +98,28 @@ class ClockSampler:
         self.gpu = gpu_index
         self.path = tempfile.mktemp(suffix=".csv")
         self.proc = None
+        self.t0 = self.t1 = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                                          "-lms", "200", "-i", str(gpu_index)],
+                                          "-lms", "20", "-i", str(gpu_index)],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return
+        deadline = time.time() + 5.0  # the first sample shows the sampler is running before the timing starts
+        while time.time() < deadline and os.path.getsize(self.path) == 0 and self.proc.poll() is None:
+            time.sleep(0.01)
+
+    def mark_start(self):
+        self.t0 = datetime.datetime.now()
+
+    def mark_end(self):
+        self.t1 = datetime.datetime.now()
 
     def stop(self):
         if self.proc is None:
             return None
+        time.sleep(0.05)  # one more sample after the region
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -113,19 +128,23 @@ class ClockSampler:
         rows = []
         for line in open(self.path):
             parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 9:
+            if len(parts) < 10:
                 continue
             try:
-                rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+                ts = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f")
+                rows.append((ts, float(parts[2]), float(parts[3]), parts[6:10]))
             except ValueError:
                 continue
         os.unlink(self.path)
         if not rows:
             return None
+        inside = [r for r in rows if self.t0 is not None and self.t1 is not None and self.t0 <= r[0] <= self.t1]
+        use = inside or rows
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v.lower() == "active"})
-        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
-                "reasons": reasons, "samples": len(rows)}
+        reasons = sorted({names[i] for _, _, _, r in use for i, v in enumerate(r) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[1] for r in use), "sm_max_mhz": max(r[2] for r in use),
+                "reasons": reasons, "samples": len(use), "in_timed_region": bool(inside),
+                "interval_ms": 20}
 
 
 def profile_traffic():
@@ -211,6 +230,7 @@ def run_ours(args):
 
     sampler = ClockSampler(local)
     barrier()
+    sampler.mark_start()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
            torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     tests = chunks = scan = 0
@@ -221,6 +241,7 @@ def run_ours(args):
         dd.decode(dev[args.warmup + s], out, kernel_events=(k0, k1))
         e1.record(stream)
     torch.cuda.synchronize()
+    sampler.mark_end()
     step_ms = [e0.elapsed_time(e1) for e0, _, _, e1 in ev]
     kern_ms = [k0.elapsed_time(k1) for _, k0, k1, _ in ev]
     barrier()
