@@ -185,3 +185,25 @@ def test_pool_exhaustion_is_reported(multi):
     torch.cuda.synchronize()
     assert int(small.status.item()) == abi.ERR_CAPACITY
     assert np.isnan(out.cpu().numpy()).any()
+
+
+def test_large_batch_takes_the_one_warp_tier():
+    """64 uneven instances x 256 chromosomes (some 50,000 items, past sixteen
+    waves of 2-warp CTAs) decode with the automatic shape — 1 warp per item —
+    and two rows of every instance equal the oracle's decode."""
+    import torch
+    from brkga_fft2_b200.evaluator import MultiDecoder
+    insts = [instances.uneven(s) for s in range(64)]
+    packs = [pack_problem(i.problem_data, i.nb_parts, i.nb_machines, i.thresholds, i.instance_parts) for i in insts]
+    pops = [256] * 64
+    md = MultiDecoder(packs, max_pops=pops)
+    items = sum(p * pk.n_machines for p, pk in zip(pops, packs))
+    assert md.launch_config(items=items)[0] == 1
+    chroms = [instances.chromosomes(p, i.nb_parts, 500 + k) for k, (p, i) in enumerate(zip(pops, insts))]
+    out = md.decode_concat(torch.from_numpy(np.concatenate([c.reshape(-1) for c in chroms])).cuda(), pops)
+    torch.cuda.synchronize()
+    assert int(md.status.item()) == 0
+    got = out.cpu().numpy().reshape(64, 256)
+    for k, (pk, ch) in enumerate(zip(packs, chroms)):
+        rows = [0, 255 - k]
+        np.testing.assert_array_equal(got[k, rows], oracle_decode(pk, ch[rows], n_threads=2), err_msg=f"instance {k}")
