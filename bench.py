@@ -62,6 +62,13 @@ def load_workload():
     return inst, packed
 
 
+def workload_config(pop: int, world: int) -> dict:
+    """The `config` record both arms print: the same workload, whichever arm runs it."""
+    return {"workload": f"{WORKLOAD} pop {pop}", "parts": 100, "machines": 4, "plates": "2x300x300 + 2x250x250",
+            "mask_bbox_max": 120, "l2": "flushed (256 MiB write) between timed steps",
+            "parallelism": f"dp{world} (shards)"}
+
+
 def measured_peaks():
     path = os.path.join(HERE, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -185,7 +192,8 @@ def run_reference(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
         "data": "synthetic (seeded generator, P100M4 shapes)",
-        "config": {"workload": f"{WORKLOAD} pop {args.pop}", "sample_per_step": n, "l2": "n/a (CPU)"},
+        "config": workload_config(args.pop, args.gpus),
+        "sample_per_step": n,
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
@@ -281,9 +289,7 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int32",
             "data": "synthetic (seeded generator, P100M4 shapes)",
-            "config": {"workload": f"{WORKLOAD} pop {P}", "parts": N, "machines": inst.nb_machines,
-                       "plates": "2x300x300 + 2x250x250", "mask_bbox_max": 120,
-                       "l2": "flushed (256 MiB write) between timed steps", "parallelism": f"dp{world} (shards)"},
+            "config": workload_config(P, world),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                          "frac": achieved / hbm_peak, "traffic": profile_traffic(),
                          "kernel": "decode_kernel", "kernel_ms": statistics.mean(kern_ms),
