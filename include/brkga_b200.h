@@ -104,7 +104,9 @@ int brkga_problem_create(const BrkgaProblemDesc* desc, BrkgaProblem** out);
 void brkga_problem_destroy(BrkgaProblem* problem);
 
 /* Device bytes a caller must provide to brkga_decode for P chromosomes with
- * a bin pool of `pool_bins` plates (0 = the library's default for P). */
+ * a bin pool of `pool_bins` plates (0 = the library's default for P).  A
+ * workspace of that size serves every population of at most P chromosomes
+ * under the same launch configuration. */
 int brkga_workspace_bytes(const BrkgaProblem* problem, int32_t P, int64_t pool_bins,
                           size_t* bytes);
 
