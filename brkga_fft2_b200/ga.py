@@ -72,6 +72,16 @@ class DeviceBRKGA:
             raise ValueError("need 1 <= num_elites and num_elites + num_mutants <= num_individuals")
         if self.num_individuals > MAX_RANK:
             raise ValueError(f"num_individuals must be <= {MAX_RANK} (device rank)")
+        if self.num_generations < 0:
+            raise ValueError("num_generations must be >= 0")
+        if not 0.0 <= self.eliteCProb <= 1.0:
+            raise ValueError("eliteCProb must be in [0, 1]")
+        if not 0.0 <= float(audit_fraction) <= 1.0:
+            raise ValueError("audit_fraction must be in [0, 1]")
+        if screening and (int(oversample) < 1 or not 0.0 <= float(explore) <= 1.0 or int(train_steps) < 0
+                          or int(train_batch) < 1):
+            raise ValueError("screening needs oversample >= 1, 0 <= explore <= 1, train_steps >= 0 and "
+                             "train_batch >= 1")
         self.packed = packed if packed is not None else pack_problem(
             problem_data, nbParts, nbMachines, thresholds, instanceParts, threshold_mode)
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())

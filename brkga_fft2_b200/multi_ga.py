@@ -56,6 +56,8 @@ class MultiBRKGA:
             if not (1 <= e and e + m <= P <= MAX_RANK):
                 raise ValueError(f"need 1 <= num_elites, num_elites + num_mutants <= num_individuals <= {MAX_RANK}")
         self.rho = float(eliteCProb)
+        if not 0.0 <= self.rho <= 1.0 or self.num_generations < 0:
+            raise ValueError("need 0 <= eliteCProb <= 1 and num_generations >= 0")
         self.seed = int(seed)
         self.use_graph = bool(use_graph)
         self.nkeys = [2 * p.n_genes for p in self.packs]

@@ -1,6 +1,7 @@
 """GA oracle checks on the CPU: Philox4x32-10 known answers and the
 operators of BRKGA_alg3.py:178-265 as restated for the device GA."""
 import numpy as np
+import pytest
 
 from brkga_fft2_b200 import instances, pack_problem
 from oracle import ga_oracle as go
@@ -47,3 +48,28 @@ def test_small_run_history():
     assert best == hist[-1, 0] == fit.min()
     from oracle import oracle_decode
     assert oracle_decode(pk, sol[None])[0] == best
+
+
+@pytest.mark.parametrize("kwargs", [dict(num_elites=0), dict(num_elites=5, num_mutants=96), dict(num_individuals=70000),
+                                    dict(num_generations=-1), dict(eliteCProb=1.5), dict(audit_fraction=2.0),
+                                    dict(screening=True, oversample=0), dict(screening=True, explore=-0.1),
+                                    dict(screening=True, explore=1.5), dict(screening=True, train_batch=0)])
+def test_device_ga_refuses_bad_arguments_before_any_gpu_work(kwargs):
+    """Argument errors surface as ValueError on the host, before a decoder or
+    any device buffer exists (an oversample below 1 would otherwise gather
+    more rows than the pool holds)."""
+    from brkga_fft2_b200.ga import DeviceBRKGA
+    args = dict(num_generations=2, num_individuals=100, num_elites=10, num_mutants=15)
+    args.update(kwargs)
+    with pytest.raises(ValueError):
+        DeviceBRKGA(None, 10, 2, [0.5], np.arange(10), **args)
+
+
+@pytest.mark.parametrize("kwargs", [dict(eliteCProb=-0.1), dict(num_generations=-2), dict(num_elites=0),
+                                    dict(num_individuals=[10, 10]), dict(num_mutants=300)])
+def test_multi_ga_refuses_bad_arguments_before_any_gpu_work(kwargs):
+    from brkga_fft2_b200.multi_ga import MultiBRKGA
+    inst = instances.small(1)
+    pk = pack_problem(inst.problem_data, inst.nb_parts, inst.nb_machines, inst.thresholds, inst.instance_parts)
+    with pytest.raises(ValueError):
+        MultiBRKGA([pk], **dict(dict(num_generations=2, num_individuals=100), **kwargs))
