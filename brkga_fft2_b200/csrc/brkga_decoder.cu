@@ -590,6 +590,14 @@ __device__ __forceinline__ unsigned long long search_plate(const Tables& tb, con
       const uint2* runs = tb.truns + rd.trun;
       const int n_runs = rd.ntrun, qsolo = solo_runs(n_runs);
       for (int t0 = 0; t0 < ntask; t0 += 32) {
+        {  // the round's first pair has the smallest key left in the chunk: stop when it cannot win
+          unsigned long long cur = 0;
+          if (lane == 0) cur = *(volatile unsigned long long*)&sh.best;
+          cur = __shfl_sync(kFull, cur, 0);
+          const int si0 = t0 / nwo, k0 = t0 - si0 * nwo;
+          const int ty0 = ty_hi - surv[si0];
+          if (key_of(max(enc, md.L - ty0), ty0 + rd.h - 1, k0 << 5, r) >= cur) break;
+        }
         // Solo phase: each lane walks the first runs of its own pair, two per
         // step; most blocked words close within them.
         const int t = t0 + lane;
@@ -632,6 +640,15 @@ __device__ __forceinline__ unsigned long long search_plate(const Tables& tb, con
           const int kl = __shfl_sync(kFull, k, l);
           const int sll = __shfl_sync(kFull, sl, l);
           const int row0 = ty_hi - sll, base = kl << 5;
+          {  // pairs come in key order: stop when this one cannot beat the best found
+            unsigned long long cur = 0;
+            if (lane == 0) cur = *(volatile unsigned long long*)&sh.best;
+            cur = __shfl_sync(kFull, cur, 0);
+            if (key_of(max(enc, md.L - row0), row0 + rd.h - 1, base + __ffs(Fp) - 1, r) >= cur) {
+              win = -1;
+              break;
+            }
+          }
           for (int qq = ql + lane; qq < n_runs && Fp; qq += 32) {
             const uint2 e = __ldg(runs + qq);
             Fp &= ~blocked_checked(grid, row0 + (int)e.y, md.L, md.RS, base + (int)(e.x & 0xFFFFu), (int)(e.x >> 16),
