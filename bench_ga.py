@@ -47,6 +47,9 @@ def main():
     ap.add_argument("--explore", default="0",
                     help="share of the decoded rows spread over the lower-ranked pool; a comma list runs one "
                          "screened GA per value (and per training budget)")
+    ap.add_argument("--overlap", default="1",
+                    help="1: surrogate training beside the decode on a second stream, 0: after it; a comma list "
+                         "runs one screened GA per value")
     ap.add_argument("--screened-limit", type=float, default=2.0,
                     help="the screened run may use up to this many times the plain run's generations")
     args = ap.parse_args()
@@ -58,7 +61,8 @@ def main():
     pk = pack_problem(inst.problem_data, inst.nb_parts, inst.nb_machines, inst.thresholds, inst.instance_parts)
     P = args.pop
     ne, nm = math.ceil(0.1 * P), math.ceil(0.15 * P)
-    variants = [(int(t), float(x)) for t in str(args.train_steps).split(",") for x in str(args.explore).split(",")]
+    variants = [(int(t), float(x), int(o)) for t in str(args.train_steps).split(",")
+                for x in str(args.explore).split(",") for o in str(args.overlap).split(",")]
     runs = []
     for seed in range(args.seeds):
         plain = DeviceBRKGA(None, inst.nb_parts, inst.nb_machines, inst.thresholds, inst.instance_parts,
@@ -71,39 +75,43 @@ def main():
         t_plain_hit = plain.history["time"][p_hit]
         del plain
         torch.cuda.empty_cache()
-        for ts, ex in variants:
-            runs.append(screened_run(args, inst, pk, P, ne, nm, seed, ts, ex, target, t_plain, p_hit, t_plain_hit))
+        for ts, ex, ov in variants:
+            runs.append(screened_run(args, inst, pk, P, ne, nm, seed, ts, ex, ov, target, t_plain, p_hit,
+                                     t_plain_hit))
             torch.cuda.empty_cache()
     by_variant = {}
-    for ts, ex in variants:
-        rs = [r for r in runs if (r["train_steps"], r["explore"]) == (ts, ex)]
-        by_variant[f"train_steps={ts},explore={ex:g}"] = {
+    for ts, ex, ov in variants:
+        rs = [r for r in runs if (r["train_steps"], r["explore"], r["overlap"]) == (ts, ex, ov)]
+        by_variant[f"train_steps={ts},explore={ex:g},overlap={ov}"] = {
             "ratio_median": float(np.median([r["ratio"] for r in rs])),
             "ratio_vs_plain_hit_median": float(np.median([r["ratio_vs_plain_hit"] for r in rs])),
             "reached": sum(math.isfinite(r["ratio"]) for r in rs)}
-    first = by_variant[f"train_steps={variants[0][0]},explore={variants[0][1]:g}"]
+    first = by_variant["train_steps={},explore={:g},overlap={}".format(*variants[0])]
     print(json.dumps({"metric": "time to plain-GA best makespan, screened vs plain", "workload": args.workload,
                       "pop": P, "generations": args.generations, "oversample": args.oversample,
                       "screened_limit": args.screened_limit, "train_steps": variants[0][0],
-                      "explore": variants[0][1], "reached": first["reached"], "ratio_median": first["ratio_median"],
+                      "explore": variants[0][1], "overlap": variants[0][2], "reached": first["reached"],
+                      "ratio_median": first["ratio_median"],
                       "ratio_vs_plain_hit_median": first["ratio_vs_plain_hit_median"],
                       "by_variant": by_variant, "runs": runs}))
 
 
-def screened_run(args, inst, pk, P, ne, nm, seed, train_steps, explore, target, t_plain, p_hit, t_plain_hit):
+def screened_run(args, inst, pk, P, ne, nm, seed, train_steps, explore, overlap, target, t_plain, p_hit,
+                 t_plain_hit):
     """One screened GA against the plain run's target; a dict for the JSON line."""
     from brkga_fft2_b200.ga import DeviceBRKGA
     scr = DeviceBRKGA(None, inst.nb_parts, inst.nb_machines, inst.thresholds, inst.instance_parts,
                       num_generations=max(1, int(round(args.generations * args.screened_limit))),
                       num_individuals=P, num_elites=ne, num_mutants=nm,
                       eliteCProb=0.7, seed=seed, packed=pk, screening=True, oversample=args.oversample,
-                      train_steps=train_steps, explore=explore, target=target)
+                      train_steps=train_steps, explore=explore, overlap_training=bool(overlap), target=target)
     scr.fit()
     mins = np.array(scr.history["min"])
     hit = np.flatnonzero(mins <= target)
     t_scr = scr.history["time"][int(hit[0])] if hit.size else float("inf")
     sp = np.array(scr.history["spearman"][1:])
-    return {"seed": seed, "train_steps": train_steps, "explore": explore, "target": target, "plain_s": t_plain,
+    return {"seed": seed, "train_steps": train_steps, "explore": explore, "overlap": overlap, "target": target,
+            "plain_s": t_plain,
             "plain_gen_ms": 1000 * t_plain / args.generations,
             "screened_s": t_scr, "screened_generations": int(hit[0]) if hit.size else None,
             "screened_best": float(mins.min()), "ratio": t_scr / t_plain,

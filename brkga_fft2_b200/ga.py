@@ -11,7 +11,9 @@ the last ``check_every`` generations stays below ``spearman_threshold``
 (the surrogate keeps learning from plain generations meanwhile).  With
 ``explore > 0`` that share of the decoded rows is not the surrogate's top but
 spread evenly over the rest of the ranked pool, which keeps lower-ranked
-offspring in the population.
+offspring in the population.  With ``overlap_training`` (the default) the
+surrogate trains on a second stream while the decode kernel runs, on the
+rows observed up to the previous generation.
 
 With ``audit_fraction > 0`` every generation also copies an evenly spaced
 sample of the rows it decoded (that fraction of them), with their exact
@@ -53,7 +55,7 @@ class DeviceBRKGA:
                  oversample: int = 5, train_steps: int = 8, train_batch: int = 512, lr: float = 1e-3,
                  spearman_threshold: float = 0.3, check_every: int = 5, warmup_generations: int = 5,
                  buffer_capacity: int = 200_000, target: Optional[float] = None, audit_fraction: float = 0.0,
-                 explore: float = 0.0):
+                 explore: float = 0.0, overlap_training: bool = True):
         import torch
         del collision_backend, eval_mode, eval_workers, eval_chunksize
         self.torch = torch
@@ -114,6 +116,7 @@ class DeviceBRKGA:
             self.audit_pop = torch.zeros(self.num_generations + 1, self.n_audit, K, dtype=torch.float32, device=dev)
             self.audit_fit = torch.zeros(self.num_generations + 1, self.n_audit, dtype=torch.float64, device=dev)
         self.screening = bool(screening)
+        self.overlap_training = False
         if self.screening:
             from .surrogate import Surrogate
             self.oversample = int(oversample)
@@ -136,6 +139,10 @@ class DeviceBRKGA:
             self.stats_dev = torch.full((self.num_generations + 1, 2), float("nan"), dtype=torch.float64, device=dev)
             self.surrogate = Surrogate(self.decoder.native, max_batch=max(self.train_batch, 1024),
                                        buffer_capacity=buffer_capacity, seed=self.seed ^ 0x5EED)
+            # Training runs on a second stream while the decode kernel runs (on the rows
+            # observed up to the previous generation), joined before the next prediction.
+            self.overlap_training = bool(overlap_training)
+            self._train_stream = torch.cuda.Stream(dev) if self.overlap_training else None
             # exploration: that share of the decoded rows is spread evenly over the
             # pool's lower-ranked candidates instead of taken from its top
             cand = self.pool_rows - self.num_elites
@@ -184,8 +191,19 @@ class DeviceBRKGA:
     def _rank(self, values, n, order):
         abi.check(self.lib.brkga_ga_rank(self._ptr(values), n, self._ptr(order), self._stream()), "brkga_ga_rank")
 
+    def _train_fork(self):
+        """Start this generation's surrogate training beside the decode (overlap mode)."""
+        if self.overlap_training:
+            self._train_stream.wait_stream(self.torch.cuda.current_stream(self.device))
+            self.surrogate.train(self.train_steps, self.train_batch, self.lr, stream=self._train_stream)
+
+    def _train_join(self):
+        if self.overlap_training:
+            self.torch.cuda.current_stream(self.device).wait_stream(self._train_stream)
+
     def _monitor_and_learn(self, nxt):
-        """Surrogate quality on this generation's decoded rows, then learn from them."""
+        """Surrogate quality on this generation's decoded rows, then learn from them
+        (the training itself ran beside the decode in overlap mode)."""
         ne, rows = self.num_elites, self.num_individuals - self.num_elites
         if rows < 1:
             return
@@ -199,7 +217,8 @@ class DeviceBRKGA:
                                                  self._ptr(self.stat_scratch), self._stream()),
                   "brkga_ga_screen_stats")
         self.surrogate.observe(decoded, exact)
-        self.surrogate.train(self.train_steps, self.train_batch, self.lr)
+        if not self.overlap_training:
+            self.surrogate.train(self.train_steps, self.train_batch, self.lr)
 
     def _step_learn(self, cur):
         """Plain generation that also measures and trains the surrogate."""
@@ -211,8 +230,10 @@ class DeviceBRKGA:
                                           ctypes.c_uint64(self.seed), self._ptr(self.generation),
                                           self._ptr(self.pop[nxt]), self._ptr(self.fitness_buf[nxt]),
                                           self._stream()), "brkga_ga_breed")
+        self._train_fork()
         if P > ne:
             self.decoder.decode(self.pop[nxt][ne:], out=self.fitness_buf[nxt][ne:])
+        self._train_join()
         self._monitor_and_learn(nxt)
         self._track(nxt)
 
@@ -238,8 +259,10 @@ class DeviceBRKGA:
                                            self._ptr(self.pop[nxt][ne:]), self._stream()), "brkga_ga_gather")
         self.pop[nxt][:ne].copy_(self.pool[:ne])
         self.fitness_buf[nxt][:ne].copy_(self.pool_fit[:ne])
+        self._train_fork()
         if rows > 0:
             self.decoder.decode(self.pop[nxt][ne:], out=self.fitness_buf[nxt][ne:])
+        self._train_join()
         self._monitor_and_learn(nxt)
         self._track(nxt)
 
