@@ -101,3 +101,16 @@ def test_multi_instance_arguments(lib):
         abi.ERR_INVALID_ARGUMENT
     assert lib.brkga_set_launch_config(None, 4, 1, 0, -1) == abi.ERR_INVALID_ARGUMENT
     assert lib.brkga_get_launch_config(None, 0, None, None, None, None, None) == abi.ERR_INVALID_ARGUMENT
+
+
+def test_header_status_codes_match_the_python_mirror():
+    """Every BrkgaStatus value of include/brkga_b200.h has the same value in abi.py."""
+    import os
+    import re
+    hdr = open(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include",
+                            "brkga_b200.h")).read()
+    enum = hdr[hdr.index("typedef enum BrkgaStatus"):hdr.index("} BrkgaStatus;")]
+    codes = dict((name, int(v)) for name, v in re.findall(r"BRKGA_(OK|ERR_[A-Z_]+)\s*=\s*(\d+)", enum))
+    assert codes and len(codes) == len(abi.STATUS_NAMES)
+    for name, value in codes.items():
+        assert getattr(abi, name) == value, name
