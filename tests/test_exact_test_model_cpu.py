@@ -1,6 +1,7 @@
-"""A CPU model of one round of the decode kernel's exact collision test
-(search_plate in brkga_fft2_b200/csrc/brkga_decoder.cu), checked against the
-direct per-pair result on random rounds.
+"""CPU models of the decode kernel's exact collision test (search_plate in
+brkga_fft2_b200/csrc/brkga_decoder.cu): one round of the two-phase test,
+checked against the direct per-pair result on random rounds, and the key
+order of the dealt pairs on which the kernel's early stops rely.
 
 A round holds up to 32 (candidate, 32-column word) pairs in key order.  Each
 pair's open columns F start full and every run of the mask clears the columns
@@ -81,3 +82,39 @@ def test_two_phase_round_equals_direct_walk(solo):
             blocks = [int(np.packbits(row[::-1]).view(">u4")[0]) for row in bits]
             pairs.append((f0, blocks))
         assert two_phase(pairs, solo) == direct(pairs)
+
+
+def key_of(newlen, y, x, r):
+    """The kernel's selection key (smaller is better): newLen, then larger y, smaller x, lower rotation."""
+    return (newlen << 28) | ((8191 - y) << 15) | (x << 2) | r
+
+
+def test_pairs_come_in_key_order():
+    """The decode kernel stops a chunk's rounds, and the shared phase's pairs,
+    as soon as the next pair cannot beat the best key found.  That is exact
+    because pairs are dealt in key order: for survivors from the bottom up and
+    words from the left, every key a pair can produce is at least its own
+    bound, and the bounds never decrease along the dealing order."""
+    rng = np.random.default_rng(7)
+    for _ in range(3000):
+        L = int(rng.integers(2, 600))
+        h = int(rng.integers(1, L + 1))
+        W = int(rng.integers(1, 600))
+        w = int(rng.integers(1, W + 1))
+        enc = int(rng.integers(0, L + 1))
+        r = int(rng.integers(0, 4))
+        level = int(rng.integers(0, max(1, (L - h) // 32 + 1)))
+        ty_hi = L - h - 32 * level
+        if ty_hi < 0:
+            continue
+        lanes = sorted(set(int(v) for v in rng.integers(0, min(32, ty_hi + 1), size=int(rng.integers(1, 33)))))
+        nwo = (W - w + 1 + 31) // 32
+        bounds, worst = [], []
+        for sl in lanes:  # survivors in lane order = bottom-most candidate first
+            ty = ty_hi - sl
+            for k in range(nwo):
+                nl = max(enc, L - ty)
+                bounds.append(key_of(nl, ty + h - 1, 32 * k, r))
+                worst.append(key_of(nl, ty + h - 1, min(32 * k + 31, W - w), r))
+        assert all(b1 <= b2 for b1, b2 in zip(bounds, bounds[1:]))
+        assert all(hi <= b for hi, b in zip(worst, bounds[1:]))  # a pair's worst key is below the next bound
