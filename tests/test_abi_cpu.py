@@ -114,3 +114,29 @@ def test_header_status_codes_match_the_python_mirror():
     assert codes and len(codes) == len(abi.STATUS_NAMES)
     for name, value in codes.items():
         assert getattr(abi, name) == value, name
+
+
+def test_no_cpu_fallback(tmp_path):
+    """Without the CUDA library or without a GPU the product path raises; it never
+    decodes on the CPU."""
+    import pytest as _pytest
+    import torch
+    from brkga_fft2_b200 import instances
+    with _pytest.raises(RuntimeError, match="no CPU fallback"):
+        _load_missing(tmp_path)
+    if torch.cuda.is_available():
+        return
+    from brkga_fft2_b200.evaluator import B200DecoderEvaluator
+    inst = instances.small(2)
+    with _pytest.raises(RuntimeError):
+        B200DecoderEvaluator(inst.problem_data, inst.nb_parts, inst.nb_machines, inst.thresholds, inst.instance_parts)
+
+
+def _load_missing(tmp_path):
+    """abi.load_library on a path with no library, the loaded one put back after."""
+    saved = abi._lib
+    abi._lib = None
+    try:
+        return abi.load_library(str(tmp_path / "missing.so"))
+    finally:
+        abi._lib = saved
