@@ -3,7 +3,11 @@
 best makespan the plain GPU GA finds in its first G generations.
 
     python bench_ga.py [--workload P200M6] [--pop 1000] [--generations 200] [--seeds 3]
-                       [--screened-limit 2.0]
+                       [--screened-limit 2.0] [--train-steps 8] [--explore 0] [--overlap 1]
+
+``--train-steps``, ``--explore`` and ``--overlap`` take comma lists: every
+combination runs its own screened GA against the same plain run per seed,
+and ``by_variant`` holds each one's medians.
 
 Both runs use the same instance, GA parameters (elites ceil(0.1 pop), mutants
 ceil(0.15 pop), rho 0.7 as BRKGA_alg3.py:618) and decoder; each generation is
