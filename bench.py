@@ -6,11 +6,22 @@
 A step decodes one population of 500 seeded synthetic chromosomes of the
 P100M4 workload (100 parts with masks up to 120x120 cells, two 300x300 and
 two 250x250 plates).  ``value`` times the device path with the populations
-already in HBM (CUDA events, L2 flushed by a 256 MiB write between steps);
-``e2e`` times the drop-in ``evaluate_batch`` call with host buffers (H2D copy
-of the chromosomes and D2H of the makespans inside the timed region).  Under
-torchrun every rank decodes its own populations (weak scaling, no data-path
-collective); the time is the max over ranks.
+already in HBM (CUDA events, L2 flushed by a 256 MiB write between steps).
+``e2e`` times the drop-in ``evaluate_batch`` call the way the reference's GA
+makes it (BRKGA_alg3.py:119-123: a fresh pageable ``np.array`` of the
+population), host-to-device copy of the chromosomes and device-to-host copy
+of the makespans inside the timed region; ``e2e_pinned`` is the same call on
+page-locked input.  ``parity`` decodes the rows of the first and the last
+timed step again with placement logs and compares makespans and every
+placement with the CPU oracle (the run fails on any difference); the oracle's
+time on those rows is the ``cpu_baseline``.  ``roofline`` scores the decode
+kernel against the resource that bounds it, integer-ALU issue on chip, with
+its on-chip scan rate against the shared-memory bandwidth measured by this
+library's own streaming probe beside it, and HBM traffic as a check that
+memory does not bound it.  ``time_to_target`` runs the plain GPU GA for 200
+generations and the surrogate-screened GA against its best makespan.
+Under torchrun every rank decodes its own populations (weak scaling, no
+data-path collective); the time is the max over ranks.
 
 ``--impl reference`` times the CPU restatement of the reference decoder on the
 host cores instead (the reference itself is Python and cannot be shipped).
@@ -44,8 +55,11 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--pop", type=int, default=POP)
-    ap.add_argument("--cpu-seconds", type=float, default=12.0)
-    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true",
+                    help="skip the oracle leg (parity check of the timed rows and the CPU baseline)")
+    ap.add_argument("--no-ttt", action="store_true", help="skip the time-to-target record")
+    ap.add_argument("--ttt-seeds", type=int, default=3)
+    ap.add_argument("--ttt-generations", type=int, default=200)
     return ap.parse_args()
 
 
@@ -69,6 +83,14 @@ def workload_config(pop: int, world: int) -> dict:
             "parallelism": f"dp{world} (shards)"}
 
 
+# What the CPU figures time, said in the JSON line itself.
+CPU_CODE = "oracle/brkga_oracle.c"
+CPU_NOTE = ("the C restatement (port) of the reference's sequential decoder, placement.py:94-165 with "
+            "binClassNew.py:45-174; not the reference's own Python placementProcedure + numba + torch_cpu path, "
+            "which cannot be installed or shipped to this box; that path's single-core rate measured on the "
+            "reference's real P100M4-0 instance is 1.33 decodes/s (the port: about 7 per thread)")
+
+
 def measured_peaks():
     path = os.path.join(HERE, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -76,22 +98,6 @@ def measured_peaks():
             d = json.load(f)
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
-
-
-def cpu_rate(packed, n_parts, seconds, threads, seed=12345):
-    """Decodes/s of the CPU oracle on a bounded sample of the workload."""
-    from brkga_fft2_b200 import instances
-    from oracle import oracle_decode
-    probe = instances.chromosomes(threads, n_parts, seed)
-    t0 = time.perf_counter()
-    oracle_decode(packed, probe, n_threads=threads)
-    dt = time.perf_counter() - t0
-    n = int(max(threads, min(20 * threads * 50, threads * round(seconds / max(dt, 1e-3)))))
-    sample = instances.chromosomes(n, n_parts, seed + 1)
-    t0 = time.perf_counter()
-    oracle_decode(packed, sample, n_threads=threads)
-    dt = time.perf_counter() - t0
-    return n / dt, n, dt
 
 
 class ClockSampler:
@@ -154,13 +160,92 @@ class ClockSampler:
                 "interval_ms": 20}
 
 
-def profile_traffic():
-    """dram bytes per decode-kernel launch from the committed ncu summary, if any."""
+def decode_profile():
+    """Per-launch counters of the decode kernel on this workload from the
+    committed ncu summary (instruction counts, DRAM bytes, pipe peaks), or {}."""
     path = os.path.join(HERE, "profiles", "decode_kernel_P100M4.json")
     if os.path.exists(path):
         with open(path) as f:
-            return json.load(f).get("dram_bytes_per_launch")
-    return None
+            return json.load(f)
+    return {}
+
+
+def smem_probe(torch, lib, sm_count):
+    """Shared-memory bandwidth of this GPU from the library's streaming probe
+    (brkga_probe_smem_stream): GB/s over the whole GPU and bytes per SM clock."""
+    import ctypes
+    blocks, threads, iters = 2 * sm_count, 1024, 1024
+    sink = torch.empty(blocks * threads, dtype=torch.int32, device="cuda")
+    cycles = torch.empty(blocks, dtype=torch.int64, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def launch():
+        st = lib.brkga_probe_smem_stream(blocks, threads, iters, ctypes.c_void_p(sink.data_ptr()),
+                                         ctypes.c_void_p(cycles.data_ptr()), ctypes.c_void_p(stream.cuda_stream))
+        if st != 0:
+            raise RuntimeError(f"brkga_probe_smem_stream: status {st}")
+
+    for _ in range(3):
+        launch()
+    times = []
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        launch()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1) / 1000.0)
+    nbytes = blocks * threads * iters * 128
+    per_block = threads * iters * 128
+    cyc = float(cycles.max().item())
+    return {"gbs": nbytes / statistics.median(times) / 1e9, "bytes_per_clk_per_sm": 2 * per_block / cyc,
+            "kernel": "smem_stream_kernel", "bytes_per_launch": nbytes, "launch": f"{blocks}x{threads}"}
+
+
+def roofline_record(prof, kern_s, scan, tests, sm_count, sm_mhz, smem, hbm_peak, peak_kind, build_id):
+    """The decode kernel against the resource that bounds it: integer-ALU issue.
+
+    achieved = ALU-pipe warp instructions of one launch (ncu count of this
+    workload, committed in profiles/) over the launch's live CUDA-event time;
+    peak = SMs x the ALU pipe's warp instructions per SM cycle (ncu's peak
+    for this pipe) x the SM clock sampled during the timed region.  Beside it:
+    all warp instructions against the 4-per-cycle issue limit of an SM, the
+    on-chip scan bytes against the measured shared-memory bandwidth, and the
+    DRAM traffic against HBM."""
+    rec = {"bound": "int_alu", "unit": "G warp-instructions/s", "kernel": "decode_kernel",
+           "kernel_ms": kern_s * 1000.0, "tests_per_launch": tests, "placement_tests_per_s": tests / kern_s}
+    alu = prof.get("alu_warp_inst_per_launch")
+    alu_peak = prof.get("alu_peak_warp_inst_per_cycle_per_sm")
+    clock_hz = (sm_mhz or prof.get("sm_mhz", 1965.0)) * 1e6
+    if alu and alu_peak:
+        achieved = alu / kern_s / 1e9
+        peak = sm_count * alu_peak * clock_hz / 1e9
+        rec.update({"achieved": achieved, "peak": peak, "frac": achieved / peak,
+                    "alu_warp_inst_per_launch": alu, "alu_peak_warp_inst_per_cycle_per_sm": alu_peak,
+                    "sm_clock_mhz": clock_hz / 1e6})
+    else:
+        rec.update({"achieved": None, "peak": None, "frac": None,
+                    "note_missing": "no ALU instruction count in profiles/decode_kernel_P100M4.json"})
+    inst = prof.get("warp_inst_per_launch")
+    if inst:
+        issue = inst / kern_s / 1e9
+        issue_peak = sm_count * 4 * clock_hz / 1e9
+        rec["issue"] = {"achieved": issue, "peak": issue_peak, "frac": issue / issue_peak,
+                        "unit": "G warp-instructions/s", "warp_inst_per_launch": inst}
+    scan_gbs = scan / kern_s / 1e9
+    rec["smem"] = {"achieved": scan_gbs, "peak": smem["gbs"], "frac": scan_gbs / smem["gbs"], "unit": "GB/s",
+                   "algorithmic_bytes_per_launch": scan, "peak_source": "measured (brkga_probe_smem_stream)",
+                   "note": "algorithmic bytes = per placement test one read of the bit-packed plate and rotated "
+                           "mask, 4*(L*ceil(W/32)+h*ceil(w/32)); the kernel stops early, so this is a scan "
+                           "rate, not traffic"}
+    traffic = prof.get("dram_bytes_per_launch")
+    rec["traffic"] = traffic
+    if traffic:
+        rec["hbm"] = {"achieved": traffic / kern_s / 1e9, "peak": hbm_peak, "frac": traffic / kern_s / 1e9 / hbm_peak,
+                      "unit": "GB/s", "peak_source": peak_kind, "dram_bytes_per_launch": traffic}
+    rec["profile_build_id"] = prof.get("build_id")
+    rec["profile_matches_build"] = prof.get("build_id") == build_id
+    return rec
 
 
 def run_reference(args):
@@ -186,7 +271,8 @@ def run_reference(args):
         oracle_decode(packed, ch, n_threads=threads)
         total += time.perf_counter() - t0
     value = n * args.steps / total
-    sample = f"{n} of the {args.pop} chromosomes per step ({WORKLOAD}, instance seed {INSTANCE_SEED})"
+    sample = (f"the first {n} of the {args.pop} chromosomes of each step ({WORKLOAD}, instance seed "
+              f"{INSTANCE_SEED}), {threads} threads")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * total / args.steps,
@@ -194,9 +280,44 @@ def run_reference(args):
         "data": "synthetic (seeded generator, P100M4 shapes)",
         "config": workload_config(args.pop, args.gpus),
         "sample_per_step": n,
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "code": CPU_CODE,
+                         "note": CPU_NOTE, "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
+
+
+def parity_and_cpu(dd, packed, host_rows, P, M, N, torch):
+    """Decode the given host populations again on the GPU with placement logs
+    and with the CPU oracle on all host threads; compare every makespan and
+    every placement.  Returns (parity record, cpu_baseline record)."""
+    import numpy as np
+    from oracle import oracle_decode
+    threads = os.cpu_count() or 1
+    rows = exact = placements_bad = 0
+    cpu_s = 0.0
+    for h in host_rows:
+        dev = torch.from_numpy(h).cuda()
+        log = torch.empty((P, M, N, 5), dtype=torch.int32, device="cuda")
+        ms = dd.decode(dev, log=log).cpu().numpy()
+        glog = log.cpu().numpy()
+        t0 = time.perf_counter()
+        rms, rlog = oracle_decode(packed, h, n_threads=threads, with_log=True)
+        cpu_s += time.perf_counter() - t0
+        rl = np.stack([rlog[f] for f in ("gene", "bin", "x", "y", "rot")], axis=-1)
+        same_row = np.array([np.array_equal(a, b) for a, b in zip(ms, rms)])
+        same_log = (glog == rl).reshape(P, -1).all(axis=1)
+        rows += P
+        exact += int(same_row.sum())
+        placements_bad += int((~same_log).sum())
+    parity = {"rows": rows, "exact": exact, "placements_exact": placements_bad == 0,
+              "rows_with_placement_differences": placements_bad,
+              "checked": "every makespan (==) and every placement (gene, plate, x, bottom row y, rotation) of "
+                         "the first and last timed steps' populations against the CPU oracle"}
+    cpu = {"value": rows / cpu_s, "unit": UNIT, "cores": threads, "kind": "port", "code": CPU_CODE,
+           "note": CPU_NOTE,
+           "sample": f"the {rows} chromosomes of the parity check (the first and last timed steps), decoded "
+                     f"with placement logs on {threads} threads in {cpu_s:.1f} s"}
+    return parity, cpu
 
 
 def run_ours(args):
@@ -211,13 +332,13 @@ def run_ours(args):
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
-    from brkga_fft2_b200 import build as libbuild
+    from brkga_fft2_b200 import abi, build as libbuild
     libbuild.build()
     from brkga_fft2_b200 import instances
     from brkga_fft2_b200.evaluator import B200DecoderEvaluator, DeviceDecoder
 
     inst, packed = load_workload()
-    P, N = args.pop, inst.nb_parts
+    P, N, M = args.pop, inst.nb_parts, inst.nb_machines
     dd = DeviceDecoder(packed, max_pop=P)
     host = [instances.chromosomes(P, N, chrom_seed(rank, s)) for s in range(args.warmup + args.steps)]
     dev = [torch.from_numpy(h).cuda() for h in host]
@@ -241,7 +362,6 @@ def run_ours(args):
     sampler.mark_start()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
            torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    tests = chunks = scan = 0
     for s in range(args.steps):
         flush.fill_(s & 0xFF)  # evict the previous step's data from the 126 MB L2
         e0, k0, k1, e1 = ev[s]
@@ -256,67 +376,84 @@ def run_ours(args):
     clocks = sampler.stop()
     status = int(dd.status.item())
     tests, chunks, bins, scan = dd.counters()  # counters of the last step
+    device_last = out.cpu().numpy()
 
     from brkga_fft2_b200.shard import max_over_ranks, weak_throughput
     total_ms = max_over_ranks(sum(step_ms), dist, "cuda")
     value = weak_throughput(P * args.steps, world, total_ms / 1000.0)
 
-    # e2e through the drop-in evaluator (host buffers, pinned input)
+    # e2e through the drop-in evaluator with host buffers: a fresh pageable array
+    # per call as the reference's GA passes it, and page-locked input beside it
     evaluator = B200DecoderEvaluator(inst.problem_data, inst.nb_parts, inst.nb_machines, inst.thresholds,
                                      inst.instance_parts)
+
+    def e2e_time(inputs):
+        for s in range(args.warmup):
+            evaluator.evaluate_batch(inputs[s])
+        barrier()
+        t, last = 0.0, None
+        for s in range(args.steps):
+            flush.fill_(s & 0xFF)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            last = evaluator.evaluate_batch(inputs[args.warmup + s])
+            t += time.perf_counter() - t0
+        return weak_throughput(P * args.steps, world, max_over_ranks(t, dist, "cuda")), last
+
+    pageable = [np.array(h) for h in host]
+    e2e_value, last_pageable = e2e_time(pageable)
     pinned = [torch.from_numpy(h).pin_memory().numpy() for h in host]
-    for s in range(args.warmup):
-        evaluator.evaluate_batch(pinned[s])
-    barrier()
-    e2e_t = 0.0
-    last = None
-    for s in range(args.steps):
-        flush.fill_(s & 0xFF)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        last = evaluator.evaluate_batch(pinned[args.warmup + s])
-        e2e_t += time.perf_counter() - t0
-    e2e_value = weak_throughput(P * args.steps, world, max_over_ranks(e2e_t, dist, "cuda"))
-    ref_last = out.cpu().numpy()
-    same = bool(np.array_equal(np.asarray(last), ref_last))
+    e2e_pinned, last_pinned = e2e_time(pinned)
+    same = bool(np.array_equal(np.asarray(last_pageable), device_last) and
+                np.array_equal(np.asarray(last_pinned), device_last))
+    failed = False
 
     if rank == 0:
         hbm_peak, peak_kind = measured_peaks()
+        lib = abi.load_library()
+        bid = abi.library_build_id()
+        sm_count = torch.cuda.get_device_properties(local).multi_processor_count
+        smem = smem_probe(torch, lib, sm_count)
         kern_avg_s = statistics.mean(kern_ms) / 1000.0
-        achieved = scan / kern_avg_s / 1e9
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int32",
             "data": "synthetic (seeded generator, P100M4 shapes)",
             "config": workload_config(P, world),
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                         "frac": achieved / hbm_peak, "traffic": profile_traffic(),
-                         "kernel": "decode_kernel", "kernel_ms": statistics.mean(kern_ms),
-                         "algorithmic_bytes_per_launch": scan, "tests_per_launch": tests,
-                         "placement_tests_per_s": tests / kern_avg_s,
-                         "peak_source": peak_kind,
-                         "note": "algorithmic bytes = per placement test one read of the bit-packed plate "
-                                 "and rotated mask, 4*(L*ceil(W/32)+h*ceil(w/32))"},
+            "roofline": roofline_record(decode_profile(), kern_avg_s, scan, tests, sm_count,
+                                        clocks["sm_mhz"] if clocks else None, smem, hbm_peak, peak_kind, bid),
+            "smem_probe": smem,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": P * 2 * N * 4,
-                    "d2h_bytes_per_step": P * 8, "matches_device_path": same},
+                    "d2h_bytes_per_step": P * 8, "input": "pageable (a fresh np.array per call, as "
+                                                          "BRKGA_alg3.py:119-123 passes it)",
+                    "matches_device_path": same},
+            "e2e_pinned": {"value": e2e_pinned, "unit": UNIT, "h2d_bytes_per_step": P * 2 * N * 4,
+                           "d2h_bytes_per_step": P * 8, "input": "page-locked"},
             "gpu_launches": 4 * args.steps,  # assign_sort, order_items, decode, reduce per step
             "kernel_share": statistics.mean(kern_ms) / statistics.mean(step_ms),
             "counters_last_step": {"tests": tests, "row_chunks": chunks, "plates": bins},
             "status": status,
+            "build_id": bid,
         }
         if clocks:
             line["clocks"] = clocks
-        if world == 1 and not args.no_cpu_baseline:
-            threads = os.cpu_count() or 1
-            rate, n, dt = cpu_rate(packed, N, args.cpu_seconds, threads)
-            line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
-                                    "sample": f"{n} seeded {WORKLOAD} chromosomes decoded by the C oracle "
-                                              f"on {threads} threads in {dt:.1f} s"}
+        if not args.no_cpu_baseline:
+            steps = [host[args.warmup]] + ([host[args.warmup + args.steps - 1]] if args.steps > 1 else [])
+            parity, cpu = parity_and_cpu(dd, packed, steps, P, M, N, torch)
+            line["parity"] = parity
+            if world == 1:
+                line["cpu_baseline"] = cpu
+            failed = parity["exact"] != parity["rows"] or not parity["placements_exact"]
+        if world == 1 and not args.no_ttt:
+            import bench_ga
+            line["time_to_target"] = bench_ga.time_to_target(WORKLOAD, P, args.ttt_generations, args.ttt_seeds)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+    if rank == 0 and failed:
+        raise SystemExit("parity check failed: the timed rows differ from the CPU oracle")
 
 
 def main():

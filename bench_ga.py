@@ -57,20 +57,29 @@ def main():
     ap.add_argument("--screened-limit", type=float, default=2.0,
                     help="the screened run may use up to this many times the plain run's generations")
     args = ap.parse_args()
-    import torch
-    from brkga_fft2_b200 import build, instances, pack_problem
-    from brkga_fft2_b200.ga import DeviceBRKGA
+    from brkga_fft2_b200 import build
     build.build()
-    inst = instances.WORKLOADS[args.workload](0)
-    pk = pack_problem(inst.problem_data, inst.nb_parts, inst.nb_machines, inst.thresholds, inst.instance_parts)
-    P = args.pop
-    ne, nm = math.ceil(0.1 * P), math.ceil(0.15 * P)
     variants = [(int(t), float(x), int(o)) for t in str(args.train_steps).split(",")
                 for x in str(args.explore).split(",") for o in str(args.overlap).split(",")]
+    print(json.dumps(time_to_target(args.workload, args.pop, args.generations, args.seeds, args.oversample,
+                                    variants, args.screened_limit)))
+
+
+def time_to_target(workload, P, generations, seeds, oversample=5, variants=((8, 0.0, 1),), screened_limit=2.0):
+    """Plain GPU GA for `generations` generations, then each screened variant
+    (train_steps, explore, overlap) against its best makespan, per seed; the
+    record printed by this script (medians per variant and every run)."""
+    import torch
+    from brkga_fft2_b200 import instances, pack_problem
+    from brkga_fft2_b200.ga import DeviceBRKGA
+    inst = instances.WORKLOADS[workload](0)
+    pk = pack_problem(inst.problem_data, inst.nb_parts, inst.nb_machines, inst.thresholds, inst.instance_parts)
+    ne, nm = math.ceil(0.1 * P), math.ceil(0.15 * P)
+    variants = [tuple(v) for v in variants]
     runs = []
-    for seed in range(args.seeds):
+    for seed in range(seeds):
         plain = DeviceBRKGA(None, inst.nb_parts, inst.nb_machines, inst.thresholds, inst.instance_parts,
-                            num_generations=args.generations, num_individuals=P, num_elites=ne, num_mutants=nm,
+                            num_generations=generations, num_individuals=P, num_elites=ne, num_mutants=nm,
                             eliteCProb=0.7, seed=seed, packed=pk)
         plain.fit()
         target = plain.best_fitness
@@ -80,8 +89,8 @@ def main():
         del plain
         torch.cuda.empty_cache()
         for ts, ex, ov in variants:
-            runs.append(screened_run(args, inst, pk, P, ne, nm, seed, ts, ex, ov, target, t_plain, p_hit,
-                                     t_plain_hit))
+            runs.append(screened_run(generations, screened_limit, oversample, inst, pk, P, ne, nm, seed, ts, ex, ov,
+                                     target, t_plain, p_hit, t_plain_hit))
             torch.cuda.empty_cache()
     by_variant = {}
     for ts, ex, ov in variants:
@@ -91,23 +100,23 @@ def main():
             "ratio_vs_plain_hit_median": float(np.median([r["ratio_vs_plain_hit"] for r in rs])),
             "reached": sum(math.isfinite(r["ratio"]) for r in rs)}
     first = by_variant["train_steps={},explore={:g},overlap={}".format(*variants[0])]
-    print(json.dumps({"metric": "time to plain-GA best makespan, screened vs plain", "workload": args.workload,
-                      "pop": P, "generations": args.generations, "oversample": args.oversample,
-                      "screened_limit": args.screened_limit, "train_steps": variants[0][0],
-                      "explore": variants[0][1], "overlap": variants[0][2], "reached": first["reached"],
-                      "ratio_median": first["ratio_median"],
-                      "ratio_vs_plain_hit_median": first["ratio_vs_plain_hit_median"],
-                      "by_variant": by_variant, "runs": runs}))
+    return {"metric": "time to plain-GA best makespan, screened vs plain", "workload": workload,
+            "pop": P, "generations": generations, "oversample": oversample,
+            "screened_limit": screened_limit, "train_steps": variants[0][0],
+            "explore": variants[0][1], "overlap": variants[0][2], "seeds": seeds, "reached": first["reached"],
+            "ratio_median": first["ratio_median"],
+            "ratio_vs_plain_hit_median": first["ratio_vs_plain_hit_median"],
+            "by_variant": by_variant, "runs": runs}
 
 
-def screened_run(args, inst, pk, P, ne, nm, seed, train_steps, explore, overlap, target, t_plain, p_hit,
-                 t_plain_hit):
+def screened_run(generations, screened_limit, oversample, inst, pk, P, ne, nm, seed, train_steps, explore, overlap,
+                 target, t_plain, p_hit, t_plain_hit):
     """One screened GA against the plain run's target; a dict for the JSON line."""
     from brkga_fft2_b200.ga import DeviceBRKGA
     scr = DeviceBRKGA(None, inst.nb_parts, inst.nb_machines, inst.thresholds, inst.instance_parts,
-                      num_generations=max(1, int(round(args.generations * args.screened_limit))),
+                      num_generations=max(1, int(round(generations * screened_limit))),
                       num_individuals=P, num_elites=ne, num_mutants=nm,
-                      eliteCProb=0.7, seed=seed, packed=pk, screening=True, oversample=args.oversample,
+                      eliteCProb=0.7, seed=seed, packed=pk, screening=True, oversample=oversample,
                       train_steps=train_steps, explore=explore, overlap_training=bool(overlap), target=target)
     scr.fit()
     mins = np.array(scr.history["min"])
@@ -116,7 +125,7 @@ def screened_run(args, inst, pk, P, ne, nm, seed, train_steps, explore, overlap,
     sp = np.array(scr.history["spearman"][1:])
     return {"seed": seed, "train_steps": train_steps, "explore": explore, "overlap": overlap, "target": target,
             "plain_s": t_plain,
-            "plain_gen_ms": 1000 * t_plain / args.generations,
+            "plain_gen_ms": 1000 * t_plain / generations,
             "screened_s": t_scr, "screened_generations": int(hit[0]) if hit.size else None,
             "screened_best": float(mins.min()), "ratio": t_scr / t_plain,
             "plain_hit_generation": p_hit, "plain_hit_s": t_plain_hit,

@@ -111,6 +111,7 @@ def load_library(path: str = LIB_PATH):
     sig = {
         "brkga_abi_version": (c_int, []),
         "brkga_status_string": (ctypes.c_char_p, [c_int]),
+        "brkga_build_id": (ctypes.c_char_p, []),
         "brkga_problem_create": (c_int, [P(BrkgaProblemDesc), P(vp)]),
         "brkga_problem_destroy": (None, [vp]),
         "brkga_workspace_bytes": (c_int, [vp, c_i32, c_i64, P(c_sz)]),
@@ -153,6 +154,7 @@ def load_library(path: str = LIB_PATH):
         "brkga_get_launch_config": (c_int, [vp, c_i64, P(c_i32), P(c_i32), P(c_i32), P(c_i32), P(c_i32)]),
         "brkga_evaluate_host": (c_int, [vp, P(ctypes.c_float), c_i32, P(ctypes.c_double), vp]),
         "brkga_last_counters": (c_int, [vp, P(c_i64), P(c_i64), P(c_i64), P(c_i64)]),
+        "brkga_probe_smem_stream": (c_int, [c_i32, c_i32, c_i32, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -160,8 +162,19 @@ def load_library(path: str = LIB_PATH):
         fn.argtypes = args
     if lib.brkga_abi_version() != ABI_VERSION:
         raise RuntimeError("libbrkga_b200.so ABI version mismatch; rebuild it")
+    if path == LIB_PATH:
+        from .build import build_id
+        have, want = lib.brkga_build_id().decode(), build_id()
+        if have != want:
+            raise RuntimeError(f"{path} was built from other sources (build id {have}, the tree's is {want}); "
+                               "rebuild it (python -m brkga_fft2_b200.build)")
     _lib = lib
     return lib
+
+
+def library_build_id() -> str:
+    """Build id compiled into the loaded library (hash of its sources and flags)."""
+    return load_library().brkga_build_id().decode()
 
 
 def check(status: int, what: str = "") -> None:

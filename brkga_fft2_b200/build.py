@@ -1,13 +1,21 @@
 """Build ``libbrkga_b200.so`` in-tree with nvcc for sm_100a.
 
-    python -m brkga_fft2_b200.build [--force]
+    python -m brkga_fft2_b200.build [--force] [-v]
 
 The library is plain CUDA C++ behind the C ABI of ``include/brkga_b200.h``
 (cudart linked statically), loaded with ctypes by :mod:`brkga_fft2_b200.abi`.
+
+Build identity: the SHA-256 of every source and header together with the
+nvcc command line is the build id.  It is compiled into the library
+(``brkga_build_id()``) and written beside it (``libbrkga_b200.so.buildid``);
+the library is rebuilt whenever the id of the current tree differs from the
+stamp, and :func:`brkga_fft2_b200.abi.load_library` refuses a library whose
+compiled-in id is not the current tree's.
 """
 from __future__ import annotations
 
 import glob
+import hashlib
 import os
 import shutil
 import subprocess
@@ -18,7 +26,9 @@ REPO = os.path.dirname(PKG)
 SOURCES = sorted(glob.glob(os.path.join(PKG, "csrc", "*.cu")))
 HEADERS = sorted(glob.glob(os.path.join(REPO, "include", "*.h"))) + sorted(glob.glob(os.path.join(PKG, "csrc", "*.cuh")))
 LIB = os.path.join(PKG, "libbrkga_b200.so")
+STAMP = LIB + ".buildid"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2", "-shared"]
 
 
 def nvcc() -> str:
@@ -28,18 +38,42 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found")
 
 
+def build_id() -> str:
+    """SHA-256 (first 16 hex digits) of the sources, headers and nvcc flags."""
+    h = hashlib.sha256()
+    for path in SOURCES + HEADERS:
+        h.update(os.path.relpath(path, REPO).encode())
+        h.update(b"\0")
+        with open(path, "rb") as f:
+            h.update(f.read())
+        h.update(b"\0")
+    h.update(" ".join(ARCH + FLAGS).encode())
+    return h.hexdigest()[:16]
+
+
+def stamped_id() -> str:
+    try:
+        with open(STAMP) as f:
+            return f.read().strip()
+    except OSError:
+        return ""
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
-    newest = max(os.path.getmtime(p) for p in SOURCES + HEADERS)
-    if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= newest:
+    bid = build_id()
+    if not force and os.path.exists(LIB) and stamped_id() == bid:
         return LIB
     tmp = LIB + f".tmp{os.getpid()}"
-    cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2", "-shared",
-           "-I", os.path.join(REPO, "include"), "-o", tmp, *SOURCES]
+    cmd = [nvcc(), *ARCH, *FLAGS, f"-DBRKGA_BUILD_ID=\"{bid}\"", "-I", os.path.join(REPO, "include"), "-o", tmp,
+           *SOURCES]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)
     os.replace(tmp, LIB)
+    with open(STAMP + f".tmp{os.getpid()}", "w") as f:
+        f.write(bid + "\n")
+    os.replace(STAMP + f".tmp{os.getpid()}", STAMP)
     return LIB
 
 

@@ -1567,6 +1567,11 @@ extern "C" {
 
 int brkga_abi_version(void) { return BRKGA_ABI_VERSION; }
 
+#ifndef BRKGA_BUILD_ID
+#define BRKGA_BUILD_ID "unstamped"
+#endif
+const char* brkga_build_id(void) { return BRKGA_BUILD_ID; }
+
 // Device tables for the surrogate (same library, not part of the public ABI;
 // single-instance problems, whose table bases are all 0).
 __attribute__((visibility("hidden"))) int brkga_internal_problem_tables(

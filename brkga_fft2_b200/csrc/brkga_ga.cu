@@ -18,6 +18,8 @@
 
 #include <cuda_runtime.h>
 
+#include <mutex>
+
 #include <cstdint>
 
 #include "../../include/brkga_b200.h"
@@ -313,6 +315,24 @@ __global__ void track_kernel(const double* fit, const float* pop, int P, int K, 
   }
 }
 
+// rank_kernel's opt-in to more than 48 KB of dynamic shared memory, once per
+// device: std::call_once makes concurrent first calls from several host
+// threads wait for the one that sets the attribute.
+constexpr int kMaxDevices = 64;
+std::once_flag g_rank_once[kMaxDevices];
+int g_rank_opt_status[kMaxDevices];
+
+int rank_opt_in(int dev) {
+  std::call_once(g_rank_once[dev], [dev] {
+    g_rank_opt_status[dev] =
+        cudaFuncSetAttribute(rank_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kMaxRank * (int)(sizeof(unsigned long long) + sizeof(int))) == cudaSuccess
+            ? BRKGA_OK
+            : BRKGA_ERR_CUDA;
+  });
+  return g_rank_opt_status[dev];
+}
+
 int grid_for(long long n) {
   long long g = (n + 255) / 256;
   if (g > 148 * 16) g = 148 * 16;
@@ -348,15 +368,10 @@ int brkga_ga_rank(const double* d_fitness, int32_t P, int32_t* d_order, void* st
   while (S2 < P) S2 <<= 1;
   const size_t smem = (size_t)S2 * (sizeof(unsigned long long) + sizeof(int));
   if (smem > 48 * 1024) {  // above the default limit: opt in once per device (first call outside capture)
-    static int opted[64] = {0};
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return BRKGA_ERR_CUDA;
-    if (!opted[dev]) {
-      if (cudaFuncSetAttribute(rank_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               kMaxRank * (int)(sizeof(unsigned long long) + sizeof(int))) != cudaSuccess)
-        return BRKGA_ERR_CUDA;
-      opted[dev] = 1;
-    }
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return BRKGA_ERR_CUDA;
+    const int st = rank_opt_in(dev);
+    if (st) return st;
   }
   rank_kernel<<<1, 1024, smem, (cudaStream_t)stream>>>(d_fitness, P, S2, d_order);
   return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;

@@ -93,6 +93,11 @@ typedef struct BrkgaProblem BrkgaProblem; /* opaque, device-resident tables */
 /* Library ABI version (BRKGA_ABI_VERSION). */
 int brkga_abi_version(void);
 
+/* Build identity compiled into the library: a hash of the sources, headers
+ * and compiler flags it was built from ("unstamped" when built without one).
+ * No reference counterpart. */
+const char* brkga_build_id(void);
+
 /* Static text for a status code. */
 const char* brkga_status_string(int status);
 
@@ -377,6 +382,18 @@ int brkga_surrogate_buffers(const BrkgaSurrogate* surrogate, float** params, flo
                             float** y, int32_t** err, int64_t** count, double** norm);
 /* Synchronous copy of an internal array to/from host memory (see brkga_surrogate.cu). */
 int brkga_surrogate_io(BrkgaSurrogate* surrogate, int32_t what, void* host, int64_t bytes, int32_t to_device);
+
+/* ---- Measurement probe (no reference counterpart) ----
+ * Shared-memory streaming kernel: `blocks` CTAs of `threads` threads (a
+ * multiple of 32, at most 1024) each stream `iters` x 8 conflict-free 16-byte
+ * ld.shared loads per thread over a 32 KB buffer.  d_sink: device uint32
+ * [blocks * threads] (a fold of the loaded words, so the loads stay live);
+ * d_cycles: device int64 [blocks], the clock64 cycles each CTA spent in its
+ * load loop.  Bytes moved = blocks * threads * iters * 128; timed by the
+ * caller, they give the shared-memory bandwidth that the decode kernel's
+ * on-chip plate and mask reads are measured against. */
+int brkga_probe_smem_stream(int32_t blocks, int32_t threads, int32_t iters, uint32_t* d_sink,
+                            int64_t* d_cycles, void* stream);
 
 #ifdef __cplusplus
 }

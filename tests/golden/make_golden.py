@@ -369,6 +369,21 @@ def main():
     syn_case("syn_P50M2_s0", i50, syn.chromosomes(32, 50, 1))
     i100 = syn.p100m4(0)
     syn_case("syn_P100M4_s0", i100, syn.chromosomes(8, 100, 1))
+    # six machines: the thresholds 1/6, 2/6, 4/6, 5/6 are not float32-exact
+    # (placement.py:122-127 compares in float32); some machine keys sit on
+    # f32(k/6) and on the next float above it
+    if want("syn_P200M6_s0"):
+        i200 = syn.p200m6(0)
+        ch = syn.chromosomes(4, 200, 1)
+        for r in range(4):
+            for k in range(1, 6):
+                t = np.float32(k / 6)
+                ch[r, 200 + (7 * k + 11 * r) % 200] = t
+                ch[r, 200 + (7 * k + 11 * r + 3) % 200] = np.nextafter(t, np.float32(1))
+        syn_case("syn_P200M6_s0", i200, ch)
+    # the large stress geometry: 600x600 plates, masks up to 240x240 cells
+    if want("syn_P400M8_s0"):
+        syn_case("syn_P400M8_s0", syn.p400m8(0), syn.chromosomes(2, 400, 1))
     small = syn.small(3, n_parts=14, plates=((64, 48), (40, 72)), bbox_max=30)
     syn_case("syn_small_nonsquare", small, syn.chromosomes(48, 14, 2))
     # infeasible parts: machine 1's plate is smaller than some masks (placement.py:47-53)

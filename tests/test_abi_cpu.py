@@ -140,3 +140,14 @@ def _load_missing(tmp_path):
         return abi.load_library(str(tmp_path / "missing.so"))
     finally:
         abi._lib = saved
+
+
+def test_library_carries_the_build_id_of_this_tree(lib):
+    """The loaded library was compiled from the sources now in the tree: its
+    compiled-in id is the hash of the sources, headers and nvcc flags, and the
+    stamp beside it says the same (a stale library is rebuilt, never reused)."""
+    bid = build.build_id()
+    assert len(bid) == 16
+    assert lib.brkga_build_id().decode() == bid
+    assert build.stamped_id() == bid
+    assert abi.library_build_id() == bid

@@ -87,3 +87,26 @@ def test_synthetic_goldens(name):
     np.testing.assert_array_equal(ms, z["makespans"])
     ok = ms < 1e15
     assert (goldens.part_ids_of_log(packed, log)[ok] == z["logs"][ok]).all()
+
+
+def test_six_machine_golden_exercises_the_float32_thresholds():
+    """syn_P200M6_s0 puts machine keys on f32(k/6) and the float above it.
+    placement.py:122-127 compares them with k/6 in float32, the reference's
+    C++ decoder in float64: the two modes must assign some of those genes
+    differently, so the golden really pins the float32 choice (hazard H1)."""
+    from brkga_fft2_b200 import THRESH_F64
+    z = np.load(f"{goldens.GOLDEN}/syn_P200M6_s0.npz")
+    ch = z["chromosomes"]
+    n = ch.shape[1] // 2
+    on = np.zeros(ch.shape[0], bool)
+    for k in range(1, 6):
+        t = np.float32(k / 6)
+        on |= (ch[:, n:] == t).any(axis=1)
+        assert (np.float64(t) != k / 6) == (k != 3)  # only 3/6 is exact in float32
+    assert on.all()
+    p32, _, _ = goldens.load("syn_P200M6_s0")
+    p64, _, _ = goldens.load("syn_P200M6_s0", THRESH_F64)
+    m32 = oracle_decode(p32, ch, n_threads=4)
+    m64 = oracle_decode(p64, ch, n_threads=4)
+    np.testing.assert_array_equal(m32, z["makespans"])
+    assert (m32 != m64).any()

@@ -73,3 +73,38 @@ def test_noalloc_rejects_population_beyond_scratch(setup):
                                      ctypes.c_void_p(s.cuda_stream))
     assert st == abi.ERR_WORKSPACE
     assert abi.NOALLOC_SCRATCH_BYTES == 64 << 20
+
+
+def test_noalloc_full_plate_pool_reports_capacity(setup):
+    """Tables that fit but plates that do not: 600x600 plates (51 KB each, so
+    about 1,300 of them in the scratch array) for 96 P400M8 chromosomes, whose
+    768 items open several plates each.  The device status says
+    BRKGA_ERR_CAPACITY, the rows with an item that ran out are NaN, every other
+    row equals the workspace decode, and a smaller batch afterwards decodes in
+    full."""
+    torch, _, _ = setup
+    from brkga_fft2_b200.evaluator import DeviceDecoder
+    inst = instances.p400m8(0)
+    packed = pack_problem(inst.problem_data, inst.nb_parts, inst.nb_machines, inst.thresholds,
+                          inst.instance_parts)
+    N, M = inst.nb_parts, inst.nb_machines
+    dd = DeviceDecoder(packed, max_pop=96, pool_bins=8 * 96 * M)  # room for 8 plates per item
+    chrom = torch.from_numpy(instances.chromosomes(96, N, 41)).cuda()
+    ref = dd.decode(chrom).clone()
+    torch.cuda.synchronize()
+    assert int(dd.status.item()) == abi.OK
+    out = torch.full((96,), -1.0, dtype=torch.float64, device="cuda")
+    status = torch.full((1,), -1, dtype=torch.int32, device="cuda")
+    assert _noalloc(torch, dd, chrom, out, None, status) == abi.OK
+    torch.cuda.synchronize()
+    assert int(status.item()) == abi.ERR_CAPACITY
+    nan = torch.isnan(out)
+    assert bool(nan.any()), "the pool should have run out for some rows"
+    assert torch.equal(out[~nan], ref[~nan])
+    small = chrom[:8].contiguous()
+    out8 = torch.full((8,), -1.0, dtype=torch.float64, device="cuda")
+    status.fill_(-1)
+    assert _noalloc(torch, dd, small, out8, None, status) == abi.OK
+    torch.cuda.synchronize()
+    assert int(status.item()) == abi.OK
+    assert torch.equal(out8, ref[:8])
