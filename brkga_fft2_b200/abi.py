@@ -76,6 +76,12 @@ class BrkgaPlacement(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int32) for n in ("gene", "bin", "x", "y", "rot")]
 
 
+COLLISION_BITSET = 0
+COLLISION_INT8_TC = 1
+# BrkgaChunkTest: plate, out (device pointers), machine, part_type, rot, ty_hi
+CHUNK_TEST_DTYPE = np.dtype([("plate", "<u8"), ("out", "<u8"), ("machine", "<i4"), ("part_type", "<i4"),
+                             ("rot", "<i4"), ("ty_hi", "<i4")])
+
 PLACEMENT_DTYPE = np.dtype([("gene", "<i4"), ("bin", "<i4"), ("x", "<i4"), ("y", "<i4"), ("rot", "<i4")])
 
 
@@ -155,6 +161,7 @@ def load_library(path: str = LIB_PATH):
         "brkga_evaluate_host": (c_int, [vp, P(ctypes.c_float), c_i32, P(ctypes.c_double), vp]),
         "brkga_last_counters": (c_int, [vp, P(c_i64), P(c_i64), P(c_i64), P(c_i64)]),
         "brkga_probe_smem_stream": (c_int, [c_i32, c_i32, c_i32, vp, vp, vp]),
+        "brkga_chunk_free": (c_int, [vp, c_i32, vp, c_i32, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

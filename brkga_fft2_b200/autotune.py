@@ -130,3 +130,47 @@ def autotune(decoder, chrom, pops=None, shapes: Optional[Iterable[Tuple[int, int
         with open(cache_path, "w") as f:
             json.dump(cache, f, indent=1, sort_keys=True)
     return {"key": key, "config": (w, c, s, t), "ms": ms, "table": table, "cached": False}
+
+
+def collision_paths(decoder, chrom, limit: int = 512, levels=(0, 1, 2), repeats: int = 5,
+                    cache_path: Optional[str] = None, key: Optional[str] = None) -> dict:
+    """Time the two collision-test paths per mask-size bucket on the decoder's own chunks.
+
+    ``chrom`` (float32 CUDA [P, 2N]) is decoded once with placement logs; the
+    plates each part met are replayed (:func:`collision.chunk_cases`) and the
+    chunks of every rotation with a side of at least 64 cells are timed
+    through both paths of ``brkga_chunk_free``: the bit-packed search and the
+    INT8 tensor-core correlation.  Returns ``{"key", "table": [per bucket:
+    chunks, ms and ns per chunk of each path, "choice"], "choices":
+    {bucket: path}, "cached"}``; buckets without chunks are absent.  The
+    decode kernel runs the bit-packed search; the tensor-core path would be
+    taken for a bucket only where it is timed faster.
+    """
+    import torch
+    from . import collision
+    key = (key or grid_key([decoder.packed], decoder.device.index or 0)) + "|collision"
+    cache = {}
+    if cache_path and os.path.exists(cache_path):
+        with open(cache_path) as f:
+            cache = json.load(f)
+    if key in cache:
+        return {"key": key, "table": cache[key]["table"], "choices": cache[key]["choices"], "cached": True}
+    P, pk = chrom.shape[0], decoder.packed
+    log = torch.empty((P, pk.n_machines, pk.n_genes, 5), dtype=torch.int32, device=chrom.device)
+    decoder.decode(chrom, log=log)
+    torch.cuda.synchronize()
+    if int(decoder.status.item()) != 0:
+        raise abi.BrkgaError(int(decoder.status.item()), "decode before the collision-path timing")
+    log = log.cpu().numpy().view(abi.PLACEMENT_DTYPE).reshape(P, pk.n_machines, pk.n_genes)
+    cases, spans = collision.sort_by_bucket(collision.chunk_cases(pk, log, min_side=64, levels=levels, limit=limit))
+    if not cases:
+        return {"key": key, "table": [], "choices": {}, "cached": False}
+    batch = collision.ChunkBatch(decoder.native, pk, cases, device=chrom.device)
+    table = collision.path_table(batch, spans, repeats)
+    choices = {r["bucket"]: r["choice"] for r in table}
+    if cache_path:
+        cache[key] = {"table": table, "choices": choices}
+        os.makedirs(os.path.dirname(os.path.abspath(cache_path)), exist_ok=True)
+        with open(cache_path, "w") as f:
+            json.dump(cache, f, indent=1, sort_keys=True)
+    return {"key": key, "table": table, "choices": choices, "cached": False}

@@ -50,6 +50,7 @@
 #include <vector>
 
 #include "../../include/brkga_b200.h"
+#include "corr_i8.cuh"
 
 namespace {
 
@@ -1051,6 +1052,78 @@ __global__ void __launch_bounds__(kGreedyThreads) greedy_kernel(const __grid_con
   }
 }
 
+// ---------------------------------------------------------------- chunk tests
+// The collision test of one 32-row candidate chunk by either path, for the
+// measurement that decides between them (brkga_chunk_free): the bit-packed
+// run-dilation search the decode kernel uses (word_free, every word tested
+// to the end, no early stop) and the INT8 tensor-core correlation
+// (corr_i8.cuh).  Both write the same words: row n = candidate top row
+// ty_hi - n, bit b of word k = placement at x = 32k + b is collision-free.
+
+// The item's plate geometry and rotation, checked against the tables; false
+// (and BRKGA_ERR_INVALID_ARGUMENT raised) when the item is malformed.
+__device__ __forceinline__ bool chunk_item(const Tables& tb, const BrkgaChunkTest& it, int M, int T, int max_side,
+                                           corr::ChunkArgs* a, RotDev* rdo, int32_t* status) {
+  bool ok = it.plate && it.out && it.machine >= 0 && it.machine < M && it.part_type >= 0 && it.part_type < T &&
+            it.rot >= 0 && it.rot < tb.nrot[it.part_type];
+  if (ok) {
+    const MachDev md = tb.mach[it.machine];
+    const RotDev rd = tb.rot[it.part_type * 4 + it.rot];
+    ok = rd.h <= md.L && rd.w <= md.W && rd.h <= max_side && rd.w <= max_side && it.ty_hi >= 0 &&
+         it.ty_hi <= md.L - rd.h;
+    a->plate = it.plate;
+    a->L = md.L;
+    a->W = md.W;
+    a->RS = md.RS;
+    a->mask = tb.maskbits + rd.mask_base;
+    a->h = rd.h;
+    a->w = rd.w;
+    a->mw = rd.mw;
+    a->ty_hi = it.ty_hi;
+    a->out = it.out;
+    *rdo = rd;
+  }
+  if (!ok && threadIdx.x == 0 && blockIdx.y == 0) raise_status(status, BRKGA_ERR_INVALID_ARGUMENT);
+  return ok;
+}
+
+__global__ void __launch_bounds__(128, 8) chunk_free_bitset_kernel(const Tables tb, const BrkgaChunkTest* items, int M,
+                                                                int T, int32_t* status) {
+  const BrkgaChunkTest it = items[blockIdx.x];
+  corr::ChunkArgs a;
+  RotDev rd;
+  if (!chunk_item(tb, it, M, T, kMaxSide, &a, &rd, status)) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nx = a.W - a.w + 1, nwo = (nx + 31) >> 5;
+  for (int n = warp; n < corr::kN; n += 4) {
+    const int ty = a.ty_hi - n;
+    for (int k = lane; k < nwo; k += 32) {
+      uint32_t F = 0u;
+      if (ty >= 0) {
+        const uint32_t F0 = (k == nwo - 1 && (nx & 31)) ? ((1u << (nx & 31)) - 1u) : kFull;
+        F = word_free(a.plate + (size_t)ty * a.RS, a.RS, k << 5, F0, rd, tb.truns);
+      }
+      a.out[(size_t)n * nwo + k] = F;
+    }
+  }
+}
+
+// grid (items, candidate-column tiles of 128); one CTA per SM (its shared memory)
+__global__ void __launch_bounds__(corr::kThreads, 1) chunk_free_i8_kernel(const Tables tb,
+                                                                          const BrkgaChunkTest* items, int M, int T,
+                                                                          int32_t* status) {
+  extern __shared__ __align__(1024) unsigned char csmem[];
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ uint32_t tmem_slot;
+  __shared__ int fail;
+  const BrkgaChunkTest it = items[blockIdx.x];
+  corr::ChunkArgs a;
+  RotDev rd;
+  if (!chunk_item(tb, it, M, T, corr::kMaxSide, &a, &rd, status)) return;
+  if ((int)blockIdx.y * corr::kTileM > a.W - a.w) return;  // no candidate column in this tile
+  corr::chunk_tile(a, (int)blockIdx.y, csmem, bar, &tmem_slot, &fail, status);
+}
+
 // ---------------------------------------------------------------- host side
 
 size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
@@ -1276,6 +1349,9 @@ int configure(BrkgaProblem* pb, int warps_req, int ctas_req, int plates_req) {
     return BRKGA_ERR_CUDA;
   if (cudaFuncSetAttribute(order_items_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (kMaxGenes + 1) * (int)sizeof(int)) != cudaSuccess)
+    return BRKGA_ERR_CUDA;
+  if (cudaFuncSetAttribute(chunk_free_i8_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           corr::smem_bytes(corr::kMaxSide, corr::kMaxSide)) != cudaSuccess)
     return BRKGA_ERR_CUDA;
   auto fit_for = [&](int ctas) {  // plates per item that fit when `ctas` CTAs share an SM
     const size_t share = per_sm / ctas;
@@ -1970,6 +2046,26 @@ int brkga_initial_solution_host(BrkgaProblem* pb, const int32_t* h_order, int32_
   } while (false);
   cudaFree(d);
   return st;
+}
+
+int brkga_chunk_free(const BrkgaProblem* pb, int32_t path, const BrkgaChunkTest* d_items, int32_t n_items,
+                     int32_t* d_status, void* stream) {
+  if (!pb || pb->K != 1 || n_items < 0 || (path != BRKGA_COLLISION_BITSET && path != BRKGA_COLLISION_INT8_TC))
+    return BRKGA_ERR_INVALID_ARGUMENT;
+  if (n_items == 0) return BRKGA_OK;
+  if (!d_items || !d_status) return BRKGA_ERR_INVALID_ARGUMENT;
+  DeviceGuard g(pb->device);
+  const cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (path == BRKGA_COLLISION_BITSET) {
+    chunk_free_bitset_kernel<<<n_items, 128, 0, s>>>(pb->tb, d_items, pb->M, pb->T, d_status);
+  } else {
+    int wmax = 1;
+    for (const MachDev& m : pb->mach) wmax = std::max(wmax, m.W);
+    const dim3 grid((unsigned)n_items, (unsigned)((wmax + corr::kTileM - 1) / corr::kTileM));
+    chunk_free_i8_kernel<<<grid, corr::kThreads, corr::smem_bytes(corr::kMaxSide, corr::kMaxSide), s>>>(
+        pb->tb, d_items, pb->M, pb->T, d_status);
+  }
+  return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
 }
 
 int brkga_last_counters(const BrkgaProblem* pb, int64_t* tests, int64_t* chunks, int64_t* bins,

@@ -383,6 +383,42 @@ int brkga_surrogate_buffers(const BrkgaSurrogate* surrogate, float** params, flo
 /* Synchronous copy of an internal array to/from host memory (see brkga_surrogate.cu). */
 int brkga_surrogate_io(BrkgaSurrogate* surrogate, int32_t what, void* host, int64_t bytes, int32_t to_device);
 
+/* ---- The collision test of one candidate chunk by either path ----
+ * Replaces, for measurement and for the autotuner's choice of path, the
+ * reference's FFT collision test (collision_backend.py:109-128; native
+ * batch_fft_all_tests, full_native_decoder.py:1004-1234): the overlap of a
+ * rotated part mask with a plate at 32 candidate top rows and every column.
+ *   BRKGA_COLLISION_BITSET   the decode kernel's bit-packed run-dilation search
+ *                            (every output word tested to the end)
+ *   BRKGA_COLLISION_INT8_TC  an INT8 tensor-core correlation (tcgen05.mma
+ *                            kind::i8, INT32 accumulators in tensor memory);
+ *                            masks of at most 256 x 256 cells
+ * One item: `plate` (device) holds L rows of ceil(W/32) + 2 uint32 words of
+ * `machine`'s plate, bit c of a row = column c, zero past column W (the
+ * decoder's plate format); `part_type` and `rot` name a rotation of the
+ * problem; the candidates are top rows ty_hi - n, n = 0..31, with
+ * 0 <= ty_hi <= L - h (rows below 0 come out empty); `out` (device) receives
+ * 32 x ceil((W - w + 1) / 32) words, row n for candidate ty_hi - n, bit b of
+ * word k set when the placement at column x = 32k + b overlaps nothing.
+ * Both paths write identical words. */
+#define BRKGA_COLLISION_BITSET 0
+#define BRKGA_COLLISION_INT8_TC 1
+typedef struct BrkgaChunkTest {
+  const uint32_t* plate;
+  uint32_t* out;
+  int32_t machine;
+  int32_t part_type;
+  int32_t rot;
+  int32_t ty_hi;
+} BrkgaChunkTest;
+
+/* Test n_items chunks (d_items: device array) by `path` on `stream`.  A
+ * malformed item raises BRKGA_ERR_INVALID_ARGUMENT in *d_status (which the
+ * caller zeroes) and writes nothing; a tensor-core wait that times out raises
+ * BRKGA_ERR_CUDA.  Single-instance problems. */
+int brkga_chunk_free(const BrkgaProblem* problem, int32_t path, const BrkgaChunkTest* d_items, int32_t n_items,
+                     int32_t* d_status, void* stream);
+
 /* ---- Measurement probe (no reference counterpart) ----
  * Shared-memory streaming kernel: `blocks` CTAs of `threads` threads (a
  * multiple of 32, at most 1024) each stream `iters` x 8 conflict-free 16-byte
