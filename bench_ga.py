@@ -4,10 +4,14 @@ best makespan the plain GPU GA finds in its first G generations.
 
     python bench_ga.py [--workload P200M6] [--pop 1000] [--generations 200] [--seeds 3]
                        [--screened-limit 2.0] [--train-steps 8] [--explore 0] [--overlap 1]
+                       [--features decode]
 
-``--train-steps``, ``--explore`` and ``--overlap`` take comma lists: every
-combination runs its own screened GA against the same plain run per seed,
-and ``by_variant`` holds each one's medians.
+``--train-steps``, ``--explore``, ``--overlap`` and ``--features`` take comma
+lists: every combination runs its own screened GA against the same plain run
+per seed, and ``by_variant`` holds each one's medians.  ``--features``: the
+surrogate's input, "decode" (per part in decode order its machine, proc time
+and height time, plus per machine its loads) or "order" (per part its
+sequencing key, area and height, parts sorted by key).
 
 Both runs use the same instance, GA parameters (elites ceil(0.1 pop), mutants
 ceil(0.15 pop), rho 0.7 as BRKGA_alg3.py:618) and decoder; each generation is
@@ -54,21 +58,26 @@ def main():
     ap.add_argument("--overlap", default="1",
                     help="1: surrogate training beside the decode on a second stream, 0: after it; a comma list "
                          "runs one screened GA per value")
+    ap.add_argument("--features", default="decode",
+                    help="surrogate input: decode or order; a comma list runs one screened GA per value")
     ap.add_argument("--screened-limit", type=float, default=2.0,
                     help="the screened run may use up to this many times the plain run's generations")
     args = ap.parse_args()
     from brkga_fft2_b200 import build
     build.build()
-    variants = [(int(t), float(x), int(o)) for t in str(args.train_steps).split(",")
-                for x in str(args.explore).split(",") for o in str(args.overlap).split(",")]
+    variants = [(int(t), float(x), int(o), f) for t in str(args.train_steps).split(",")
+                for x in str(args.explore).split(",") for o in str(args.overlap).split(",")
+                for f in str(args.features).split(",")]
     print(json.dumps(time_to_target(args.workload, args.pop, args.generations, args.seeds, args.oversample,
                                     variants, args.screened_limit)))
 
 
-def time_to_target(workload, P, generations, seeds, oversample=5, variants=((8, 0.0, 1),), screened_limit=2.0):
+def time_to_target(workload, P, generations, seeds, oversample=5, variants=((8, 0.0, 1, "decode"),),
+                   screened_limit=2.0):
     """Plain GPU GA for `generations` generations, then each screened variant
-    (train_steps, explore, overlap) against its best makespan, per seed; the
-    record printed by this script (medians per variant and every run)."""
+    (train_steps, explore, overlap, surrogate features) against its best
+    makespan, per seed; the record printed by this script (medians per
+    variant and every run)."""
     import torch
     from brkga_fft2_b200 import instances, pack_problem
     from brkga_fft2_b200.ga import DeviceBRKGA
@@ -88,42 +97,48 @@ def time_to_target(workload, P, generations, seeds, oversample=5, variants=((8, 
         t_plain_hit = plain.history["time"][p_hit]
         del plain
         torch.cuda.empty_cache()
-        for ts, ex, ov in variants:
+        for ts, ex, ov, ft in variants:
             runs.append(screened_run(generations, screened_limit, oversample, inst, pk, P, ne, nm, seed, ts, ex, ov,
-                                     target, t_plain, p_hit, t_plain_hit))
+                                     ft, target, t_plain, p_hit, t_plain_hit))
             torch.cuda.empty_cache()
     by_variant = {}
-    for ts, ex, ov in variants:
-        rs = [r for r in runs if (r["train_steps"], r["explore"], r["overlap"]) == (ts, ex, ov)]
-        by_variant[f"train_steps={ts},explore={ex:g},overlap={ov}"] = {
+    for ts, ex, ov, ft in variants:
+        rs = [r for r in runs if (r["train_steps"], r["explore"], r["overlap"], r["features"]) == (ts, ex, ov, ft)]
+        by_variant[f"train_steps={ts},explore={ex:g},overlap={ov},features={ft}"] = {
             "ratio_median": float(np.median([r["ratio"] for r in rs])),
             "ratio_vs_plain_hit_median": float(np.median([r["ratio_vs_plain_hit"] for r in rs])),
+            "spearman_median": float(np.nanmedian([r["spearman_median"] if r["spearman_median"] is not None
+                                                   else np.nan for r in rs])),
+            "screened_gen_ms_median": float(np.median([r["screened_gen_ms"] for r in rs])),
             "reached": sum(math.isfinite(r["ratio"]) for r in rs)}
-    first = by_variant["train_steps={},explore={:g},overlap={}".format(*variants[0])]
+    first = by_variant["train_steps={},explore={:g},overlap={},features={}".format(*variants[0])]
     return {"metric": "time to plain-GA best makespan, screened vs plain", "workload": workload,
             "pop": P, "generations": generations, "oversample": oversample,
             "screened_limit": screened_limit, "train_steps": variants[0][0],
-            "explore": variants[0][1], "overlap": variants[0][2], "seeds": seeds, "reached": first["reached"],
+            "explore": variants[0][1], "overlap": variants[0][2], "features": variants[0][3], "seeds": seeds,
+            "reached": first["reached"],
             "ratio_median": first["ratio_median"],
             "ratio_vs_plain_hit_median": first["ratio_vs_plain_hit_median"],
             "by_variant": by_variant, "runs": runs}
 
 
 def screened_run(generations, screened_limit, oversample, inst, pk, P, ne, nm, seed, train_steps, explore, overlap,
-                 target, t_plain, p_hit, t_plain_hit):
+                 features, target, t_plain, p_hit, t_plain_hit):
     """One screened GA against the plain run's target; a dict for the JSON line."""
     from brkga_fft2_b200.ga import DeviceBRKGA
     scr = DeviceBRKGA(None, inst.nb_parts, inst.nb_machines, inst.thresholds, inst.instance_parts,
                       num_generations=max(1, int(round(generations * screened_limit))),
                       num_individuals=P, num_elites=ne, num_mutants=nm,
                       eliteCProb=0.7, seed=seed, packed=pk, screening=True, oversample=oversample,
-                      train_steps=train_steps, explore=explore, overlap_training=bool(overlap), target=target)
+                      train_steps=train_steps, explore=explore, overlap_training=bool(overlap), target=target,
+                      surrogate_features=features)
     scr.fit()
     mins = np.array(scr.history["min"])
     hit = np.flatnonzero(mins <= target)
     t_scr = scr.history["time"][int(hit[0])] if hit.size else float("inf")
     sp = np.array(scr.history["spearman"][1:])
-    return {"seed": seed, "train_steps": train_steps, "explore": explore, "overlap": overlap, "target": target,
+    return {"seed": seed, "train_steps": train_steps, "explore": explore, "overlap": overlap, "features": features,
+            "target": target,
             "plain_s": t_plain,
             "plain_gen_ms": 1000 * t_plain / generations,
             "screened_s": t_scr, "screened_generations": int(hit[0]) if hit.size else None,

@@ -137,6 +137,7 @@ def load_library(path: str = LIB_PATH):
         "brkga_ga_audit": (c_int, [vp, vp, vp, c_i32, c_i32, vp, c_i32, vp, vp, vp]),
         "brkga_gemm_bf16": (c_int, [vp, c_i32, vp, c_i32, vp, c_i32, c_i32, c_i32, c_i32, vp, vp]),
         "brkga_surrogate_create": (c_int, [vp, c_i32, c_i32, ctypes.c_uint64, P(vp)]),
+        "brkga_surrogate_create_ex": (c_int, [vp, c_i32, c_i32, ctypes.c_uint64, c_i32, P(vp)]),
         "brkga_surrogate_destroy": (None, [vp]),
         "brkga_surrogate_reset": (c_int, [vp]),
         "brkga_surrogate_dims": (c_int, [vp, P(c_i32), P(c_i32), P(c_i64)]),

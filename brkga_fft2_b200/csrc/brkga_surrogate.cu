@@ -43,6 +43,7 @@ namespace {
 constexpr int kH1 = 512;
 constexpr int kH2 = 256;
 constexpr int kMaxGenes = 8192;
+constexpr int kMaxTrainBatch = 16384;  // rows of one gradient step (the backward kernel keeps dy in shared memory)
 
 struct U4 {
   uint32_t x, y, z, w;
@@ -88,6 +89,8 @@ __device__ inline int machine_of(float mv, const double* thr, int M, int mode) {
 struct FeatParams {
   const float* chrom;
   int P, N, M, T, mode, in_pad;
+  int kind;               // BRKGA_SURROGATE_FEATURES_DECODE or _ORDER
+  float inv_area;         // 1 / largest part area (order features)
   const double* thr;
   const int32_t* gene_type;
   const double* part_area;
@@ -101,6 +104,9 @@ struct FeatParams {
 
 // One CTA per chromosome: sort (machine, key, gene) like the decoder, write the
 // feature row.  Per-machine sums run in decode order, so features are deterministic.
+// Order features (kind BRKGA_SURROGATE_FEATURES_ORDER): the parts sorted by
+// sequencing key alone, machine keys ignored, and per part its key, its area
+// over the largest part area and its height time on machine 0 over the largest.
 __global__ void features_kernel(FeatParams p) {
   extern __shared__ unsigned long long keys[];
   __shared__ float s_area[256], s_pt[256];
@@ -114,7 +120,7 @@ __global__ void features_kernel(FeatParams p) {
   for (int i = tid; i < S2; i += nt) {
     unsigned long long key = ~0ull;
     if (i < p.N) {
-      const int m = machine_of(ch[p.N + i], p.thr, p.M, p.mode);
+      const int m = p.kind == BRKGA_SURROGATE_FEATURES_ORDER ? 0 : machine_of(ch[p.N + i], p.thr, p.M, p.mode);
       key = ((unsigned long long)m << 48) | ((unsigned long long)ordered_bits(ch[i]) << 16) | (unsigned long long)i;
       atomicAdd(&s_cnt[m], 1);
     }
@@ -155,6 +161,18 @@ __global__ void features_kernel(FeatParams p) {
   }
   __syncthreads();
   __nv_bfloat16* row = p.X + (size_t)(p.row_offset + c) * p.in_pad;
+  if (p.kind == BRKGA_SURROGATE_FEATURES_ORDER) {
+    for (int i = tid; i < p.in_pad; i += nt) {
+      float v = 0.f;
+      if (i < 3 * p.N) {
+        const int g = (int)(keys[i / 3] & 0xFFFFu), f = i % 3;
+        const int t = p.gene_type[g];
+        v = f == 0 ? ch[g] : f == 1 ? (float)p.part_area[t] * p.inv_area : (float)p.pth[t] * p.inv_pth;
+      }
+      row[i] = __float2bfloat16(v);
+    }
+    return;
+  }
   const float mscale = p.M > 1 ? 1.f / (float)(p.M - 1) : 0.f;
   for (int i = tid; i < p.in_pad; i += nt) {
     float v = 0.f;
@@ -172,54 +190,6 @@ __global__ void features_kernel(FeatParams p) {
       v = (q & 1) ? s_pt[q >> 1] : s_area[q >> 1];
     }
     row[i] = __float2bfloat16(v);
-  }
-}
-
-// Z <- max(Z + b, 0) in place; optional bf16 copies row-major and transposed
-__global__ void bias_relu_kernel(float* Z, const float* bias, int B, int H, __nv_bfloat16* out,
-                                 __nv_bfloat16* outT) {
-  const long long n = (long long)B * H;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    const int b = (int)(i / H), h = (int)(i - (long long)b * H);
-    const float v = fmaxf(Z[i] + bias[h], 0.f);
-    Z[i] = v;
-    const __nv_bfloat16 q = __float2bfloat16(v);
-    if (out) out[i] = q;
-    if (outT) outT[(size_t)h * B + b] = q;
-  }
-}
-
-// y[b] = sum_k A[b, k] w[k] + b0 (one warp per row)
-__global__ void out_layer_kernel(const float* A, const float* w, const float* b0, int B, int H, float* y) {
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  if (warp >= B) return;
-  float s = 0.f;
-  for (int k = lane; k < H; k += 32) s += A[(size_t)warp * H + k] * w[k];
-  for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xFFFFFFFFu, s, o);
-  if (lane == 0) y[warp] = s + b0[0];
-}
-
-// dZ2 = dy (x) w3, masked by ReLU'; bf16 row-major and transposed
-__global__ void out_backward_kernel(const float* Z2, const float* dy, const float* w3, int B, int H,
-                                    __nv_bfloat16* dZ, __nv_bfloat16* dZT) {
-  const long long n = (long long)B * H;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    const int b = (int)(i / H), h = (int)(i - (long long)b * H);
-    const float g = Z2[i] > 0.f ? dy[b] * w3[h] : 0.f;
-    const __nv_bfloat16 q = __float2bfloat16(g);
-    dZ[i] = q;
-    dZT[(size_t)h * B + b] = q;
-  }
-}
-
-// dZ1 = dH1 masked by ReLU' (in place) and its bf16 transpose
-__global__ void relu_backward_kernel(float* dH, const float* Z, int B, int H, __nv_bfloat16* dZT) {
-  const long long n = (long long)B * H;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    const int b = (int)(i / H), h = (int)(i - (long long)b * H);
-    const float g = Z[i] > 0.f ? dH[i] : 0.f;
-    dH[i] = g;
-    dZT[(size_t)h * B + b] = __float2bfloat16(g);
   }
 }
 
@@ -258,9 +228,88 @@ void col_reduce(const float* A, const float* scale, const float* mask, const flo
   col_reduce_kernel<<<(H + 31) / 32, dim3(32, kColRows), 0, st>>>(A, scale, mask, colscale, B, H, out);
 }
 
-// Adam (Kingma & Ba); the step count t is read from device memory so graph replays stay correct
-__global__ void adam_kernel(float* w, const float* g, float* m, float* v, int n, float lr, float b1, float b2,
-                            float eps, const long long* t_ptr) {
+// The output layer's backward pass and the loss, from the partial dot
+// products the Z2 GEMM's epilogue left per column tile: y = sum of the
+// partials + b3; dy = 2 (y - t) / n on the n valid rows (MSE), 0 on padding;
+// dZ2 = (Z2 > 0) dy w3 as bf16, row-major and transposed; column sums
+// gw3 = sum_b Z2 dy and gb2 = sum_b dZ2 for 32 columns per CTA (rows split
+// over kColRows thread rows, summed in a fixed order).  CTA 0 also writes y,
+// gb3 = sum_b dy, the loss and, with `bump`, advances the minibatch and Adam
+// step counters (read by the next gather and by this step's Adam).
+__global__ void __launch_bounds__(32 * kColRows) out_backward_kernel(
+    const float* part, int n_tiles, int ld_part, const float* b3, const float* t, const int* n_valid, const float* Z2,
+    const float* w3, int B, float* y, __nv_bfloat16* dZ, __nv_bfloat16* dZT, float* gw3, float* gb2, float* gb3,
+    float* loss, long long* step, long long* adam_t, int bump) {
+  extern __shared__ float s_dy[];  // [B]
+  __shared__ float pw[kColRows][33], pb[kColRows][33];
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx, nt = 32 * kColRows;
+  const int n = *n_valid;
+  for (int b = tid; b < B; b += nt) {
+    float v = b3[0];
+    for (int q = 0; q < n_tiles; ++q) v += part[(size_t)q * ld_part + b];
+    s_dy[b] = b < n ? 2.f * (v - t[b]) / (float)n : 0.f;
+    if (blockIdx.x == 0) y[b] = v;
+  }
+  __syncthreads();
+  const int h = blockIdx.x * 32 + tx;
+  const float wh = w3[h];
+  float aw = 0.f, ab = 0.f;
+  for (int b = ty; b < B; b += kColRows) {
+    const float z = Z2[(size_t)b * kH2 + h], d = s_dy[b];
+    const float g = z > 0.f ? d * wh : 0.f;
+    const __nv_bfloat16 q = __float2bfloat16(g);
+    dZ[(size_t)b * kH2 + h] = q;
+    dZT[(size_t)h * B + b] = q;
+    aw += z * d;
+    ab += g;
+  }
+  pw[ty][tx] = aw;
+  pb[ty][tx] = ab;
+  __syncthreads();
+  if (ty == 0) {
+    float sw = 0.f, sb = 0.f;
+#pragma unroll
+    for (int r = 0; r < kColRows; ++r) {
+      sw += pw[r][tx];
+      sb += pb[r][tx];
+    }
+    gw3[h] = sw;
+    gb2[h] = sb;
+  }
+  if (blockIdx.x == 0 && tid == 0) {
+    float sd = 0.f, l = 0.f;
+    for (int b = 0; b < B; ++b) {
+      sd += s_dy[b];
+      const float e = 0.5f * s_dy[b] * (float)n;  // y - t on the valid rows
+      l += b < n ? e * e / (float)n : 0.f;
+    }
+    gb3[0] = sd;
+    *loss = l;
+    if (bump) {
+      *step += 1;
+      *adam_t += 1;
+    }
+  }
+}
+
+// Predictions: y = sum of the output layer's partials + b3, in makespan units
+// once the target scaling is set.
+__global__ void predict_out_kernel(const float* part, int n_tiles, int ld_part, const float* b3, int P,
+                                   const double* norm, float* y, double* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P) return;
+  float v = b3[0];
+  for (int q = 0; q < n_tiles; ++q) v += part[(size_t)q * ld_part + i];
+  y[i] = v;
+  out[i] = norm[2] != 0.0 ? (double)v * norm[1] + norm[0] : (double)v;
+}
+
+// Adam (Kingma & Ba) on every parameter, then the bf16 copies the GEMMs read
+// (W1; W2 row-major and transposed) from the updated values; the step count
+// t is read from device memory so graph replays stay correct.
+__global__ void adam_cast_kernel(float* w, const float* g, float* m, float* v, int n, float lr, float b1, float b2,
+                                 float eps, const long long* t_ptr, int nW1, int offW2, int nW2, __nv_bfloat16* W1b,
+                                 __nv_bfloat16* W2b, __nv_bfloat16* W2Tb) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const float t = (float)(*t_ptr);
@@ -270,7 +319,16 @@ __global__ void adam_kernel(float* w, const float* g, float* m, float* v, int n,
   const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
   m[i] = mi;
   v[i] = vi;
-  w[i] -= lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+  const float wi = w[i] - lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+  w[i] = wi;
+  if (i < nW1) {
+    W1b[i] = __float2bfloat16(wi);
+  } else if (i >= offW2 && i < offW2 + nW2) {
+    const int j = i - offW2, r = j / kH1, c = j - r * kH1;
+    const __nv_bfloat16 q = __float2bfloat16(wi);
+    W2b[j] = q;
+    W2Tb[(size_t)c * kH2 + r] = q;
+  }
 }
 
 __global__ void cast_kernel(const float* W, int rows, int cols, __nv_bfloat16* out, __nv_bfloat16* outT) {
@@ -402,25 +460,6 @@ __global__ void transpose_bf16_kernel(const __nv_bfloat16* X, int B, int I, __nv
   }
 }
 
-__global__ void loss_grad_dev_kernel(const float* y, const float* t, const int* n_valid, int B, float* dy,
-                                     float* loss) {
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= B) return;
-  const int n = *n_valid;
-  float g = 0.f;
-  if (b < n) {
-    const float e = y[b] - t[b];
-    g = 2.f * e / (float)n;
-    atomicAdd(loss, e * e / (float)n);
-  }
-  dy[b] = g;
-}
-
-__global__ void denorm_kernel(const float* y, int P, const double* norm, double* out) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < P) out[i] = norm[2] != 0.0 ? (double)y[i] * norm[1] + norm[0] : (double)y[i];
-}
-
 int grid_for(long long n, int block = 256) {
   long long g = (n + block - 1) / block;
   return (int)std::max(1LL, std::min(g, 148LL * 32));
@@ -451,7 +490,10 @@ struct BrkgaSurrogate {
   __nv_bfloat16 *W1b, *W2b, *W2Tb;
   // activations for up to max_batch rows
   __nv_bfloat16 *X, *XT, *H1b, *H1Tb, *dZ2b, *dZ2Tb, *dZ1Tb;
-  float *Z1, *Z2, *y, *t, *dy, *dH1, *loss;
+  float *Z1, *Z2, *y, *t, *dH1, *loss;
+  float* part;  // [4, max_batch]: the output layer's partial dot per Z2 column tile
+  int features_kind = BRKGA_SURROGATE_FEATURES_DECODE;
+  float inv_area = 1.f;
   int* n_valid;
   int* slot;
   int* err;
@@ -492,17 +534,27 @@ int prepare_gemm() {
 
 // 128 x 128 tiles when they alone fill the GPU twice over, else 128 x 64
 // (these GEMMs are small: more CTAs matter more than tile reuse).
-int gemm(const __nv_bfloat16* A, int lda, const __nv_bfloat16* B, int ldb, float* C, int ldc, int M, int N, int K,
-         int* err, cudaStream_t st) {
+int tile_n(int M, int N) { return (N % 128 == 0 && (long long)(M / 128) * (N / 128) >= 2 * 148) ? 128 : 64; }
+
+int gemm(const __nv_bfloat16* A, int lda, const __nv_bfloat16* B, int ldb, const umma::Epilogue& ep, int M, int N,
+         int K, int* err, cudaStream_t st) {
   if (M % 128 || K % 64 || N % 64) return BRKGA_ERR_INVALID_ARGUMENT;
-  if (N % 128 == 0 && (long long)(M / 128) * (N / 128) >= 2 * 148) {
+  if (tile_n(M, N) == 128) {
     umma::gemm_bf16_kernel<128><<<dim3(M / 128, N / 128), 128, umma::gemm_smem_bytes<128>(), st>>>(A, lda, B, ldb,
-                                                                                                  C, ldc, K, err);
+                                                                                                  ep, K, err);
   } else {
-    umma::gemm_bf16_kernel<64><<<dim3(M / 128, N / 64), 128, umma::gemm_smem_bytes<64>(), st>>>(A, lda, B, ldb, C,
-                                                                                               ldc, K, err);
+    umma::gemm_bf16_kernel<64><<<dim3(M / 128, N / 64), 128, umma::gemm_smem_bytes<64>(), st>>>(A, lda, B, ldb, ep,
+                                                                                               K, err);
   }
   return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
+}
+
+umma::Epilogue store_to(float* C, int ldc) {
+  umma::Epilogue e;
+  e.kind = umma::kStore;
+  e.C = C;
+  e.ldc = ldc;
+  return e;
 }
 
 int features(BrkgaSurrogate* s, const float* d_chrom, int P, __nv_bfloat16* X, cudaStream_t st) {
@@ -522,6 +574,8 @@ int features(BrkgaSurrogate* s, const float* d_chrom, int P, __nv_bfloat16* X, c
   fp.bin_area = s->bin_area;
   fp.inv_pt = s->inv_pt;
   fp.inv_pth = s->inv_pth;
+  fp.kind = s->features_kind;
+  fp.inv_area = s->inv_area;
   fp.X = X;
   fp.row_offset = 0;
   int S2 = 1;
@@ -530,21 +584,78 @@ int features(BrkgaSurrogate* s, const float* d_chrom, int P, __nv_bfloat16* X, c
   return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
 }
 
-// forward on s->X [B, in_pad] (B % 128 == 0) -> s->y; keeps activations for backward
-int forward(BrkgaSurrogate* s, int B, bool keep_transposes, cudaStream_t st) {
+// Forward pass on s->X [B, in_pad] (B % 128 == 0), two GEMMs: Z1 = X W1^T
+// with bias + ReLU in its epilogue -> H1 (bf16; with `train` also Z1 fp32 and
+// H1 transposed for the backward pass), Z2 = H1 W2^T with bias + ReLU and the
+// output layer's dot with w3 per column tile -> s->part (with `train` also Z2
+// fp32).  *n_tiles: the partials per row, summed by the next kernel.
+int forward(BrkgaSurrogate* s, int B, bool train, int* n_tiles, cudaStream_t st) {
   int r;
-  if ((r = gemm(s->X, s->in_pad, s->W1b, s->in_pad, s->Z1, kH1, B, kH1, s->in_pad, s->err, st))) return r;
-  bias_relu_kernel<<<grid_for((long long)B * kH1), 256, 0, st>>>(s->Z1, s->b1, B, kH1, s->H1b,
-                                                                 keep_transposes ? s->H1Tb : nullptr);
-  if ((r = gemm(s->H1b, kH1, s->W2b, kH1, s->Z2, kH2, B, kH2, kH1, s->err, st))) return r;
-  bias_relu_kernel<<<grid_for((long long)B * kH2), 256, 0, st>>>(s->Z2, s->b2, B, kH2, nullptr, nullptr);
-  out_layer_kernel<<<(B * 32 + 255) / 256, 256, 0, st>>>(s->Z2, s->w3, s->b3, B, kH2, s->y);
-  return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
+  umma::Epilogue e1;
+  e1.kind = umma::kBiasRelu;
+  e1.bias = s->b1;
+  e1.out = s->H1b;
+  e1.ld_out = kH1;
+  if (train) {
+    e1.C = s->Z1;
+    e1.ldc = kH1;
+    e1.outT = s->H1Tb;
+    e1.ld_outT = B;
+  }
+  if ((r = gemm(s->X, s->in_pad, s->W1b, s->in_pad, e1, B, kH1, s->in_pad, s->err, st))) return r;
+  umma::Epilogue e2;
+  e2.kind = umma::kBiasRelu;
+  e2.bias = s->b2;
+  e2.dotw = s->w3;
+  e2.part = s->part;
+  e2.ld_part = s->max_batch;
+  if (train) {
+    e2.C = s->Z2;
+    e2.ldc = kH2;
+  }
+  if ((r = gemm(s->H1b, kH1, s->W2b, kH1, e2, B, kH2, kH1, s->err, st))) return r;
+  *n_tiles = kH2 / tile_n(B, kH2);
+  return BRKGA_OK;
 }
 
 int cast_weights(BrkgaSurrogate* s, cudaStream_t st) {
   cast_kernel<<<grid_for((long long)kH1 * s->in_pad), 256, 0, st>>>(s->W1, kH1, s->in_pad, s->W1b, nullptr);
   cast_kernel<<<grid_for((long long)kH2 * kH1), 256, 0, st>>>(s->W2, kH2, kH1, s->W2b, s->W2Tb);
+  return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
+}
+
+// Gradients of the MSE on the minibatch in the activation buffers (forward
+// pass included): the output layer's backward pass in one kernel, then
+// dW2 = dZ2^T H1, dH1 = dZ2 W2 with the ReLU derivative (Z1 > 0) in its
+// epilogue (-> dH1 fp32 and dZ1 transposed bf16), gb1 = column sums of dH1,
+// dW1 = dZ1^T X.  With `bump` the step counters advance (training loop).
+int gradients(BrkgaSurrogate* s, int B, int bump, cudaStream_t st) {
+  int r, n_tiles = 0;
+  const int I = s->in_pad;
+  if ((r = forward(s, B, true, &n_tiles, st))) return r;
+  out_backward_kernel<<<kH2 / 32, dim3(32, kColRows), (size_t)B * sizeof(float), st>>>(
+      s->part, n_tiles, s->max_batch, s->b3, s->t, s->n_valid, s->Z2, s->w3, B, s->y, s->dZ2b, s->dZ2Tb, s->gw3,
+      s->gb2, s->gb3, s->loss, s->step, s->adam_t, bump);
+  if ((r = gemm(s->dZ2Tb, B, s->H1Tb, B, store_to(s->gW2, kH1), kH2, kH1, B, s->err, st))) return r;
+  umma::Epilogue eh;
+  eh.kind = umma::kReluMask;
+  eh.ref = s->Z1;
+  eh.ld_ref = kH1;
+  eh.C = s->dH1;
+  eh.ldc = kH1;
+  eh.outT = s->dZ1Tb;
+  eh.ld_outT = B;
+  if ((r = gemm(s->dZ2b, kH2, s->W2Tb, kH2, eh, B, kH1, kH2, s->err, st))) return r;
+  col_reduce(s->dH1, nullptr, nullptr, nullptr, B, kH1, s->gb1, st);
+  if ((r = gemm(s->dZ1Tb, B, s->XT, B, store_to(s->gW1, I), kH1, I, B, s->err, st))) return r;
+  return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
+}
+
+int adam_cast(BrkgaSurrogate* s, float lr, cudaStream_t st) {
+  const long long nW1 = (long long)kH1 * s->in_pad;
+  adam_cast_kernel<<<grid_for(s->n_params), 256, 0, st>>>(s->params, s->grads, s->mom, s->vel, (int)s->n_params, lr,
+                                                          0.9f, 0.999f, 1e-8f, s->adam_t, (int)nW1,
+                                                          (int)(nW1 + kH1), kH2 * kH1, s->W1b, s->W2b, s->W2Tb);
   return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
 }
 
@@ -580,8 +691,8 @@ int brkga_gemm_bf16(const void* d_A, int32_t lda, const void* d_B, int32_t ldb, 
   if (M == 0 || N == 0 || K == 0) return BRKGA_OK;
   const int st = prepare_gemm();
   if (st) return st;
-  return gemm(static_cast<const __nv_bfloat16*>(d_A), lda, static_cast<const __nv_bfloat16*>(d_B), ldb, d_C, ldc, M,
-              N, K, d_err, static_cast<cudaStream_t>(stream));
+  return gemm(static_cast<const __nv_bfloat16*>(d_A), lda, static_cast<const __nv_bfloat16*>(d_B), ldb,
+              store_to(d_C, ldc), M, N, K, d_err, static_cast<cudaStream_t>(stream));
 }
 
 void brkga_surrogate_destroy(BrkgaSurrogate* s) {
@@ -592,10 +703,18 @@ void brkga_surrogate_destroy(BrkgaSurrogate* s) {
 
 int brkga_surrogate_create(const BrkgaProblem* problem, int32_t max_batch, int32_t buffer_capacity, uint64_t seed,
                            BrkgaSurrogate** out) {
-  if (!problem || !out || max_batch < 128 || max_batch % 128 || buffer_capacity < 1) return BRKGA_ERR_INVALID_ARGUMENT;
+  return brkga_surrogate_create_ex(problem, max_batch, buffer_capacity, seed, BRKGA_SURROGATE_FEATURES_DECODE, out);
+}
+
+int brkga_surrogate_create_ex(const BrkgaProblem* problem, int32_t max_batch, int32_t buffer_capacity, uint64_t seed,
+                              int32_t features, BrkgaSurrogate** out) {
+  if (!problem || !out || max_batch < 128 || max_batch % 128 || buffer_capacity < 1 ||
+      (features != BRKGA_SURROGATE_FEATURES_DECODE && features != BRKGA_SURROGATE_FEATURES_ORDER))
+    return BRKGA_ERR_INVALID_ARGUMENT;
   *out = nullptr;
   BrkgaSurrogate* s = new BrkgaSurrogate();
   s->problem = problem;
+  s->features_kind = features;
   const double* bin_area = nullptr;
   if (brkga_internal_problem_tables(problem, &s->N, &s->M, &s->T, &s->mode, &s->thr, &s->gene_type, &s->part_area,
                                     &s->pt, &s->pth, &bin_area) != BRKGA_OK || s->N > kMaxGenes || s->M > 256) {
@@ -603,7 +722,7 @@ int brkga_surrogate_create(const BrkgaProblem* problem, int32_t max_batch, int32
     return BRKGA_ERR_INVALID_ARGUMENT;
   }
   s->bin_area = bin_area;
-  s->in = 3 * s->N + 2 * s->M;
+  s->in = features == BRKGA_SURROGATE_FEATURES_ORDER ? 3 * s->N : 3 * s->N + 2 * s->M;
   s->in_pad = round_up(s->in, 64);
   s->max_batch = max_batch;
   s->cap = buffer_capacity;
@@ -616,12 +735,21 @@ int brkga_surrogate_create(const BrkgaProblem* problem, int32_t max_batch, int32
       delete s;
       return BRKGA_ERR_CUDA;
     }
+    std::vector<double> area(s->T);
+    if (cudaMemcpy(area.data(), s->part_area, area.size() * 8, cudaMemcpyDeviceToHost) != cudaSuccess) {
+      delete s;
+      return BRKGA_ERR_CUDA;
+    }
     const double mp = *std::max_element(pt.begin(), pt.end()), mh = *std::max_element(pth.begin(), pth.end());
+    const double ma = *std::max_element(area.begin(), area.end());
     s->inv_pt = mp > 0 ? (float)(1.0 / mp) : 1.f;
     s->inv_pth = mh > 0 ? (float)(1.0 / mh) : 1.f;
+    s->inv_area = ma > 0 ? (float)(1.0 / ma) : 1.f;
   }
   if (cudaFuncSetAttribute(features_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxGenes * 8) !=
           cudaSuccess ||
+      cudaFuncSetAttribute(out_backward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           kMaxTrainBatch * (int)sizeof(float)) != cudaSuccess ||
       prepare_gemm() != BRKGA_OK) {
     delete s;
     return BRKGA_ERR_CUDA;
@@ -638,7 +766,7 @@ int brkga_surrogate_create(const BrkgaProblem* problem, int32_t max_batch, int32
       (st = dalloc(s, &s->dZ2b, (size_t)B * kH2)) || (st = dalloc(s, &s->dZ2Tb, (size_t)B * kH2)) ||
       (st = dalloc(s, &s->dZ1Tb, (size_t)B * kH1)) || (st = dalloc(s, &s->Z1, (size_t)B * kH1)) ||
       (st = dalloc(s, &s->Z2, (size_t)B * kH2)) || (st = dalloc(s, &s->y, B)) || (st = dalloc(s, &s->t, B)) ||
-      (st = dalloc(s, &s->dy, B)) || (st = dalloc(s, &s->dH1, (size_t)B * kH1)) || (st = dalloc(s, &s->loss, 1)) ||
+      (st = dalloc(s, &s->part, (size_t)4 * B)) || (st = dalloc(s, &s->dH1, (size_t)B * kH1)) || (st = dalloc(s, &s->loss, 1)) ||
       (st = dalloc(s, &s->n_valid, 1)) || (st = dalloc(s, &s->slot, B)) || (st = dalloc(s, &s->err, 1)) || (st = dalloc(s, &s->count, 1)) ||
       (st = dalloc(s, &s->step, 1)) || (st = dalloc(s, &s->adam_t, 1)) || (st = dalloc(s, &s->norm, 3)) ||
       (st = dalloc(s, &s->bufX, (size_t)s->cap * I)) || (st = dalloc(s, &s->bufY, s->cap))) {
@@ -689,8 +817,10 @@ int brkga_surrogate_predict(BrkgaSurrogate* s, const float* d_chrom, int32_t P, 
     if (B > n && cudaMemsetAsync(s->X + (size_t)n * s->in_pad, 0, (size_t)(B - n) * s->in_pad * 2, st) != cudaSuccess)
       return BRKGA_ERR_CUDA;
     if ((r = features(s, d_chrom + (size_t)off * 2 * s->N, n, s->X, st))) return r;
-    if ((r = forward(s, B, false, st))) return r;
-    denorm_kernel<<<(n + 255) / 256, 256, 0, st>>>(s->y, n, s->norm, d_pred + off);
+    int n_tiles = 0;
+    if ((r = forward(s, B, false, &n_tiles, st))) return r;
+    predict_out_kernel<<<(n + 255) / 256, 256, 0, st>>>(s->part, n_tiles, s->max_batch, s->b3, n, s->norm, s->y,
+                                                        d_pred + off);
   }
   return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
 }
@@ -719,56 +849,34 @@ int brkga_surrogate_observe(BrkgaSurrogate* s, const float* d_chrom, const doubl
   return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
 }
 
-static int gradients(BrkgaSurrogate* s, int B, cudaStream_t st) {
-  int r;
-  const int I = s->in_pad;
-  loss_grad_dev_kernel<<<(B + 255) / 256, 256, 0, st>>>(s->y, s->t, s->n_valid, B, s->dy, s->loss);
-  // output layer
-  col_reduce(s->Z2, s->dy, nullptr, nullptr, B, kH2, s->gw3, st);
-  col_reduce(nullptr, s->dy, nullptr, nullptr, B, 1, s->gb3, st);
-  out_backward_kernel<<<grid_for((long long)B * kH2), 256, 0, st>>>(s->Z2, s->dy, s->w3, B, kH2, s->dZ2b, s->dZ2Tb);
-  col_reduce(nullptr, s->dy, s->Z2, s->w3, B, kH2, s->gb2, st);
-  // layer 2: dW2 = dZ2^T H1, dH1 = dZ2 W2
-  if ((r = gemm(s->dZ2Tb, B, s->H1Tb, B, s->gW2, kH1, kH2, kH1, B, s->err, st))) return r;
-  if ((r = gemm(s->dZ2b, kH2, s->W2Tb, kH2, s->dH1, kH1, B, kH1, kH2, s->err, st))) return r;
-  relu_backward_kernel<<<grid_for((long long)B * kH1), 256, 0, st>>>(s->dH1, s->Z1, B, kH1, s->dZ1Tb);
-  col_reduce(s->dH1, nullptr, nullptr, nullptr, B, kH1, s->gb1, st);
-  // layer 1: dW1 = dZ1^T X
-  if ((r = gemm(s->dZ1Tb, B, s->XT, B, s->gW1, I, kH1, I, B, s->err, st))) return r;
-  return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
-}
-
 int brkga_surrogate_gradients(BrkgaSurrogate* s, int32_t B, void* stream) {
   // gradients of the MSE on the rows already in the activation buffers
   // (s->X, s->XT, s->t, *n_valid) — used by tests and by brkga_surrogate_train
-  if (!s || B < 128 || B % 128 || B > s->max_batch) return BRKGA_ERR_INVALID_ARGUMENT;
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
-  int r;
-  if ((r = forward(s, B, true, st))) return r;
-  if (cudaMemsetAsync(s->loss, 0, sizeof(float), st) != cudaSuccess) return BRKGA_ERR_CUDA;
-  return gradients(s, B, st);
+  if (!s || B < 128 || B % 128 || B > s->max_batch || B > kMaxTrainBatch) return BRKGA_ERR_INVALID_ARGUMENT;
+  return gradients(s, B, 0, static_cast<cudaStream_t>(stream));
 }
 
 int brkga_surrogate_adam(BrkgaSurrogate* s, float lr, void* stream) {
   if (!s) return BRKGA_ERR_INVALID_ARGUMENT;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   bump_kernel<<<1, 1, 0, st>>>(s->adam_t);
-  adam_kernel<<<grid_for(s->n_params), 256, 0, st>>>(s->params, s->grads, s->mom, s->vel, (int)s->n_params, lr, 0.9f,
-                                                      0.999f, 1e-8f, s->adam_t);
-  return cast_weights(s, st);
+  return adam_cast(s, lr, st);
 }
 
 int brkga_surrogate_train(BrkgaSurrogate* s, int32_t steps, int32_t batch, float lr, void* stream) {
-  if (!s || steps < 0 || batch < 128 || batch % 128 || batch > s->max_batch) return BRKGA_ERR_INVALID_ARGUMENT;
+  if (!s || steps < 0 || batch < 128 || batch % 128 || batch > s->max_batch || batch > kMaxTrainBatch)
+    return BRKGA_ERR_INVALID_ARGUMENT;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   int r;
+  // one step = 9 launches: minibatch gather, two forward GEMMs, the output
+  // layer's backward pass (which also advances the step counters), three
+  // backward GEMMs, one column reduction, Adam with the bf16 casts
   for (int i = 0; i < steps; ++i) {
     gather_kernel<<<batch, 128, 0, st>>>(s->bufX, s->bufY, s->count, s->cap, batch, batch, s->in_pad,
                                          (uint32_t)s->seed, (uint32_t)(s->seed >> 32), s->step, s->X, s->XT, s->t,
                                          s->n_valid);
-    bump_kernel<<<1, 1, 0, st>>>(s->step);
-    if ((r = brkga_surrogate_gradients(s, batch, stream))) return r;
-    if ((r = brkga_surrogate_adam(s, lr, stream))) return r;
+    if ((r = gradients(s, batch, 1, st))) return r;
+    if ((r = adam_cast(s, lr, st))) return r;
   }
   return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
 }

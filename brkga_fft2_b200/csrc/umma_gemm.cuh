@@ -16,6 +16,14 @@
 // The epilogue reads the accumulator with tcgen05.ld.32x32b (warp w owns
 // lanes 32w..32w+31 = output rows) and stores fp32.
 //
+// The epilogue (Epilogue below) either stores the fp32 tile, or applies the
+// surrogate's elementwise step in registers before anything leaves the SM:
+// bias + ReLU, or the ReLU derivative of a forward activation, then any of
+// an fp32 store, a bf16 row-major copy, a bf16 transposed copy (the lanes of
+// a warp own consecutive rows, so those stores coalesce) and one partial dot
+// product per row with a weight vector (the 256 -> 1 output layer; each CTA
+// writes the partial of its BN columns, summed later in a fixed order).
+//
 // Every wait is bounded: after kSpinLimit polls the kernel records
 // BRKGA_ERR_CUDA in *err, skips its epilogue, frees its tensor memory and
 // returns.  No TMA and no multicast are used.
@@ -101,6 +109,29 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
+// What the epilogue does with an output tile (see the file comment).
+//   kind kStore:     C[row, col] = acc                                  (fp32)
+//   kind kBiasRelu:  v = max(acc + bias[col], 0)
+//   kind kReluMask:  v = ref[row, col] > 0 ? acc : 0   (ref: the forward activation)
+// then, where the pointer is set: C[row, col] = v, out[row, col] = bf16(v),
+// outT[col, row] = bf16(v), part[tile_n, row] = sum over the tile's columns of v * dotw[col].
+enum EpiKind { kStore = 0, kBiasRelu = 1, kReluMask = 2 };
+struct Epilogue {
+  int kind = kStore;
+  float* C = nullptr;
+  int ldc = 0;
+  const float* bias = nullptr;
+  const float* ref = nullptr;
+  int ld_ref = 0;
+  __nv_bfloat16* out = nullptr;
+  int ld_out = 0;
+  __nv_bfloat16* outT = nullptr;
+  int ld_outT = 0;
+  const float* dotw = nullptr;
+  float* part = nullptr;
+  int ld_part = 0;
+};
+
 // Pipeline: the threads keep kAhead K steps of tiles in flight as
 // asynchronous copies (cp.async, straight into shared memory) while one
 // thread issues the MMAs of the oldest complete step; a buffer is refilled
@@ -109,7 +140,7 @@ __device__ __forceinline__ void cp_async_wait() {
 template <int BN>
 __global__ void __launch_bounds__(128) gemm_bf16_kernel(const __nv_bfloat16* __restrict__ A, int lda,
                                                         const __nv_bfloat16* __restrict__ B, int ldb,
-                                                        float* __restrict__ C, int ldc, int K, int* err) {
+                                                        const __grid_constant__ Epilogue ep, int K, int* err) {
   static_assert(BN == 64 || BN == 128, "BN must be 64 or 128");
   constexpr int kCols = BN;                    // tensor-memory columns (power of two >= 32)
   constexpr int kAWords = kTileM * kTileK / 8;  // uint4 per A stage
@@ -210,6 +241,7 @@ __global__ void __launch_bounds__(128) gemm_bf16_kernel(const __nv_bfloat16* __r
 
   if (!s_fail) {
     const int row = m0 + warp * 32 + lane;
+    float dot = 0.f;
 #pragma unroll 1
     for (int c0 = 0; c0 < BN; c0 += 32) {
       uint32_t v[32];
@@ -224,12 +256,52 @@ __global__ void __launch_bounds__(128) gemm_bf16_kernel(const __nv_bfloat16* __r
             "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
           : "r"(taddr));
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      float4* dst = reinterpret_cast<float4*>(C + (size_t)row * ldc + n0 + c0);
+      const int col0 = n0 + c0;
+      float x[32];
 #pragma unroll
-      for (int q = 0; q < 8; ++q)
-        dst[q] = make_float4(__uint_as_float(v[4 * q]), __uint_as_float(v[4 * q + 1]), __uint_as_float(v[4 * q + 2]),
-                             __uint_as_float(v[4 * q + 3]));
+      for (int j = 0; j < 32; ++j) x[j] = __uint_as_float(v[j]);
+      if (ep.kind == kBiasRelu) {
+#pragma unroll
+        for (int j = 0; j < 32; ++j) x[j] = fmaxf(x[j] + ep.bias[col0 + j], 0.f);
+      } else if (ep.kind == kReluMask) {
+        const float4* r4 = reinterpret_cast<const float4*>(ep.ref + (size_t)row * ep.ld_ref + col0);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const float4 r = r4[q];
+          if (!(r.x > 0.f)) x[4 * q] = 0.f;
+          if (!(r.y > 0.f)) x[4 * q + 1] = 0.f;
+          if (!(r.z > 0.f)) x[4 * q + 2] = 0.f;
+          if (!(r.w > 0.f)) x[4 * q + 3] = 0.f;
+        }
+      }
+      if (ep.C) {
+        float4* dst = reinterpret_cast<float4*>(ep.C + (size_t)row * ep.ldc + col0);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) dst[q] = make_float4(x[4 * q], x[4 * q + 1], x[4 * q + 2], x[4 * q + 3]);
+      }
+      if (ep.out) {
+        uint4* dst = reinterpret_cast<uint4*>(ep.out + (size_t)row * ep.ld_out + col0);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          uint32_t w[4];
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const __nv_bfloat162 pr = __floats2bfloat162_rn(x[8 * q + 2 * e], x[8 * q + 2 * e + 1]);
+            w[e] = *reinterpret_cast<const uint32_t*>(&pr);
+          }
+          dst[q] = make_uint4(w[0], w[1], w[2], w[3]);
+        }
+      }
+      if (ep.outT) {
+#pragma unroll
+        for (int j = 0; j < 32; ++j) ep.outT[(size_t)(col0 + j) * ep.ld_outT + row] = __float2bfloat16(x[j]);
+      }
+      if (ep.dotw) {
+#pragma unroll
+        for (int j = 0; j < 32; ++j) dot += x[j] * ep.dotw[col0 + j];
+      }
     }
+    if (ep.dotw) ep.part[(size_t)blockIdx.y * ep.ld_part + row] = dot;
   } else if (tid == 0) {
     atomicExch(err, 3 /* BRKGA_ERR_CUDA */);
     // let the MMAs still in flight finish before the tensor memory is released

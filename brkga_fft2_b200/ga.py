@@ -13,7 +13,10 @@ the last ``check_every`` generations stays below ``spearman_threshold``
 spread evenly over the rest of the ranked pool, which keeps lower-ranked
 offspring in the population.  With ``overlap_training`` (the default) the
 surrogate trains on a second stream while the decode kernel runs, on the
-rows observed up to the previous generation.
+rows observed up to the previous generation.  ``surrogate_features`` picks
+the surrogate's input: "decode" (per part in decode order its machine, proc
+time and height time, then per machine its loads) or "order" (per part its
+sequencing key, area and height, the parts sorted by key).
 
 With ``audit_fraction > 0`` every generation also copies an evenly spaced
 sample of the rows it decoded (that fraction of them), with their exact
@@ -55,7 +58,7 @@ class DeviceBRKGA:
                  oversample: int = 5, train_steps: int = 8, train_batch: int = 512, lr: float = 1e-3,
                  spearman_threshold: float = 0.3, check_every: int = 5, warmup_generations: int = 5,
                  buffer_capacity: int = 200_000, target: Optional[float] = None, audit_fraction: float = 0.0,
-                 explore: float = 0.0, overlap_training: bool = True):
+                 explore: float = 0.0, overlap_training: bool = True, surrogate_features: str = "decode"):
         import torch
         del collision_backend, eval_mode, eval_workers, eval_chunksize
         self.torch = torch
@@ -137,8 +140,11 @@ class DeviceBRKGA:
             self.o_exact = torch.zeros(max(rows, 1), dtype=torch.int32, device=dev)
             self.stat_scratch = torch.zeros(2 * max(rows, 1), dtype=torch.int32, device=dev)
             self.stats_dev = torch.full((self.num_generations + 1, 2), float("nan"), dtype=torch.float64, device=dev)
-            self.surrogate = Surrogate(self.decoder.native, max_batch=max(self.train_batch, 1024),
-                                       buffer_capacity=buffer_capacity, seed=self.seed ^ 0x5EED)
+            # one prediction batch covers the whole candidate pool
+            batch = max(self.train_batch, self.pool_rows - self.num_elites, 128)
+            self.surrogate = Surrogate(self.decoder.native, max_batch=(batch + 127) // 128 * 128,
+                                       buffer_capacity=buffer_capacity, seed=self.seed ^ 0x5EED,
+                                       features=surrogate_features)
             # Training runs on a second stream while the decode kernel runs (on the rows
             # observed up to the previous generation), joined before the next prediction.
             self.overlap_training = bool(overlap_training)

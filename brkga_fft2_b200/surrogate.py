@@ -31,17 +31,29 @@ def split_params(flat: np.ndarray, in_pad: int):
     return out
 
 
+FEATURES = {"decode": 0, "order": 1}  # BRKGA_SURROGATE_FEATURES_DECODE / _ORDER
+
+
 class Surrogate:
-    def __init__(self, native_problem, max_batch: int = 4096, buffer_capacity: int = 200_000, seed: int = 0):
+    """``features``: "decode" (per part in decode order its machine, proc time
+    and height time, then per machine its area and time load) or "order"
+    (the parts sorted by sequencing key, per part its key, area and height)."""
+
+    def __init__(self, native_problem, max_batch: int = 4096, buffer_capacity: int = 200_000, seed: int = 0,
+                 features: str = "decode"):
         import torch
         self.torch = torch
         self.lib = abi.load_library()
         self.native_problem = native_problem  # keeps the BrkgaProblem alive
         if max_batch % 128:
             raise ValueError("max_batch must be a multiple of 128")
+        if features not in FEATURES:
+            raise ValueError(f"features must be one of {sorted(FEATURES)}")
+        self.features_kind = features
         h = ctypes.c_void_p()
-        abi.check(self.lib.brkga_surrogate_create(native_problem.handle, int(max_batch), int(buffer_capacity),
-                                                  ctypes.c_uint64(seed), ctypes.byref(h)), "brkga_surrogate_create")
+        abi.check(self.lib.brkga_surrogate_create_ex(native_problem.handle, int(max_batch), int(buffer_capacity),
+                                                     ctypes.c_uint64(seed), FEATURES[features], ctypes.byref(h)),
+                  "brkga_surrogate_create_ex")
         self.handle = h
         a, b, n = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int64()
         abi.check(self.lib.brkga_surrogate_dims(h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(n)))

@@ -356,6 +356,16 @@ int brkga_gemm_bf16(const void* d_A, int32_t lda, const void* d_B, int32_t ldb, 
 typedef struct BrkgaSurrogate BrkgaSurrogate;
 int brkga_surrogate_create(const BrkgaProblem* problem, int32_t max_batch /* % 128 == 0 */,
                            int32_t buffer_capacity, uint64_t seed, BrkgaSurrogate** out);
+/* Feature sets: DECODE (the default above) = per part in decode order its
+ * machine, proc time and height time, then per machine its area and time
+ * load (3N + 2M values); ORDER = the parts sorted by sequencing key alone,
+ * per part its key, its area over the largest part area and its height time
+ * over the largest (3N values: the 600-value input of the 200-part screened
+ * configuration).  A gradient step takes at most 16384 rows. */
+#define BRKGA_SURROGATE_FEATURES_DECODE 0
+#define BRKGA_SURROGATE_FEATURES_ORDER 1
+int brkga_surrogate_create_ex(const BrkgaProblem* problem, int32_t max_batch, int32_t buffer_capacity,
+                              uint64_t seed, int32_t features, BrkgaSurrogate** out);
 void brkga_surrogate_destroy(BrkgaSurrogate* surrogate);
 /* Initial weights again, empty example buffer, unset target scaling (synchronous). */
 int brkga_surrogate_reset(BrkgaSurrogate* surrogate);

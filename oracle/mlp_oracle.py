@@ -128,3 +128,29 @@ def features(packed, chrom, in_pad):
         f[3 * N + 1:3 * N + 2 * M:2] = load
         out[r] = bf16(f)
     return out
+
+
+def order_features(packed, chrom, in_pad):
+    """Order feature rows (BRKGA_SURROGATE_FEATURES_ORDER) of host chromosomes:
+    the parts sorted by sequencing key (ties by gene index, machine keys
+    ignored), per part its key, area / largest part area and height time on
+    machine 0 / largest height time, as bf16 values."""
+    a = packed.arrays
+    N, M, T = packed.n_genes, packed.n_machines, packed.n_types
+    pth = a["proc_time_height"].reshape(M, T)
+    inv_pth = np.float32(1.0 / pth.max()) if pth.max() > 0 else np.float32(1)
+    inv_area = np.float32(1.0 / a["part_area"].max())
+    gt = a["gene_type"]
+    out = np.zeros((chrom.shape[0], in_pad), np.float64)
+    for r, ch in enumerate(np.asarray(chrom, np.float32)):
+        sv = ch[:N]
+        svc = np.where(sv == 0, np.float32(0), sv)
+        order = np.lexsort((np.arange(N), svc))
+        f = np.zeros(in_pad, np.float32)
+        for pos, j in enumerate(order):
+            t = gt[j]
+            f[3 * pos] = ch[j]
+            f[3 * pos + 1] = np.float32(a["part_area"][t]) * inv_area
+            f[3 * pos + 2] = np.float32(pth[0, t]) * inv_pth
+        out[r] = bf16(f)
+    return out

@@ -60,6 +60,20 @@ def test_features_match_oracle(torch, p100):
     np.testing.assert_array_equal(got, ref)
 
 
+def test_order_features_match_oracle(torch, p100):
+    """The screened configuration's input (per part its sequencing key, area
+    and height, parts sorted by key); here P100M4: 300 values."""
+    from brkga_fft2_b200.surrogate import Surrogate
+    inst, pk, dd, _ = p100
+    sur = Surrogate(dd.native, max_batch=256, buffer_capacity=1000, seed=3, features="order")
+    assert sur.in_features == 3 * inst.nb_parts and sur.in_pad == 320
+    ch = instances.chromosomes(40, inst.nb_parts, 5)
+    ch[0, :10] = ch[0, 10]  # tied keys keep gene order
+    got = sur.features(torch.from_numpy(ch).cuda())
+    np.testing.assert_array_equal(got, mo.order_features(pk, ch, sur.in_pad))
+    sur.close()
+
+
 def test_forward_gradients_adam_match_oracle(torch, p100):
     from brkga_fft2_b200.surrogate import split_params
     inst, pk, dd, sur = p100
