@@ -350,21 +350,15 @@ __device__ __forceinline__ void raise_status(int32_t* status, int code) {
   atomicCAS(status, 0, code);
 }
 
-// blocked() with the plate row and the words it reads checked first: a run
-// whose access would leave the plate raises BRKGA_ERR_INTERNAL and blocks
-// every column instead of being read.  The checks never fire on consistent
-// tables; they keep the exact test's cooperative phase in bounds whatever
-// the values its lanes exchange.
-__device__ __forceinline__ uint32_t blocked_checked(const uint32_t* grid, int row, int L, int RS, int p0, int d,
-                                                    int32_t* status) {
-  const int whi = ((d <= 32 ? p0 + 32 : p0 + d) >> 5) + 1;
-  if (row < 0 || row >= L || p0 < 0 || d < 1 || whi >= RS) {
-    raise_status(status, BRKGA_ERR_INTERNAL);
-    return kFull;
-  }
-  return blocked(grid + (size_t)row * RS, p0, d);
+// The window a (candidate, output word) pair of the exact test reads: plate
+// rows row0 .. row0 + h - 1 and, in each, the words that the dilations of the
+// mask's runs touch for the 32 columns base .. base + 31 — at most word
+// ((base + w + 31) >> 5) + 1 (a run starts at s >= 0 with s + d <= w, a table
+// invariant of the rotation's run list).  Checked once per pair, so the runs
+// inside need no check of their own.
+__device__ __forceinline__ bool pair_in_plate(int row0, int base, const RotDev& rd, const MachDev& md) {
+  return row0 >= 0 && row0 + rd.h <= md.L && base >= 0 && ((base + rd.w + 31) >> 5) + 1 < md.RS;
 }
-
 
 // Instance of a launch row / item: the last instance starting at or before v
 // (instances with no rows share their start with the next one, which wins).
@@ -610,14 +604,17 @@ __device__ __forceinline__ unsigned long long search_plate(const Tables& tb, con
           sl = surv[si];
           F = k == nwo - 1 ? Flast : kFull;
           const int row0 = ty_hi - sl, base = k << 5;
+          if (!pair_in_plate(row0, base, rd, md)) {  // never on consistent tables: skip the pair, flag the launch
+            raise_status(status, BRKGA_ERR_INTERNAL);
+            F = 0u;
+          }
+          const uint32_t* g0 = grid + (size_t)row0 * md.RS;
           for (; q < qsolo && F; q += 2) {
             const uint2 e0 = __ldg(runs + q);
-            uint32_t bl = blocked_checked(grid, row0 + (int)e0.y, md.L, md.RS, base + (int)(e0.x & 0xFFFFu),
-                                          (int)(e0.x >> 16), status);
+            uint32_t bl = blocked(g0 + (int)e0.y * md.RS, base + (int)(e0.x & 0xFFFFu), (int)(e0.x >> 16));
             if (q + 1 < qsolo) {
               const uint2 e1 = __ldg(runs + q + 1);
-              bl |= blocked_checked(grid, row0 + (int)e1.y, md.L, md.RS, base + (int)(e1.x & 0xFFFFu),
-                                    (int)(e1.x >> 16), status);
+              bl |= blocked(g0 + (int)e1.y * md.RS, base + (int)(e1.x & 0xFFFFu), (int)(e1.x >> 16));
             }
             F &= ~bl;
           }
@@ -650,10 +647,14 @@ __device__ __forceinline__ unsigned long long search_plate(const Tables& tb, con
               break;
             }
           }
+          if (!pair_in_plate(row0, base, rd, md)) {  // warp-uniform: the pair's values came from shuffles
+            if (lane == 0) raise_status(status, BRKGA_ERR_INTERNAL);
+            continue;
+          }
+          const uint32_t* g0 = grid + (size_t)row0 * md.RS;
           for (int qq = ql + lane; qq < n_runs && Fp; qq += 32) {
             const uint2 e = __ldg(runs + qq);
-            Fp &= ~blocked_checked(grid, row0 + (int)e.y, md.L, md.RS, base + (int)(e.x & 0xFFFFu), (int)(e.x >> 16),
-                                   status);
+            Fp &= ~blocked(g0 + (int)e.y * md.RS, base + (int)(e.x & 0xFFFFu), (int)(e.x >> 16));
           }
           for (int o = 1; o < 32; o <<= 1) Fp &= __shfl_xor_sync(kFull, Fp, o);
           if (Fp) {
