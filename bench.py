@@ -196,10 +196,12 @@ def smem_probe(torch, lib, sm_count):
         torch.cuda.synchronize()
         times.append(e0.elapsed_time(e1) / 1000.0)
     nbytes = blocks * threads * iters * 128
-    per_block = threads * iters * 128
-    cyc = float(cycles.max().item())
-    return {"gbs": nbytes / statistics.median(times) / 1e9, "bytes_per_clk_per_sm": 2 * per_block / cyc,
-            "kernel": "smem_stream_kernel", "bytes_per_launch": nbytes, "launch": f"{blocks}x{threads}"}
+    gbs = nbytes / statistics.median(times) / 1e9
+    # per SM and clock: one CTA's bytes over its own load-loop cycles (CTAs of
+    # 1024 threads run one at a time per SM)
+    per_clk = threads * iters * 128 / float(cycles.max().item())
+    return {"gbs": gbs, "bytes_per_clk_per_sm": per_clk, "kernel": "smem_stream_kernel", "bytes_per_launch": nbytes,
+            "launch": f"{blocks}x{threads}"}
 
 
 def roofline_record(prof, kern_s, scan, tests, sm_count, sm_mhz, smem, hbm_peak, peak_kind, build_id):
