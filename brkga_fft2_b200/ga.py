@@ -16,7 +16,12 @@ surrogate trains on a second stream while the decode kernel runs, on the
 rows observed up to the previous generation.  ``surrogate_features`` picks
 the surrogate's input: "decode" (per part in decode order its machine, proc
 time and height time, then per machine its loads) or "order" (per part its
-sequencing key, area and height, the parts sorted by key).
+sequencing key, area and height, the parts sorted by key).  With
+``screen_mutants=False`` (the default) the mutants of a screened generation
+enter unscreened, as in the plain GA, and only the crossover offspring are
+oversampled and ranked (a surrogate ranks random-key mutants low, so
+screening them too removes BRKGA's diversity injection); ``True`` screens
+mutants and offspring together.
 
 With ``audit_fraction > 0`` every generation also copies an evenly spaced
 sample of the rows it decoded (that fraction of them), with their exact
@@ -58,7 +63,8 @@ class DeviceBRKGA:
                  oversample: int = 5, train_steps: int = 8, train_batch: int = 512, lr: float = 1e-3,
                  spearman_threshold: float = 0.3, check_every: int = 5, warmup_generations: int = 5,
                  buffer_capacity: int = 200_000, target: Optional[float] = None, audit_fraction: float = 0.0,
-                 explore: float = 0.0, overlap_training: bool = True, surrogate_features: str = "decode"):
+                 explore: float = 0.0, overlap_training: bool = True, surrogate_features: str = "decode",
+                 screen_mutants: bool = False):
         import torch
         del collision_backend, eval_mode, eval_workers, eval_chunksize
         self.torch = torch
@@ -128,20 +134,26 @@ class DeviceBRKGA:
             self.check_every = max(1, int(check_every))
             self.warmup_generations = int(warmup_generations)
             rows = P - self.num_elites
-            self.pool_rows = self.num_elites + self.oversample * rows
-            if self.pool_rows - self.num_elites > MAX_RANK:
+            # rows that enter every screened generation as they are: the elites
+            # and, unless screen_mutants, the mutants; the rest are offspring
+            # chosen from an oversampled candidate pool by the surrogate
+            self.screen_mutants = bool(screen_mutants)
+            self.n_fixed = self.num_elites + (0 if self.screen_mutants else self.num_mutants)
+            n_screen = P - self.n_fixed
+            self.pool_rows = self.n_fixed + self.oversample * n_screen
+            if self.pool_rows - self.n_fixed > MAX_RANK:
                 raise ValueError(f"oversampled pool too large for the device rank ({MAX_RANK} rows)")
             self.pool = torch.zeros(self.pool_rows, K, dtype=torch.float32, device=dev)
             self.pool_fit = torch.zeros(self.pool_rows, dtype=torch.float64, device=dev)
-            self.pred = torch.zeros(self.pool_rows - self.num_elites, dtype=torch.float64, device=dev)
-            self.order_pool = torch.zeros(self.pool_rows - self.num_elites, dtype=torch.int32, device=dev)
+            self.pred = torch.zeros(max(self.pool_rows - self.n_fixed, 1), dtype=torch.float64, device=dev)
+            self.order_pool = torch.zeros(max(self.pool_rows - self.n_fixed, 1), dtype=torch.int32, device=dev)
             self.pred_sel = torch.zeros(max(rows, 1), dtype=torch.float64, device=dev)
             self.o_pred = torch.zeros(max(rows, 1), dtype=torch.int32, device=dev)
             self.o_exact = torch.zeros(max(rows, 1), dtype=torch.int32, device=dev)
             self.stat_scratch = torch.zeros(2 * max(rows, 1), dtype=torch.int32, device=dev)
             self.stats_dev = torch.full((self.num_generations + 1, 2), float("nan"), dtype=torch.float64, device=dev)
             # one prediction batch covers the whole candidate pool
-            batch = max(self.train_batch, self.pool_rows - self.num_elites, 128)
+            batch = max(self.train_batch, self.pool_rows - self.n_fixed, rows, 128)
             self.surrogate = Surrogate(self.decoder.native, max_batch=(batch + 127) // 128 * 128,
                                        buffer_capacity=buffer_capacity, seed=self.seed ^ 0x5EED,
                                        features=surrogate_features)
@@ -151,14 +163,14 @@ class DeviceBRKGA:
             self._train_stream = torch.cuda.Stream(dev) if self.overlap_training else None
             # exploration: that share of the decoded rows is spread evenly over the
             # pool's lower-ranked candidates instead of taken from its top
-            cand = self.pool_rows - self.num_elites
-            self.n_explore = min(rows, max(0, int(round(float(explore) * rows))))
+            cand = self.pool_rows - self.n_fixed
+            self.n_explore = min(n_screen, max(0, int(round(float(explore) * n_screen))))
             if self.n_explore:
-                top = rows - self.n_explore
-                sel = np.arange(rows, dtype=np.int64)
+                top = n_screen - self.n_explore
+                sel = np.arange(n_screen, dtype=np.int64)
                 sel[top:] = top + (np.arange(self.n_explore) * (cand - top)) // self.n_explore
                 self.sel_idx = torch.from_numpy(sel).to(dev)
-                self.order_sel = torch.zeros(rows, dtype=torch.int32, device=dev)
+                self.order_sel = torch.zeros(n_screen, dtype=torch.int32, device=dev)
 
     # ---- kernels of one generation ------------------------------------------------
     @staticmethod
@@ -247,23 +259,25 @@ class DeviceBRKGA:
         """Oversampled pool -> surrogate ranking -> exact decode of the best-predicted rows."""
         nxt = 1 - cur
         P, K, ne, nm = self.num_individuals, self.num_gene, self.num_elites, self.num_mutants
-        rows = P - ne
+        rows, nf = P - ne, self.n_fixed
         self._rank(self.fitness_buf[cur], P, self.order)
+        pool_mutants = nm * self.oversample if self.screen_mutants else nm
         abi.check(self.lib.brkga_ga_breed_pool(self._ptr(self.pop[cur]), self._ptr(self.fitness_buf[cur]),
-                                               self._ptr(self.order), P, self.pool_rows, K, ne, nm * self.oversample,
+                                               self._ptr(self.order), P, self.pool_rows, K, ne, pool_mutants,
                                                ctypes.c_float(self.eliteCProb), ctypes.c_uint64(self.seed),
                                                self._ptr(self.generation), self._ptr(self.pool),
                                                self._ptr(self.pool_fit), self._stream()), "brkga_ga_breed_pool")
-        cand = self.pool_rows - ne
-        self.surrogate.predict(self.pool[ne:], out=self.pred)
-        self._rank(self.pred, cand, self.order_pool)
-        order = self.order_pool
-        if self.n_explore:
-            self.torch.index_select(self.order_pool, 0, self.sel_idx, out=self.order_sel)
-            order = self.order_sel
-        abi.check(self.lib.brkga_ga_gather(self._ptr(self.pool[ne:]), self._ptr(order), rows, K,
-                                           self._ptr(self.pop[nxt][ne:]), self._stream()), "brkga_ga_gather")
-        self.pop[nxt][:ne].copy_(self.pool[:ne])
+        cand = self.pool_rows - nf
+        if P > nf:
+            self.surrogate.predict(self.pool[nf:], out=self.pred[:cand])
+            self._rank(self.pred, cand, self.order_pool)
+            order = self.order_pool
+            if self.n_explore:
+                self.torch.index_select(self.order_pool, 0, self.sel_idx, out=self.order_sel)
+                order = self.order_sel
+            abi.check(self.lib.brkga_ga_gather(self._ptr(self.pool[nf:]), self._ptr(order), P - nf, K,
+                                               self._ptr(self.pop[nxt][nf:]), self._stream()), "brkga_ga_gather")
+        self.pop[nxt][:nf].copy_(self.pool[:nf])
         self.fitness_buf[nxt][:ne].copy_(self.pool_fit[:ne])
         self._train_fork()
         if rows > 0:

@@ -105,11 +105,12 @@ def test_ga_initial_solution_kept(torch):
     assert ga.best_fitness == best
 
 
-@pytest.mark.parametrize("explore", [0.0, 0.3])
-def test_screened_ga_reports_exact_makespans(torch, explore):
-    """With surrogate screening (and an exploration share of the decoded rows
-    taken from the lower-ranked pool) every reported makespan still comes from
-    the exact decoder; Spearman and MAE are logged for every generation."""
+@pytest.mark.parametrize("explore,screen_mutants", [(0.0, False), (0.3, False), (0.0, True)])
+def test_screened_ga_reports_exact_makespans(torch, explore, screen_mutants):
+    """With surrogate screening (mutants unscreened or screened with the
+    offspring, and an exploration share of the decoded rows taken from the
+    lower-ranked pool) every reported makespan still comes from the exact
+    decoder; Spearman and MAE are logged for every generation."""
     from brkga_fft2_b200.ga import DeviceBRKGA
     from oracle import oracle_decode
     inst = instances.p50m2(0)
@@ -117,7 +118,7 @@ def test_screened_ga_reports_exact_makespans(torch, explore):
     ga = DeviceBRKGA(None, inst.nb_parts, inst.nb_machines, inst.thresholds, inst.instance_parts,
                      num_generations=20, num_individuals=200, num_elites=20, num_mutants=30, packed=pk, seed=3,
                      screening=True, oversample=4, warmup_generations=4, check_every=2, spearman_threshold=-1.0,
-                     explore=explore)
+                     explore=explore, screen_mutants=screen_mutants)
     ga.fit()
     np.testing.assert_array_equal(ga.fitness, oracle_decode(pk, ga.population, n_threads=8))
     assert ga.best_fitness == min(ga.history["min"])
