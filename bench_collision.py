@@ -8,7 +8,10 @@ each part met, and times brkga_chunk_free on the resulting 32-row candidate
 chunks (rotations with a side of at least 64 cells) through both paths — the
 bit-packed run-dilation search (every word tested to the end) and the INT8
 tensor-core correlation (tcgen05.mma kind::i8) — per mask-size bucket, after
-checking that both give identical free-position words.  Beside the table:
+checking that both give identical free-position words; each bucket's
+chunks are repeated until one launch holds ``--target-chunks`` of them, so
+the figures are throughput (GPU ns per chunk, and SM microseconds per
+chunk), not the latency of a handful of chunks.  Beside the table:
 the decode kernel's own GPU time per placement test on a population of 256
 (one placement test = one rotation of one part on one plate; the kernel
 stops at the first free placement of the bottom-most candidate).  Prints one
@@ -33,6 +36,8 @@ def main():
     ap.add_argument("--limit", type=int, default=512)
     ap.add_argument("--levels", default="0,1,2")
     ap.add_argument("--repeats", type=int, default=5)
+    ap.add_argument("--target-chunks", type=int, default=4736,
+                    help="chunks per timed launch (each bucket's chunks repeated to fill the GPU)")
     args = ap.parse_args()
     import torch
     from brkga_fft2_b200 import abi, build, collision, instances, pack_problem
@@ -48,20 +53,15 @@ def main():
     torch.cuda.synchronize()
     log = log.cpu().numpy().view(abi.PLACEMENT_DTYPE).reshape(P, M, N)
     levels = tuple(int(v) for v in args.levels.split(","))
-    cases, spans = collision.sort_by_bucket(collision.chunk_cases(pk, log, min_side=64, levels=levels,
-                                                                  limit=args.limit))
-    batch = collision.ChunkBatch(dd.native, pk, cases)
-    batch.run(abi.COLLISION_BITSET)
-    ref = [batch.words(i) for i in range(len(cases))]
-    batch.out.fill_(-1)
-    batch.run(abi.COLLISION_INT8_TC)
-    torch.cuda.synchronize()
-    same = all(np.array_equal(batch.words(i), ref[i]) for i in range(len(cases)))
-    if not same or int(batch.status.item()):
-        raise SystemExit(f"paths differ (status {int(batch.status.item())})")
-    table = collision.path_table(batch, spans, args.repeats)
-    total_bit = sum(r["bitset_ms"] for r in table)
-    total_i8 = sum(r["int8_tc_ms"] for r in table)
+    cases = collision.chunk_cases(pk, log, min_side=64, levels=levels, limit=args.limit)
+    table = collision.bucket_table(dd.native, pk, cases, target_chunks=args.target_chunks, repeats=args.repeats)
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    for r in table:  # SM time per chunk at throughput
+        r["bitset_sm_us_per_chunk"] = r["bitset_ns_per_chunk"] * sms / 1e3
+        r["int8_tc_sm_us_per_chunk"] = r["int8_tc_ns_per_chunk"] * sms / 1e3
+    w = [r["chunks"] for r in table]
+    mean_bit = float(np.average([r["bitset_ns_per_chunk"] for r in table], weights=w))
+    mean_i8 = float(np.average([r["int8_tc_ns_per_chunk"] for r in table], weights=w))
     # the decode kernel's own rate: GPU time per placement test on 256 chromosomes
     pop = torch.from_numpy(instances.chromosomes(256, N, 78)).cuda()
     out = torch.empty(256, dtype=torch.float64, device="cuda")
@@ -72,11 +72,10 @@ def main():
     torch.cuda.synchronize()
     tests = dd.counters()[0]
     kms = k0.elapsed_time(k1)
-    sms = torch.cuda.get_device_properties(0).multi_processor_count
     print(json.dumps({
-        "workload": args.workload, "chunks": len(cases), "levels": list(levels), "identical_words": same,
-        "table": table, "all_buckets": {"bitset_ms": total_bit, "int8_tc_ms": total_i8,
-                                        "int8_over_bitset": total_i8 / total_bit},
+        "workload": args.workload, "chunks": len(cases), "levels": list(levels), "identical_words": True,
+        "table": table, "all_buckets": {"bitset_ns_per_chunk": mean_bit, "int8_tc_ns_per_chunk": mean_i8,
+                                        "int8_over_bitset": mean_i8 / mean_bit},
         "decoder_pop256": {"kernel_ms": kms, "placement_tests": tests, "ns_per_test": 1e6 * kms / tests,
                            "sm_us_per_test": 1e3 * kms * sms / tests},
         "build_id": abi.library_build_id()}))

@@ -140,7 +140,8 @@ def collision_paths(decoder, chrom, limit: int = 512, levels=(0, 1, 2), repeats:
     plates each part met are replayed (:func:`collision.chunk_cases`) and the
     chunks of every rotation with a side of at least 64 cells are timed
     through both paths of ``brkga_chunk_free``: the bit-packed search and the
-    INT8 tensor-core correlation.  Returns ``{"key", "table": [per bucket:
+    INT8 tensor-core correlation, each bucket's chunks repeated until a launch
+    fills the GPU (throughput, not the latency of a few chunks).  Returns ``{"key", "table": [per bucket:
     chunks, ms and ns per chunk of each path, "choice"], "choices":
     {bucket: path}, "cached"}``; buckets without chunks are absent.  The
     decode kernel runs the bit-packed search; the tensor-core path would be
@@ -162,11 +163,10 @@ def collision_paths(decoder, chrom, limit: int = 512, levels=(0, 1, 2), repeats:
     if int(decoder.status.item()) != 0:
         raise abi.BrkgaError(int(decoder.status.item()), "decode before the collision-path timing")
     log = log.cpu().numpy().view(abi.PLACEMENT_DTYPE).reshape(P, pk.n_machines, pk.n_genes)
-    cases, spans = collision.sort_by_bucket(collision.chunk_cases(pk, log, min_side=64, levels=levels, limit=limit))
+    cases = collision.chunk_cases(pk, log, min_side=64, levels=levels, limit=limit)
     if not cases:
         return {"key": key, "table": [], "choices": {}, "cached": False}
-    batch = collision.ChunkBatch(decoder.native, pk, cases, device=chrom.device)
-    table = collision.path_table(batch, spans, repeats)
+    table = collision.bucket_table(decoder.native, pk, cases, repeats=repeats, device=chrom.device)
     choices = {r["bucket"]: r["choice"] for r in table}
     if cache_path:
         cache[key] = {"table": table, "choices": choices}

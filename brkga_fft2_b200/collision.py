@@ -99,14 +99,20 @@ def bucket_of(side: int) -> int:
 
 
 class ChunkBatch:
-    """Chunk cases on the device: plates, output words and the item array."""
+    """Chunk cases on the device: plates, output words and the item array.
 
-    def __init__(self, native, packed: PackedProblem, cases: List[dict], device=None):
+    With ``copies`` > 1 every case is listed that many times in a row (same
+    plate, its own output words), so that one launch over a bucket holds
+    enough chunks to fill the GPU and times throughput, not the latency of
+    a few chunks.  Ranges given to ``run`` / ``time`` count cases."""
+
+    def __init__(self, native, packed: PackedProblem, cases: List[dict], device=None, copies: int = 1):
         import torch
         self.torch = torch
         self.native = native
         self.lib = native.lib
         self.cases = cases
+        self.copies = max(1, int(copies))
         dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         a = packed.arrays
         plates, pofs, oofs, self.nwo = [], [], [], []
@@ -119,29 +125,32 @@ class ChunkBatch:
             nwo = (int(a["bin_width"][c["machine"]]) - c["w"] + 1 + 31) // 32
             self.nwo.append(nwo)
             oofs.append(o)
-            o += 32 * nwo
+            o += 32 * nwo * self.copies
         self.plates = torch.from_numpy(np.concatenate(plates).view(np.int32)).to(dev)
         self.out = torch.zeros(max(o, 1), dtype=torch.int32, device=dev)
         self.out_offsets = oofs
-        items = np.zeros(len(cases), abi.CHUNK_TEST_DTYPE)
+        items = np.zeros(len(cases) * self.copies, abi.CHUNK_TEST_DTYPE)
         pb, ob = self.plates.data_ptr(), self.out.data_ptr()
         for i, c in enumerate(cases):
-            items[i] = (pb + 4 * pofs[i], ob + 4 * oofs[i], c["machine"], c["type"], c["rot"], c["ty_hi"])
+            for k in range(self.copies):
+                items[i * self.copies + k] = (pb + 4 * pofs[i], ob + 4 * (oofs[i] + 32 * self.nwo[i] * k), c["machine"],
+                                              c["type"], c["rot"], c["ty_hi"])
         self.items = torch.from_numpy(items.view(np.uint8)).to(dev)
         self.status = torch.zeros(1, dtype=torch.int32, device=dev)
 
     def run(self, path: int, first: int = 0, count: int = -1, stream=None):
         torch = self.torch
-        n = len(self.cases) - first if count < 0 else count
+        n = (len(self.cases) - first if count < 0 else count) * self.copies
         s = stream if stream is not None else torch.cuda.current_stream()
-        ptr = self.items.data_ptr() + first * abi.CHUNK_TEST_DTYPE.itemsize
+        ptr = self.items.data_ptr() + first * self.copies * abi.CHUNK_TEST_DTYPE.itemsize
         abi.check(self.lib.brkga_chunk_free(self.native.handle, path, ctypes.c_void_p(ptr), n,
                                             ctypes.c_void_p(self.status.data_ptr()), ctypes.c_void_p(s.cuda_stream)),
                   "brkga_chunk_free")
 
-    def words(self, i: int) -> np.ndarray:
+    def words(self, i: int, copy: int = 0) -> np.ndarray:
         """Free-position words [32, nwo] of case i (synchronises)."""
-        o, nwo = self.out_offsets[i], self.nwo[i]
+        nwo = self.nwo[i]
+        o = self.out_offsets[i] + 32 * nwo * copy
         return self.out[o: o + 32 * nwo].cpu().numpy().view(np.uint32).reshape(32, nwo)
 
     def time(self, path: int, first: int = 0, count: int = -1, repeats: int = 5) -> float:
@@ -174,14 +183,39 @@ def sort_by_bucket(cases: List[dict]) -> Tuple[List[dict], Dict[int, Tuple[int, 
 
 
 def path_table(batch: ChunkBatch, spans: Dict[int, Tuple[int, int]], repeats: int = 5) -> List[dict]:
-    """Per mask-size bucket: cases, ms per launch and ns per chunk of each path."""
+    """Per mask-size bucket: distinct chunks, chunks per launch (with the
+    batch's copies), ms per launch and GPU ns per chunk of each path."""
     rows = []
     for b, (first, n) in sorted(spans.items()):
         t_bit = batch.time(abi.COLLISION_BITSET, first, n, repeats)
         t_i8 = batch.time(abi.COLLISION_INT8_TC, first, n, repeats)
         lo, hi = BUCKETS[b]
-        rows.append({"bucket": f"{lo}-{hi - 1}", "chunks": n, "bitset_ms": t_bit, "int8_tc_ms": t_i8,
-                     "bitset_ns_per_chunk": 1e6 * t_bit / n, "int8_tc_ns_per_chunk": 1e6 * t_i8 / n,
-                     "int8_over_bitset": t_i8 / t_bit,
+        per = n * batch.copies
+        rows.append({"bucket": f"{lo}-{hi - 1}", "chunks": n, "chunks_per_launch": per, "bitset_ms": t_bit,
+                     "int8_tc_ms": t_i8, "bitset_ns_per_chunk": 1e6 * t_bit / per,
+                     "int8_tc_ns_per_chunk": 1e6 * t_i8 / per, "int8_over_bitset": t_i8 / t_bit,
                      "choice": "int8_tc" if t_i8 < t_bit else "bitset"})
+    return rows
+
+
+def bucket_table(native, packed: PackedProblem, cases: List[dict], target_chunks: int = 4736, repeats: int = 5,
+                 device=None) -> List[dict]:
+    """Both paths timed per mask-size bucket at throughput: each bucket's cases
+    are repeated until one launch holds about ``target_chunks`` chunks (by
+    default four waves of the bit-packed path's 4-warp CTAs on 148 SMs at 8
+    per SM), and both paths' words are compared on the way."""
+    cases, spans = sort_by_bucket(cases)
+    rows = []
+    for b, (first, n) in sorted(spans.items()):
+        sub = cases[first: first + n]
+        copies = max(1, -(-target_chunks // n))
+        batch = ChunkBatch(native, packed, sub, device=device, copies=copies)
+        batch.run(abi.COLLISION_BITSET)
+        ref = [batch.words(i) for i in range(n)]
+        batch.out.fill_(-1)
+        batch.run(abi.COLLISION_INT8_TC)
+        if not all(np.array_equal(batch.words(i, copies - 1), ref[i]) for i in range(n)):
+            raise RuntimeError(f"bucket {BUCKETS[b]}: the two paths differ")
+        rows += path_table(batch, {b: (0, n)}, repeats)
+        del batch
     return rows
