@@ -11,7 +11,11 @@ lists: every combination runs its own screened GA against the same plain run
 per seed, and ``by_variant`` holds each one's medians.  ``--features``: the
 surrogate's input, "decode" (per part in decode order its machine, proc time
 and height time, plus per machine its loads) or "order" (per part its
-sequencing key, area and height, parts sorted by key).
+sequencing key, area and height, parts sorted by key).  ``--screen-mode``:
+"family" (every offspring slot's parent pair makes ``--oversample``
+children and the surrogate keeps its best-predicted one) or "pool" (the
+best-predicted rows of the whole oversampled pool; ``--screen-mutants`` and
+``--explore`` apply there).
 
 Both runs use the same instance, GA parameters (elites ceil(0.1 pop), mutants
 ceil(0.15 pop), rho 0.7 as BRKGA_alg3.py:618) and decoder; each generation is
@@ -58,6 +62,8 @@ def main():
     ap.add_argument("--overlap", default="1",
                     help="1: surrogate training beside the decode on a second stream, 0: after it; a comma list "
                          "runs one screened GA per value")
+    ap.add_argument("--screen-mode", default="family",
+                    help="family: the surrogate picks one child per parent pair; pool: the best rows of the pool")
     ap.add_argument("--screen-mutants", type=int, default=0,
                     help="1: the surrogate screens mutants with the offspring; 0: mutants enter unscreened")
     ap.add_argument("--features", default="decode",
@@ -71,11 +77,11 @@ def main():
                 for x in str(args.explore).split(",") for o in str(args.overlap).split(",")
                 for f in str(args.features).split(",")]
     print(json.dumps(time_to_target(args.workload, args.pop, args.generations, args.seeds, args.oversample,
-                                    variants, args.screened_limit, bool(args.screen_mutants))))
+                                    variants, args.screened_limit, bool(args.screen_mutants), args.screen_mode)))
 
 
 def time_to_target(workload, P, generations, seeds, oversample=5, variants=((8, 0.0, 1, "decode"),),
-                   screened_limit=2.0, screen_mutants=False):
+                   screened_limit=2.0, screen_mutants=False, screen_mode="family"):
     """Plain GPU GA for `generations` generations, then each screened variant
     (train_steps, explore, overlap, surrogate features) against its best
     makespan, per seed; the record printed by this script (medians per
@@ -101,7 +107,7 @@ def time_to_target(workload, P, generations, seeds, oversample=5, variants=((8, 
         torch.cuda.empty_cache()
         for ts, ex, ov, ft in variants:
             runs.append(screened_run(generations, screened_limit, oversample, inst, pk, P, ne, nm, seed, ts, ex, ov,
-                                     ft, target, t_plain, p_hit, t_plain_hit, screen_mutants))
+                                     ft, target, t_plain, p_hit, t_plain_hit, screen_mutants, screen_mode))
             torch.cuda.empty_cache()
     by_variant = {}
     for ts, ex, ov, ft in variants:
@@ -116,7 +122,8 @@ def time_to_target(workload, P, generations, seeds, oversample=5, variants=((8, 
     first = by_variant["train_steps={},explore={:g},overlap={},features={}".format(*variants[0])]
     return {"metric": "time to plain-GA best makespan, screened vs plain", "workload": workload,
             "pop": P, "generations": generations, "oversample": oversample,
-            "screened_limit": screened_limit, "screen_mutants": screen_mutants, "train_steps": variants[0][0],
+            "screened_limit": screened_limit, "screen_mode": screen_mode, "screen_mutants": screen_mutants,
+            "train_steps": variants[0][0],
             "explore": variants[0][1], "overlap": variants[0][2], "features": variants[0][3], "seeds": seeds,
             "reached": first["reached"],
             "ratio_median": first["ratio_median"],
@@ -125,7 +132,7 @@ def time_to_target(workload, P, generations, seeds, oversample=5, variants=((8, 
 
 
 def screened_run(generations, screened_limit, oversample, inst, pk, P, ne, nm, seed, train_steps, explore, overlap,
-                 features, target, t_plain, p_hit, t_plain_hit, screen_mutants=False):
+                 features, target, t_plain, p_hit, t_plain_hit, screen_mutants=False, screen_mode="family"):
     """One screened GA against the plain run's target; a dict for the JSON line."""
     from brkga_fft2_b200.ga import DeviceBRKGA
     scr = DeviceBRKGA(None, inst.nb_parts, inst.nb_machines, inst.thresholds, inst.instance_parts,
@@ -133,7 +140,7 @@ def screened_run(generations, screened_limit, oversample, inst, pk, P, ne, nm, s
                       num_individuals=P, num_elites=ne, num_mutants=nm,
                       eliteCProb=0.7, seed=seed, packed=pk, screening=True, oversample=oversample,
                       train_steps=train_steps, explore=explore, overlap_training=bool(overlap), target=target,
-                      surrogate_features=features, screen_mutants=screen_mutants)
+                      surrogate_features=features, screen_mutants=screen_mutants, screen_mode=screen_mode)
     scr.fit()
     mins = np.array(scr.history["min"])
     hit = np.flatnonzero(mins <= target)

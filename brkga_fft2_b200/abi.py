@@ -131,6 +131,9 @@ def load_library(path: str = LIB_PATH):
                                    vp, vp]),
         "brkga_ga_breed_pool": (c_int, [vp, vp, vp, c_i32, c_i32, c_i32, c_i32, c_i32, ctypes.c_float,
                                         ctypes.c_uint64, vp, vp, vp, vp]),
+        "brkga_ga_breed_families": (c_int, [vp, vp, vp, c_i32, c_i32, c_i32, c_i32, c_i32, c_i32, ctypes.c_float,
+                                            ctypes.c_uint64, vp, vp, vp, vp]),
+        "brkga_ga_select_families": (c_int, [vp, c_i32, c_i32, vp, vp]),
         "brkga_ga_gather": (c_int, [vp, vp, c_i32, c_i32, vp, vp]),
         "brkga_ga_screen_stats": (c_int, [vp, vp, vp, vp, c_i32, vp, vp, c_i32, vp, vp]),
         "brkga_ga_track": (c_int, [vp, vp, c_i32, c_i32, vp, vp, c_i32, vp, vp, vp]),

@@ -135,10 +135,15 @@ __global__ void rank_count_kernel(const double* fit, int P, int32_t* order) {
   if (i < P) order[rank] = i;
 }
 
-// One thread per (row, 4-key block) of the new population.
+// One thread per (row, 4-key block) of the new population.  Offspring come
+// in families of `family` consecutive rows that share one parent pair: the
+// pair of family f is drawn from the Philox stream of row ne + nm + f, the
+// stream the plain GA uses for that offspring row, so family = 1 is the plain
+// breed and family k > 1 gives every plain offspring slot k siblings; each
+// child's crossover mask comes from its own row.
 __global__ void breed_kernel(const float* pop, const double* fit, const int32_t* order, int P, int out_rows, int K,
-                             int ne, int nm, float rho, uint32_t k0, uint32_t k1, const long long* generation,
-                             float* next, double* next_fit) {
+                             int ne, int nm, int family, float rho, uint32_t k0, uint32_t k1,
+                             const long long* generation, float* next, double* next_fit) {
   const uint32_t gen = (uint32_t)(*generation);
   const int blocks = (K + 3) >> 2;
   const long long n = (long long)out_rows * blocks;
@@ -155,7 +160,8 @@ __global__ void breed_kernel(const float* pop, const double* fit, const int32_t*
       const uint32_t v[4] = {r.x, r.y, r.z, r.w};
       for (int q = 0; q < nk; ++q) dst[q] = unit_float(v[q]);
     } else {  // offspring of one elite and one non-elite parent
-      const U4 pr = philox(U4{0u, (uint32_t)row, gen, kTagParents}, k0, k1);
+      const int prow = ne + nm + (row - ne - nm) / family;
+      const U4 pr = philox(U4{0u, (uint32_t)prow, gen, kTagParents}, k0, k1);
       const int e = order[(int)mulhi32(pr.x, (uint32_t)ne)];
       const int o = order[ne + (int)mulhi32(pr.y, (uint32_t)(P - ne))];  // non-elites of the parent population
       const U4 r = philox(U4{(uint32_t)b, (uint32_t)row, gen, kTagMask}, k0, k1);
@@ -166,6 +172,18 @@ __global__ void breed_kernel(const float* pop, const double* fit, const int32_t*
       }
     }
   }
+}
+
+// Per family of `family` consecutive candidates, the index of the one with the
+// smallest prediction (ties: the first; NaN never wins over a number).
+__global__ void select_families_kernel(const double* pred, int n_families, int family, int32_t* out) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= n_families) return;
+  const double* p = pred + (size_t)f * family;
+  int best = 0;
+  for (int j = 1; j < family; ++j)
+    if (p[j] < p[best] || (p[best] != p[best] && p[j] == p[j])) best = j;
+  out[f] = f * family + best;
 }
 
 __global__ void gather_rows_kernel(const float* src, const int32_t* idx, int n, int K, float* dst) {
@@ -347,6 +365,10 @@ int brkga_ga_breed_pool(const float* d_pop, const double* d_fitness, const int32
                         int32_t out_rows, int32_t n_keys, int32_t n_elites, int32_t n_mutants, float rho,
                         uint64_t seed, const int64_t* d_generation, float* d_next_pop, double* d_next_fitness,
                         void* stream);
+int brkga_ga_breed_families(const float* d_pop, const double* d_fitness, const int32_t* d_order, int32_t P,
+                            int32_t out_rows, int32_t n_keys, int32_t n_elites, int32_t n_mutants, int32_t family,
+                            float rho, uint64_t seed, const int64_t* d_generation, float* d_next_pop,
+                            double* d_next_fitness, void* stream);
 
 int brkga_ga_init_population(float* d_pop, int32_t P, int32_t n_keys, uint64_t seed, int32_t skip_rows,
                              void* stream) {
@@ -391,13 +413,30 @@ int brkga_ga_breed_pool(const float* d_pop, const double* d_fitness, const int32
                         int32_t out_rows, int32_t n_keys, int32_t n_elites, int32_t n_mutants, float rho,
                         uint64_t seed, const int64_t* d_generation, float* d_next_pop, double* d_next_fitness,
                         void* stream) {
-  if (P < 1 || out_rows < n_elites || n_keys < 1 || n_elites < 1 || n_elites > P || n_mutants < 0 ||
+  return brkga_ga_breed_families(d_pop, d_fitness, d_order, P, out_rows, n_keys, n_elites, n_mutants, 1, rho, seed,
+                                 d_generation, d_next_pop, d_next_fitness, stream);
+}
+
+int brkga_ga_breed_families(const float* d_pop, const double* d_fitness, const int32_t* d_order, int32_t P,
+                            int32_t out_rows, int32_t n_keys, int32_t n_elites, int32_t n_mutants, int32_t family,
+                            float rho, uint64_t seed, const int64_t* d_generation, float* d_next_pop,
+                            double* d_next_fitness, void* stream) {
+  if (P < 1 || out_rows < n_elites || n_keys < 1 || n_elites < 1 || n_elites > P || n_mutants < 0 || family < 1 ||
       n_elites + n_mutants > out_rows || (n_elites + n_mutants < out_rows && n_elites >= P) || !d_pop ||
       !d_fitness || !d_order || !d_generation || !d_next_pop || !d_next_fitness || d_pop == d_next_pop)
     return BRKGA_ERR_INVALID_ARGUMENT;
   breed_kernel<<<grid_for((long long)out_rows * ((n_keys + 3) / 4)), 256, 0, (cudaStream_t)stream>>>(
-      d_pop, d_fitness, d_order, P, out_rows, n_keys, n_elites, n_mutants, rho, (uint32_t)seed,
+      d_pop, d_fitness, d_order, P, out_rows, n_keys, n_elites, n_mutants, family, rho, (uint32_t)seed,
       (uint32_t)(seed >> 32), reinterpret_cast<const long long*>(d_generation), d_next_pop, d_next_fitness);
+  return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
+}
+
+int brkga_ga_select_families(const double* d_pred, int32_t n_families, int32_t family, int32_t* d_index,
+                             void* stream) {
+  if (n_families < 0 || family < 1 || (n_families > 0 && (!d_pred || !d_index))) return BRKGA_ERR_INVALID_ARGUMENT;
+  if (n_families == 0) return BRKGA_OK;
+  select_families_kernel<<<(n_families + 255) / 256, 256, 0, (cudaStream_t)stream>>>(d_pred, n_families, family,
+                                                                                     d_index);
   return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
 }
 

@@ -21,7 +21,15 @@ sequencing key, area and height, the parts sorted by key).  With
 enter unscreened, as in the plain GA, and only the crossover offspring are
 oversampled and ranked (a surrogate ranks random-key mutants low, so
 screening them too removes BRKGA's diversity injection); ``True`` screens
-mutants and offspring together.
+mutants and offspring together.  ``screen_mode="family"`` (the default)
+keeps the plain GA's parents: every offspring slot's (elite, non-elite) pair
+makes ``oversample`` children and the surrogate keeps the best-predicted one,
+the mutants entering unscreened; ``"pool"`` ranks the whole oversampled pool
+and keeps its best-predicted rows (``screen_mutants`` and ``explore`` apply
+there).  Ranking the whole pool picks children that resemble the current
+elites and measurably collapses the population at P100M4 (screened runs
+stalling above the plain GA's best); choosing among siblings does not change
+who breeds with whom.
 
 With ``audit_fraction > 0`` every generation also copies an evenly spaced
 sample of the rows it decoded (that fraction of them), with their exact
@@ -64,7 +72,7 @@ class DeviceBRKGA:
                  spearman_threshold: float = 0.3, check_every: int = 5, warmup_generations: int = 5,
                  buffer_capacity: int = 200_000, target: Optional[float] = None, audit_fraction: float = 0.0,
                  explore: float = 0.0, overlap_training: bool = True, surrogate_features: str = "decode",
-                 screen_mutants: bool = False):
+                 screen_mutants: bool = False, screen_mode: str = "family"):
         import torch
         del collision_backend, eval_mode, eval_workers, eval_chunksize
         self.torch = torch
@@ -93,6 +101,10 @@ class DeviceBRKGA:
                           or int(train_batch) < 1):
             raise ValueError("screening needs oversample >= 1, 0 <= explore <= 1, train_steps >= 0 and "
                              "train_batch >= 1")
+        if screening and screen_mode not in ("family", "pool"):
+            raise ValueError('screen_mode must be "family" or "pool"')
+        if screening and screen_mode == "family" and (screen_mutants or float(explore) > 0):
+            raise ValueError("screen_mutants and explore apply to screen_mode='pool'")
         self.packed = packed if packed is not None else pack_problem(
             problem_data, nbParts, nbMachines, thresholds, instanceParts, threshold_mode)
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
@@ -137,6 +149,7 @@ class DeviceBRKGA:
             # rows that enter every screened generation as they are: the elites
             # and, unless screen_mutants, the mutants; the rest are offspring
             # chosen from an oversampled candidate pool by the surrogate
+            self.screen_mode = screen_mode
             self.screen_mutants = bool(screen_mutants)
             self.n_fixed = self.num_elites + (0 if self.screen_mutants else self.num_mutants)
             n_screen = P - self.n_fixed
@@ -261,20 +274,28 @@ class DeviceBRKGA:
         P, K, ne, nm = self.num_individuals, self.num_gene, self.num_elites, self.num_mutants
         rows, nf = P - ne, self.n_fixed
         self._rank(self.fitness_buf[cur], P, self.order)
+        family = self.oversample if self.screen_mode == "family" else 1
         pool_mutants = nm * self.oversample if self.screen_mutants else nm
-        abi.check(self.lib.brkga_ga_breed_pool(self._ptr(self.pop[cur]), self._ptr(self.fitness_buf[cur]),
-                                               self._ptr(self.order), P, self.pool_rows, K, ne, pool_mutants,
-                                               ctypes.c_float(self.eliteCProb), ctypes.c_uint64(self.seed),
-                                               self._ptr(self.generation), self._ptr(self.pool),
-                                               self._ptr(self.pool_fit), self._stream()), "brkga_ga_breed_pool")
+        abi.check(self.lib.brkga_ga_breed_families(self._ptr(self.pop[cur]), self._ptr(self.fitness_buf[cur]),
+                                                   self._ptr(self.order), P, self.pool_rows, K, ne, pool_mutants,
+                                                   family, ctypes.c_float(self.eliteCProb),
+                                                   ctypes.c_uint64(self.seed), self._ptr(self.generation),
+                                                   self._ptr(self.pool), self._ptr(self.pool_fit), self._stream()),
+                  "brkga_ga_breed_families")
         cand = self.pool_rows - nf
         if P > nf:
             self.surrogate.predict(self.pool[nf:], out=self.pred[:cand])
-            self._rank(self.pred, cand, self.order_pool)
-            order = self.order_pool
-            if self.n_explore:
-                self.torch.index_select(self.order_pool, 0, self.sel_idx, out=self.order_sel)
-                order = self.order_sel
+            if self.screen_mode == "family":  # the best-predicted child of every parent pair
+                abi.check(self.lib.brkga_ga_select_families(self._ptr(self.pred), P - nf, family,
+                                                            self._ptr(self.order_pool), self._stream()),
+                          "brkga_ga_select_families")
+                order = self.order_pool
+            else:  # the best-predicted rows of the whole pool
+                self._rank(self.pred, cand, self.order_pool)
+                order = self.order_pool
+                if self.n_explore:
+                    self.torch.index_select(self.order_pool, 0, self.sel_idx, out=self.order_sel)
+                    order = self.order_sel
             abi.check(self.lib.brkga_ga_gather(self._ptr(self.pool[nf:]), self._ptr(order), P - nf, K,
                                                self._ptr(self.pop[nxt][nf:]), self._stream()), "brkga_ga_gather")
         self.pop[nxt][:nf].copy_(self.pool[:nf])

@@ -309,6 +309,22 @@ int brkga_ga_breed_pool(const float* d_pop, const double* d_fitness, const int32
                         uint64_t seed, const int64_t* d_generation, float* d_next_pop, double* d_next_fitness,
                         void* stream);
 
+/* brkga_ga_breed_pool with offspring in families of `family` consecutive
+ * rows sharing one parent pair: family f's pair is the one the plain breed
+ * draws for offspring row n_elites + n_mutants + f, each child's crossover
+ * mask its own; family = 1 is brkga_ga_breed_pool.  Lets a surrogate choose
+ * among siblings while the parents stay those of the plain GA (no reference
+ * counterpart: BRKGA_alg3.py:188-205 makes one child per pair). */
+int brkga_ga_breed_families(const float* d_pop, const double* d_fitness, const int32_t* d_order, int32_t P,
+                            int32_t out_rows, int32_t n_keys, int32_t n_elites, int32_t n_mutants, int32_t family,
+                            float rho, uint64_t seed, const int64_t* d_generation, float* d_next_pop,
+                            double* d_next_fitness, void* stream);
+
+/* d_index[f] = f * family + the position of the smallest of d_pred[f * family
+ * .. f * family + family - 1] (ties: the first; NaN loses to any number). */
+int brkga_ga_select_families(const double* d_pred, int32_t n_families, int32_t family, int32_t* d_index,
+                             void* stream);
+
 /* d_dst[i, :] = d_src[d_index[i], :] for i < n (rows of n_keys float32). */
 int brkga_ga_gather(const float* d_src, const int32_t* d_index, int32_t n, int32_t n_keys, float* d_dst,
                     void* stream);

@@ -60,17 +60,21 @@ def rank(fit):
     return np.argsort(np.asarray(fit, dtype=np.float64), kind="stable").astype(np.int32)
 
 
-def breed(pop, fit, order, ne, nm, rho, seed, gen):
+def breed(pop, fit, order, ne, nm, rho, seed, gen, out_rows=None, family=1):
+    """Next population (or candidate pool of ``out_rows`` rows): elites,
+    mutants, then offspring in families of ``family`` rows sharing the parent
+    pair that the plain breed draws for row ne + nm + family index."""
     P, K = pop.shape
-    nxt = np.empty_like(pop)
-    nfit = np.zeros(P, np.float64)
+    R = P if out_rows is None else out_rows
+    nxt = np.empty((R, K), pop.dtype)
+    nfit = np.zeros(R, np.float64)
     nxt[:ne] = pop[order[:ne]]
     nfit[:ne] = fit[order[:ne]]
     if nm:
         nxt[ne:ne + nm] = keys_block(np.arange(ne, ne + nm), K, gen, TAG_MUTANT, seed)
-    rows = np.arange(ne + nm, P)
+    rows = np.arange(ne + nm, R)
     if rows.size:
-        pr = philox(0, rows, gen, TAG_PARENTS, seed)
+        pr = philox(0, ne + nm + (rows - ne - nm) // family, gen, TAG_PARENTS, seed)
         e = order[mulhi(pr[0], ne)]
         o = order[ne + mulhi(pr[1], P - ne)]
         u = keys_block(rows, K, gen, TAG_MASK, seed)

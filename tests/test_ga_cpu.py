@@ -53,7 +53,9 @@ def test_small_run_history():
 @pytest.mark.parametrize("kwargs", [dict(num_elites=0), dict(num_elites=5, num_mutants=96), dict(num_individuals=70000),
                                     dict(num_generations=-1), dict(eliteCProb=1.5), dict(audit_fraction=2.0),
                                     dict(screening=True, oversample=0), dict(screening=True, explore=-0.1),
-                                    dict(screening=True, explore=1.5), dict(screening=True, train_batch=0)])
+                                    dict(screening=True, explore=1.5), dict(screening=True, train_batch=0),
+                                    dict(screening=True, screen_mode="rows"),
+                                    dict(screening=True, explore=0.3), dict(screening=True, screen_mutants=True)])
 def test_device_ga_refuses_bad_arguments_before_any_gpu_work(kwargs):
     """Argument errors surface as ValueError on the host, before a decoder or
     any device buffer exists (an oversample below 1 would otherwise gather

@@ -51,6 +51,47 @@ def test_kernels_match_oracle(torch):
     np.testing.assert_array_equal(nfit.cpu().numpy()[:ne], rfit[:ne])
 
 
+def test_family_breed_and_selection_match_oracle(torch):
+    """Offspring in families of 4 siblings per parent pair (the plain breed's
+    pair for that slot), then the best-predicted child of each family."""
+    lib = abi.load_library()
+    P, K, ne, nm, k, seed = 300, 42, 30, 45, 4, 0x2468
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    pop_h = go.init_population(P, K, seed)
+    fit_h = np.round(np.random.default_rng(2).random(P) * 50)
+    pop, fit = torch.from_numpy(pop_h).cuda(), torch.from_numpy(fit_h).cuda()
+    order = torch.from_numpy(go.rank(fit_h).astype(np.int32)).cuda()
+    gen = torch.full((1,), 5, dtype=torch.int64, device="cuda")
+    R = ne + nm + (P - ne - nm) * k
+    pool = torch.zeros(R, K, dtype=torch.float32, device="cuda")
+    pfit = torch.zeros(R, dtype=torch.float64, device="cuda")
+    assert lib.brkga_ga_breed_families(_p(pop), _p(fit), _p(order), P, R, K, ne, nm, k, ctypes.c_float(0.7),
+                                       ctypes.c_uint64(seed), _p(gen), _p(pool), _p(pfit), s) == 0
+    ref, _ = go.breed(pop_h, fit_h, go.rank(fit_h), ne, nm, 0.7, seed, 5, out_rows=R, family=k)
+    np.testing.assert_array_equal(pool.cpu().numpy(), ref)
+    # family = 1 is the plain breed
+    plain, _ = go.breed(pop_h, fit_h, go.rank(fit_h), ne, nm, 0.7, seed, 5)
+    one = torch.zeros(P, K, dtype=torch.float32, device="cuda")
+    assert lib.brkga_ga_breed_families(_p(pop), _p(fit), _p(order), P, P, K, ne, nm, 1, ctypes.c_float(0.7),
+                                       ctypes.c_uint64(seed), _p(gen), _p(one), _p(pfit[:P]), s) == 0
+    np.testing.assert_array_equal(one.cpu().numpy(), plain)
+    nf = P - ne - nm
+    pred_h = np.round(np.random.default_rng(3).random(nf * k) * 9)  # ties inside families
+    pred_h[5] = np.nan
+    pred_h[8:12] = np.nan
+    idx = torch.full((nf,), -1, dtype=torch.int32, device="cuda")
+    assert lib.brkga_ga_select_families(_p(torch.from_numpy(pred_h).cuda()), nf, k, _p(idx), s) == 0
+    want = []
+    for f in range(nf):
+        blk = pred_h[f * k:(f + 1) * k]
+        best = 0
+        for j in range(1, k):
+            if blk[j] < blk[best] or (np.isnan(blk[best]) and not np.isnan(blk[j])):
+                best = j
+        want.append(f * k + best)
+    np.testing.assert_array_equal(idx.cpu().numpy(), want)
+
+
 @pytest.mark.parametrize("P", [8192, 8193, 20000, 65536])
 def test_rank_large_populations(torch, P):
     """Above 8192 rows the rank counts instead of sorting; same order (ties by index, NaN last)."""
@@ -105,8 +146,9 @@ def test_ga_initial_solution_kept(torch):
     assert ga.best_fitness == best
 
 
-@pytest.mark.parametrize("explore,screen_mutants", [(0.0, False), (0.3, False), (0.0, True)])
-def test_screened_ga_reports_exact_makespans(torch, explore, screen_mutants):
+@pytest.mark.parametrize("mode,explore,screen_mutants", [("family", 0.0, False), ("pool", 0.0, False),
+                                                         ("pool", 0.3, False), ("pool", 0.0, True)])
+def test_screened_ga_reports_exact_makespans(torch, mode, explore, screen_mutants):
     """With surrogate screening (mutants unscreened or screened with the
     offspring, and an exploration share of the decoded rows taken from the
     lower-ranked pool) every reported makespan still comes from the exact
@@ -118,7 +160,7 @@ def test_screened_ga_reports_exact_makespans(torch, explore, screen_mutants):
     ga = DeviceBRKGA(None, inst.nb_parts, inst.nb_machines, inst.thresholds, inst.instance_parts,
                      num_generations=20, num_individuals=200, num_elites=20, num_mutants=30, packed=pk, seed=3,
                      screening=True, oversample=4, warmup_generations=4, check_every=2, spearman_threshold=-1.0,
-                     explore=explore, screen_mutants=screen_mutants)
+                     explore=explore, screen_mutants=screen_mutants, screen_mode=mode)
     ga.fit()
     np.testing.assert_array_equal(ga.fitness, oracle_decode(pk, ga.population, n_threads=8))
     assert ga.best_fitness == min(ga.history["min"])
