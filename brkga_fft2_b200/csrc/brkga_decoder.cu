@@ -64,6 +64,16 @@ constexpr int kMaxInst = BRKGA_MAX_INSTANCES;
 constexpr int kMaxCtasPerSm = 32;
 constexpr int kMaxSmemPlates = 8;
 constexpr int kDefaultTaskMax = 8192;
+// Latency launches (the 4-warp shape: few waves of items) end with their
+// longest items, each sharing its SM with seven other CTAs until the queue
+// drains.  The CTA that takes one of the first kCritItems items of the
+// longest-first queue marks its SM, and the other CTAs there take no new
+// item while the mark stands, so that SM empties and the long item gets its
+// issue slots; the other SMs absorb the queue.  Measured at P100M4
+// population 500: 2-4 % faster with 8 or 16 items; on throughput launches
+// (2- and 1-warp shapes) draining SMs costs 2-7 %, so it is off there.
+constexpr int kCritItems = 16;
+constexpr int kCritSlots = 1024;  // per-SM marks, indexed by %smid
 constexpr int kMaxTaskMax = 32 * 256;  // 32 candidates x the output words of the widest plate
 constexpr unsigned long long kKeyNone = ~0ull;
 constexpr unsigned kFull = 0xFFFFFFFFu;
@@ -141,6 +151,8 @@ struct Run {
   int32_t* status;
   unsigned int* item_ctr;
   unsigned int* pool_ctr;
+  int* crit;           // kCritSlots marks: CTAs busy with a critical item, per SM
+  int crit_items;      // items at the head of the queue that mark their SM (0 = off)
   unsigned long long* counters;
   BinScal* binscal;  // Nmax per resident CTA
   uint32_t* pool;
@@ -240,8 +252,9 @@ __device__ __forceinline__ int solo_runs(int n_runs) { return min(n_runs, min(20
 // collision-test order (widest row, then coarse to fine from the bottom)
 // are checked, kVacIlp per step so their loads overlap: a candidate
 // that fails the filter fails within them almost always, and one that slips
-// through is rejected by the exact test.
-constexpr int kVacRows = 32;
+// through is rejected by the exact test (24 rows measured 1 % faster than
+// 32 on the 100- to 400-part workloads, 16 rows up to 3.5 % slower).
+constexpr int kVacRows = 24;
 __device__ __forceinline__ bool vacancy_ok(const uint16_t* vac, int ty, const RotDev& rd,
                                            const uint32_t* vtest) {
   const uint32_t* v = vtest + rd.vt;
@@ -394,6 +407,8 @@ __global__ void assign_sort_kernel(const __grid_constant__ Tables tb, const __gr
   const InstRun& ir = run.r[k];
   const InstDev id = tb.inst[k];
   const int N = id.N, M = id.M, S2 = ir.S2, c = row - ir.crow0;
+  if (row == 0)
+    for (int i = tid; i < kCritSlots; i += nt) run.crit[i] = 0;
   if (row == 0 && tid == 0) {
     *run.item_ctr = 0u;
     *run.pool_ctr = 0u;
@@ -688,9 +703,7 @@ __device__ __forceinline__ unsigned long long search_plate(const Tables& tb, con
     }
   }
   __syncthreads();
-  const unsigned long long key = sh.best;
-  __syncthreads();
-  return key;
+  return sh.best;
 }
 
 // Insert rotation r of part type t (absolute) with its top row at ty and left
@@ -775,17 +788,37 @@ template <int kThreads>
 __global__ void __launch_bounds__(kThreads, kResidentWarps * 32 / kThreads)
     decode_kernel(const Tables tb, const __grid_constant__ Run run) {
   extern __shared__ __align__(16) uint32_t smem[];
-  __shared__ SearchShared sh;
+  // Two search states, used by alternate searches: the state a search returns
+  // from is not written again until the search after next, by which time every
+  // thread has passed the next search's barriers — so a search needs no
+  // barrier after reading its result.
+  __shared__ SearchShared sh2[2];
   __shared__ ItemCtx ctx;
+  int sh_par = 0;
   __shared__ int s_fail, s_pool;
   const int tid = threadIdx.x, lane = tid & 31;
   BinScal* bs = run.binscal + (size_t)blockIdx.x * run.Nmax;
   unsigned long long c_tests = 0, c_chunks = 0, c_bins = 0, c_bytes = 0;
+  unsigned my_sm = 0;
+  asm volatile("mov.u32 %0, %%smid;" : "=r"(my_sm));
+  my_sm &= (unsigned)(kCritSlots - 1);
+  bool crit = false;  // thread 0: this CTA holds a critical item and marked its SM
 
   for (;;) {
     if (tid == 0) {
-      const int q = (int)atomicAdd(run.item_ctr, 1u);
+      if (crit) {
+        atomicSub(&run.crit[my_sm], 1);
+        crit = false;
+      }
       ctx.item = -1;
+      // While another CTA of this SM decodes a critical item, take none: the
+      // CTA that holds the mark keeps pulling, so every item is still taken.
+      const bool leave = run.crit_items > 0 && *(volatile int*)&run.crit[my_sm] > 0;
+      const int q = leave ? run.n_items : (int)atomicAdd(run.item_ctr, 1u);
+      if (q < run.crit_items && q < run.n_items) {
+        crit = true;
+        atomicAdd(&run.crit[my_sm], 1);
+      }
       if (q < run.n_items) {
         const int item = run.order[q];
         const int k = inst_of_item(run, item);
@@ -839,8 +872,9 @@ __global__ void __launch_bounds__(kThreads, kResidentWarps * 32 / kThreads)
         const uint32_t* grid = b < run.S ? smem + (size_t)b * run.slot_words
                                          : run.pool + (size_t)bs[b].pool * run.slot_words;
         const uint16_t* vac = reinterpret_cast<const uint16_t*>(grid + run.slot_vac_off);
-        key = search_plate(tb, md, grid, vac, bs[b].enc, t, run.task_max, run.status, sh, c_tests, c_chunks,
-                           c_bytes);
+        key = search_plate(tb, md, grid, vac, bs[b].enc, t, run.task_max, run.status, sh2[sh_par], c_tests,
+                           c_chunks, c_bytes);
+        sh_par ^= 1;
         if (key != kKeyNone) {
           pb = b;
           break;
@@ -952,8 +986,9 @@ struct GreedyArgs {
 
 __global__ void __launch_bounds__(kGreedyThreads) greedy_kernel(const __grid_constant__ Tables tb,
                                                                 const __grid_constant__ GreedyArgs g) {
-  __shared__ SearchShared sh;
+  __shared__ SearchShared sh2[2];  // alternate searches, as in decode_kernel
   __shared__ int s_fail;
+  int sh_par = 0;
   const int tid = threadIdx.x;
   BinScal* bs = g.binscal;
   unsigned long long c_tests = 0, c_chunks = 0, c_bytes = 0;
@@ -988,7 +1023,8 @@ __global__ void __launch_bounds__(kGreedyThreads) greedy_kernel(const __grid_con
         const uint32_t* grid = g.pool + (size_t)bs[b].pool * g.slot_words;
         const unsigned long long key =
             search_plate(tb, md, grid, reinterpret_cast<const uint16_t*>(grid + g.slot_vac_off), bs[b].enc, t,
-                         kDefaultTaskMax, g.status, sh, c_tests, c_chunks, c_bytes);
+                         kDefaultTaskMax, g.status, sh2[sh_par], c_tests, c_chunks, c_bytes);
+        sh_par ^= 1;
         if (key == kKeyNone) continue;
         const double bpth = bs[b].pth;
         const double cand2 = bpth < pthm ? ((mm - bpth) + pthm) + ptm : mm + ptm;  // :486-489
@@ -1130,7 +1166,7 @@ __global__ void __launch_bounds__(corr::kThreads, 1) chunk_free_i8_kernel(const 
 size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 struct Layout {
-  size_t off_ctr, off_seq, off_cnt, off_inf, off_ord, off_mk, off_bins, off_pool, total;
+  size_t off_ctr, off_crit, off_seq, off_cnt, off_inf, off_ord, off_mk, off_bins, off_pool, total;
 };
 
 // Sizes of one launch: chromosome rows, (chromosome, machine) items, part-order entries.
@@ -1247,6 +1283,8 @@ Layout layout_of(const BrkgaProblem* pb, const LaunchCounts& lc, int64_t pool_bi
   size_t o = 0;
   l.off_ctr = o;
   o += 64;
+  l.off_crit = o = align_up(o, 256);
+  o += (size_t)kCritSlots * sizeof(int);
   l.off_seq = o = align_up(o, 256);
   o += (size_t)lc.seq * sizeof(uint16_t);
   l.off_cnt = o = align_up(o, 256);
@@ -1594,6 +1632,8 @@ int fill_run(const BrkgaProblem* pb, const int32_t* pops, const int64_t* chrom_o
   run->item_ctr = ctr;
   run->pool_ctr = ctr + 1;
   run->counters = reinterpret_cast<unsigned long long*>(ws + l.off_ctr + 8);
+  run->crit = reinterpret_cast<int*>(ws + l.off_crit);
+  run->crit_items = pick_shape(pb, lc.items).warps == 4 ? kCritItems : 0;
   run->binscal = reinterpret_cast<BinScal*>(ws + l.off_bins);
   run->pool = reinterpret_cast<uint32_t*>(ws + l.off_pool);
   run->pool_bins = pool_bins;
