@@ -232,14 +232,23 @@ class DeviceBRKGA:
         if self.overlap_training:
             self.torch.cuda.current_stream(self.device).wait_stream(self._train_stream)
 
-    def _monitor_and_learn(self, nxt):
+    def _monitor_and_learn(self, nxt, screened=False):
         """Surrogate quality on this generation's decoded rows, then learn from them
-        (the training itself ran beside the decode in overlap mode)."""
-        ne, rows = self.num_elites, self.num_individuals - self.num_elites
+        (the training itself ran beside the decode in overlap mode).  In a
+        screened generation the quality is that of the predictions that chose
+        the screened rows (already in pred_sel, nothing is predicted again);
+        otherwise the decoded rows are predicted now."""
+        ne, P = self.num_elites, self.num_individuals
+        if P - ne < 1:
+            return
+        decoded = self.pop[nxt][ne:]
+        first = self.n_fixed if screened else ne
+        rows = P - first
         if rows < 1:
             return
-        decoded, exact = self.pop[nxt][ne:], self.fitness_buf[nxt][ne:]
-        self.surrogate.predict(decoded, out=self.pred_sel[:rows])
+        exact = self.fitness_buf[nxt][first:]
+        if not screened:
+            self.surrogate.predict(decoded, out=self.pred_sel[:rows])
         self._rank(self.pred_sel, rows, self.o_pred)
         self._rank(exact, rows, self.o_exact)
         abi.check(self.lib.brkga_ga_screen_stats(self._ptr(self.pred_sel), self._ptr(exact), self._ptr(self.o_pred),
@@ -247,7 +256,7 @@ class DeviceBRKGA:
                                                  self._ptr(self.stats_dev), self.num_generations + 1,
                                                  self._ptr(self.stat_scratch), self._stream()),
                   "brkga_ga_screen_stats")
-        self.surrogate.observe(decoded, exact)
+        self.surrogate.observe(decoded, self.fitness_buf[nxt][ne:])
         if not self.overlap_training:
             self.surrogate.train(self.train_steps, self.train_batch, self.lr)
 
@@ -298,13 +307,14 @@ class DeviceBRKGA:
                     order = self.order_sel
             abi.check(self.lib.brkga_ga_gather(self._ptr(self.pool[nf:]), self._ptr(order), P - nf, K,
                                                self._ptr(self.pop[nxt][nf:]), self._stream()), "brkga_ga_gather")
+            self.torch.index_select(self.pred[:cand], 0, order[:P - nf], out=self.pred_sel[:P - nf])
         self.pop[nxt][:nf].copy_(self.pool[:nf])
         self.fitness_buf[nxt][:ne].copy_(self.pool_fit[:ne])
         self._train_fork()
         if rows > 0:
             self.decoder.decode(self.pop[nxt][ne:], out=self.fitness_buf[nxt][ne:])
         self._train_join()
-        self._monitor_and_learn(nxt)
+        self._monitor_and_learn(nxt, screened=P > nf)
         self._track(nxt)
 
     def _initial(self):
