@@ -43,7 +43,7 @@ namespace {
 constexpr int kH1 = 512;
 constexpr int kH2 = 256;
 constexpr int kMaxGenes = 8192;
-constexpr int kMaxTrainBatch = 16384;  // rows of one gradient step (the backward kernel keeps dy in shared memory)
+constexpr int kMaxTrainBatch = 16384;  // rows of one gradient step (sizes the backward pass's row-block partials)
 
 struct U4 {
   uint32_t x, y, z, w;
@@ -229,67 +229,114 @@ void col_reduce(const float* A, const float* scale, const float* mask, const flo
 }
 
 // The output layer's backward pass and the loss, from the partial dot
-// products the Z2 GEMM's epilogue left per column tile: y = sum of the
-// partials + b3; dy = 2 (y - t) / n on the n valid rows (MSE), 0 on padding;
-// dZ2 = (Z2 > 0) dy w3 as bf16, row-major and transposed; column sums
-// gw3 = sum_b Z2 dy and gb2 = sum_b dZ2 for 32 columns per CTA (rows split
-// over kColRows thread rows, summed in a fixed order).  CTA 0 also writes y,
-// gb3 = sum_b dy, the loss and, with `bump`, advances the minibatch and Adam
-// step counters (read by the next gather and by this step's Adam).
-__global__ void __launch_bounds__(32 * kColRows) out_backward_kernel(
+// products the Z2 GEMM's epilogue left per column tile, on tiles of 32 rows x
+// 32 columns (grid kH2 / 32 x B / 32, all independent): y = sum of the
+// partials + b3; e = y - t and dy = 2 e / n on the n valid rows (MSE), 0 on
+// padding; dZ2 = (Z2 > 0) dy w3 as bf16, row-major and — through a
+// shared-memory tile, so the stores coalesce — transposed.  Each tile leaves
+// its column sums of Z2 dy (for gw3) and dZ2 (for gb2) over its 32 rows, and
+// the tiles of the first column block the row sums of dy (for gb3) and e^2
+// (the loss); out_grads() adds those row blocks in a fixed order.  Tile (0, 0)
+// also advances the minibatch and Adam step counters when `bump`.
+__global__ void __launch_bounds__(256) out_backward_kernel(
     const float* part, int n_tiles, int ld_part, const float* b3, const float* t, const int* n_valid, const float* Z2,
-    const float* w3, int B, float* y, __nv_bfloat16* dZ, __nv_bfloat16* dZT, float* gw3, float* gb2, float* gb3,
-    float* loss, long long* step, long long* adam_t, int bump) {
-  extern __shared__ float s_dy[];  // [B]
-  __shared__ float pw[kColRows][33], pb[kColRows][33];
-  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx, nt = 32 * kColRows;
+    const float* w3, int B, float* y, __nv_bfloat16* dZ, __nv_bfloat16* dZT, float* pw3, float* pb2, float* pb3,
+    float* ploss, long long* step, long long* adam_t, int bump) {
+  __shared__ float s_dy[32], s_e[32];
+  __shared__ __nv_bfloat16 s_t[32][34];  // [column][row], padded
+  __shared__ float s_w[8][33], s_b[8][33];
+  const int tx = threadIdx.x, ty = threadIdx.y, h = blockIdx.x * 32 + tx, r0 = blockIdx.y * 32;
   const int n = *n_valid;
-  for (int b = tid; b < B; b += nt) {
+  if (ty == 0) {
+    const int b = r0 + tx;
     float v = b3[0];
     for (int q = 0; q < n_tiles; ++q) v += part[(size_t)q * ld_part + b];
-    s_dy[b] = b < n ? 2.f * (v - t[b]) / (float)n : 0.f;
+    const float e = b < n ? v - t[b] : 0.f;
+    s_e[tx] = e;
+    s_dy[tx] = 2.f * e / (float)n;
     if (blockIdx.x == 0) y[b] = v;
   }
   __syncthreads();
-  const int h = blockIdx.x * 32 + tx;
   const float wh = w3[h];
   float aw = 0.f, ab = 0.f;
-  for (int b = ty; b < B; b += kColRows) {
-    const float z = Z2[(size_t)b * kH2 + h], d = s_dy[b];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int rr = ty + 8 * k, b = r0 + rr;
+    const float z = Z2[(size_t)b * kH2 + h], d = s_dy[rr];
     const float g = z > 0.f ? d * wh : 0.f;
     const __nv_bfloat16 q = __float2bfloat16(g);
     dZ[(size_t)b * kH2 + h] = q;
-    dZT[(size_t)h * B + b] = q;
+    s_t[tx][rr] = q;
     aw += z * d;
     ab += g;
   }
-  pw[ty][tx] = aw;
-  pb[ty][tx] = ab;
+  s_w[ty][tx] = aw;
+  s_b[ty][tx] = ab;
   __syncthreads();
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int c = ty + 8 * k;
+    dZT[(size_t)(blockIdx.x * 32 + c) * B + r0 + tx] = s_t[c][tx];
+  }
   if (ty == 0) {
     float sw = 0.f, sb = 0.f;
 #pragma unroll
-    for (int r = 0; r < kColRows; ++r) {
-      sw += pw[r][tx];
-      sb += pb[r][tx];
+    for (int j = 0; j < 8; ++j) {
+      sw += s_w[j][tx];
+      sb += s_b[j][tx];
     }
-    gw3[h] = sw;
-    gb2[h] = sb;
+    pw3[(size_t)blockIdx.y * kH2 + h] = sw;
+    pb2[(size_t)blockIdx.y * kH2 + h] = sb;
+    if (blockIdx.x == 0 && tx == 0) {
+      float sd = 0.f, l = 0.f;
+      for (int j = 0; j < 32; ++j) {
+        sd += s_dy[j];
+        l += s_e[j] * s_e[j];
+      }
+      pb3[blockIdx.y] = sd;
+      ploss[blockIdx.y] = l;
+      if (bump && blockIdx.y == 0) {
+        *step += 1;
+        *adam_t += 1;
+      }
+    }
   }
-  if (blockIdx.x == 0 && tid == 0) {
-    float sd = 0.f, l = 0.f;
-    for (int b = 0; b < B; ++b) {
-      sd += s_dy[b];
-      const float e = 0.5f * s_dy[b] * (float)n;  // y - t on the valid rows
-      l += b < n ? e * e / (float)n : 0.f;
-    }
-    gb3[0] = sd;
-    *loss = l;
-    if (bump) {
-      *step += 1;
-      *adam_t += 1;
-    }
+}
+
+// Where the output layer's row-block partials live and how many there are.
+struct OutPartials {
+  const float *w3, *b2, *b3, *loss;  // [nrb * kH2], [nrb * kH2], [nrb], [nrb]
+  int nrb;
+  const int* n_valid;
+  float* loss_out;
+};
+
+// Gradient of parameter i of the flat vector if it belongs to the output
+// layer's w3, b2 or b3 (row blocks added in order; b3 also writes the loss),
+// else g.  off_b2: first index of b2 (w3 and b3 follow it).
+__device__ __forceinline__ float out_grad(int i, float g, int off_b2, const OutPartials& op) {
+  if (i < off_b2) return g;
+  const int j = i - off_b2;
+  if (j < 2 * kH2) {  // b2 then w3
+    const float* src = j < kH2 ? op.b2 : op.w3;
+    const int h = j < kH2 ? j : j - kH2;
+    float acc = 0.f;
+    for (int r = 0; r < op.nrb; ++r) acc += src[(size_t)r * kH2 + h];
+    return acc;
   }
+  float acc = 0.f, l = 0.f;  // b3
+  for (int r = 0; r < op.nrb; ++r) {
+    acc += op.b3[r];
+    l += op.loss[r];
+  }
+  *op.loss_out = l / (float)*op.n_valid;
+  return acc;
+}
+
+// The output layer's gradients and the loss into the flat gradient vector
+// (the gradients entry point, which runs no Adam).
+__global__ void out_grads_kernel(float* grads, int off_b2, OutPartials op) {
+  for (int j = threadIdx.x; j < 2 * kH2 + 1; j += blockDim.x) grads[off_b2 + j] = out_grad(off_b2 + j, 0.f, off_b2, op);
 }
 
 // Predictions: y = sum of the output layer's partials + b3, in makespan units
@@ -307,14 +354,20 @@ __global__ void predict_out_kernel(const float* part, int n_tiles, int ld_part, 
 // Adam (Kingma & Ba) on every parameter, then the bf16 copies the GEMMs read
 // (W1; W2 row-major and transposed) from the updated values; the step count
 // t is read from device memory so graph replays stay correct.
-__global__ void adam_cast_kernel(float* w, const float* g, float* m, float* v, int n, float lr, float b1, float b2,
+// With `op` set (the training loop), the output layer's gradients are added
+// up from the backward kernel's row-block partials here, and written to g too.
+__global__ void adam_cast_kernel(float* w, float* g, float* m, float* v, int n, float lr, float b1, float b2,
                                  float eps, const long long* t_ptr, int nW1, int offW2, int nW2, __nv_bfloat16* W1b,
-                                 __nv_bfloat16* W2b, __nv_bfloat16* W2Tb) {
+                                 __nv_bfloat16* W2b, __nv_bfloat16* W2Tb, int off_b2, OutPartials op) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const float t = (float)(*t_ptr);
   const float bc1 = 1.f - powf(b1, t), bc2 = 1.f - powf(b2, t);
-  const float gi = g[i];
+  float gi = g[i];
+  if (op.nrb > 0 && i >= off_b2) {
+    gi = out_grad(i, gi, off_b2, op);
+    g[i] = gi;
+  }
   const float mi = b1 * m[i] + (1.f - b1) * gi;
   const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
   m[i] = mi;
@@ -492,6 +545,8 @@ struct BrkgaSurrogate {
   __nv_bfloat16 *X, *XT, *H1b, *H1Tb, *dZ2b, *dZ2Tb, *dZ1Tb;
   float *Z1, *Z2, *y, *t, *dH1, *loss;
   float* part;  // [4, max_batch]: the output layer's partial dot per Z2 column tile
+  int last_nrb = 0;  // row blocks of the last backward pass
+  float* outp;  // row-block partials of the output layer's gradients: w3, b2 [nrb, kH2], b3, loss [nrb]
   int features_kind = BRKGA_SURROGATE_FEATURES_DECODE;
   float inv_area = 1.f;
   int* n_valid;
@@ -584,6 +639,21 @@ int features(BrkgaSurrogate* s, const float* d_chrom, int P, __nv_bfloat16* X, c
   return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
 }
 
+// First index of b2 in the flat parameter vector (w3 and b3 follow it).
+int off_b2(const BrkgaSurrogate* s) { return (int)((long long)kH1 * s->in_pad + kH1 + (long long)kH2 * kH1); }
+
+OutPartials out_partials(const BrkgaSurrogate* s, int nrb) {
+  OutPartials op;
+  op.nrb = nrb;
+  op.w3 = s->outp;
+  op.b2 = s->outp + (size_t)nrb * kH2;
+  op.b3 = s->outp + (size_t)2 * nrb * kH2;
+  op.loss = op.b3 + nrb;
+  op.n_valid = s->n_valid;
+  op.loss_out = s->loss;
+  return op;
+}
+
 // Forward pass on s->X [B, in_pad] (B % 128 == 0), two GEMMs: Z1 = X W1^T
 // with bias + ReLU in its epilogue -> H1 (bf16; with `train` also Z1 fp32 and
 // H1 transposed for the backward pass), Z2 = H1 W2^T with bias + ReLU and the
@@ -633,9 +703,15 @@ int gradients(BrkgaSurrogate* s, int B, int bump, cudaStream_t st) {
   int r, n_tiles = 0;
   const int I = s->in_pad;
   if ((r = forward(s, B, true, &n_tiles, st))) return r;
-  out_backward_kernel<<<kH2 / 32, dim3(32, kColRows), (size_t)B * sizeof(float), st>>>(
-      s->part, n_tiles, s->max_batch, s->b3, s->t, s->n_valid, s->Z2, s->w3, B, s->y, s->dZ2b, s->dZ2Tb, s->gw3,
-      s->gb2, s->gb3, s->loss, s->step, s->adam_t, bump);
+  const int nrb = B / 32;
+  float* pw3 = s->outp;
+  float* pb2 = pw3 + (size_t)nrb * kH2;
+  float* pb3 = pb2 + (size_t)nrb * kH2;
+  out_backward_kernel<<<dim3(kH2 / 32, nrb), dim3(32, 8), 0, st>>>(
+      s->part, n_tiles, s->max_batch, s->b3, s->t, s->n_valid, s->Z2, s->w3, B, s->y, s->dZ2b, s->dZ2Tb, pw3, pb2,
+      pb3, pb3 + nrb, s->step, s->adam_t, bump);
+  s->last_nrb = nrb;
+  if (!bump) out_grads_kernel<<<1, 256, 0, st>>>(s->grads, off_b2(s), out_partials(s, nrb));
   if ((r = gemm(s->dZ2Tb, B, s->H1Tb, B, store_to(s->gW2, kH1), kH2, kH1, B, s->err, st))) return r;
   umma::Epilogue eh;
   eh.kind = umma::kReluMask;
@@ -651,11 +727,15 @@ int gradients(BrkgaSurrogate* s, int B, int bump, cudaStream_t st) {
   return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
 }
 
-int adam_cast(BrkgaSurrogate* s, float lr, cudaStream_t st) {
+// Adam on every parameter; `fused_out`: the output layer's gradients are
+// still row-block partials of the last backward pass (the training loop).
+int adam_cast(BrkgaSurrogate* s, float lr, bool fused_out, cudaStream_t st) {
   const long long nW1 = (long long)kH1 * s->in_pad;
+  OutPartials op = out_partials(s, fused_out ? s->last_nrb : 0);
   adam_cast_kernel<<<grid_for(s->n_params), 256, 0, st>>>(s->params, s->grads, s->mom, s->vel, (int)s->n_params, lr,
                                                           0.9f, 0.999f, 1e-8f, s->adam_t, (int)nW1,
-                                                          (int)(nW1 + kH1), kH2 * kH1, s->W1b, s->W2b, s->W2Tb);
+                                                          (int)(nW1 + kH1), kH2 * kH1, s->W1b, s->W2b, s->W2Tb,
+                                                          off_b2(s), op);
   return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
 }
 
@@ -748,8 +828,6 @@ int brkga_surrogate_create_ex(const BrkgaProblem* problem, int32_t max_batch, in
   }
   if (cudaFuncSetAttribute(features_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxGenes * 8) !=
           cudaSuccess ||
-      cudaFuncSetAttribute(out_backward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           kMaxTrainBatch * (int)sizeof(float)) != cudaSuccess ||
       prepare_gemm() != BRKGA_OK) {
     delete s;
     return BRKGA_ERR_CUDA;
@@ -766,7 +844,8 @@ int brkga_surrogate_create_ex(const BrkgaProblem* problem, int32_t max_batch, in
       (st = dalloc(s, &s->dZ2b, (size_t)B * kH2)) || (st = dalloc(s, &s->dZ2Tb, (size_t)B * kH2)) ||
       (st = dalloc(s, &s->dZ1Tb, (size_t)B * kH1)) || (st = dalloc(s, &s->Z1, (size_t)B * kH1)) ||
       (st = dalloc(s, &s->Z2, (size_t)B * kH2)) || (st = dalloc(s, &s->y, B)) || (st = dalloc(s, &s->t, B)) ||
-      (st = dalloc(s, &s->part, (size_t)4 * B)) || (st = dalloc(s, &s->dH1, (size_t)B * kH1)) || (st = dalloc(s, &s->loss, 1)) ||
+      (st = dalloc(s, &s->part, (size_t)4 * B)) ||
+      (st = dalloc(s, &s->outp, (size_t)(kMaxTrainBatch / 32) * (2 * kH2 + 2))) || (st = dalloc(s, &s->dH1, (size_t)B * kH1)) || (st = dalloc(s, &s->loss, 1)) ||
       (st = dalloc(s, &s->n_valid, 1)) || (st = dalloc(s, &s->slot, B)) || (st = dalloc(s, &s->err, 1)) || (st = dalloc(s, &s->count, 1)) ||
       (st = dalloc(s, &s->step, 1)) || (st = dalloc(s, &s->adam_t, 1)) || (st = dalloc(s, &s->norm, 3)) ||
       (st = dalloc(s, &s->bufX, (size_t)s->cap * I)) || (st = dalloc(s, &s->bufY, s->cap))) {
@@ -860,7 +939,7 @@ int brkga_surrogate_adam(BrkgaSurrogate* s, float lr, void* stream) {
   if (!s) return BRKGA_ERR_INVALID_ARGUMENT;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   bump_kernel<<<1, 1, 0, st>>>(s->adam_t);
-  return adam_cast(s, lr, st);
+  return adam_cast(s, lr, false, st);
 }
 
 int brkga_surrogate_train(BrkgaSurrogate* s, int32_t steps, int32_t batch, float lr, void* stream) {
@@ -876,7 +955,7 @@ int brkga_surrogate_train(BrkgaSurrogate* s, int32_t steps, int32_t batch, float
                                          (uint32_t)s->seed, (uint32_t)(s->seed >> 32), s->step, s->X, s->XT, s->t,
                                          s->n_valid);
     if ((r = gradients(s, batch, 1, st))) return r;
-    if ((r = adam_cast(s, lr, st))) return r;
+    if ((r = adam_cast(s, lr, true, st))) return r;
   }
   return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
 }
