@@ -212,7 +212,9 @@ def roofline_record(prof, kern_s, scan, tests, sm_count, sm_mhz, smem, hbm_peak,
     achieved = ALU-pipe warp instructions of one launch (ncu count of this
     workload, committed in profiles/) over the launch's live CUDA-event time;
     peak = SMs x the ALU pipe's warp instructions per SM cycle (ncu's peak
-    for this pipe) x the SM clock sampled during the timed region.  Beside it:
+    for this pipe) x the SM clock sampled during the timed region.  The
+    profile holds for the decoder sources it was captured from
+    (`profile_matches_build` compares their hash).  Beside it:
     all warp instructions against the 4-per-cycle issue limit of an SM, the
     on-chip scan bytes against the measured shared-memory bandwidth, and the
     DRAM traffic against HBM."""
@@ -247,8 +249,10 @@ def roofline_record(prof, kern_s, scan, tests, sm_count, sm_mhz, smem, hbm_peak,
     if traffic:
         rec["hbm"] = {"achieved": traffic / kern_s / 1e9, "peak": hbm_peak, "frac": traffic / kern_s / 1e9 / hbm_peak,
                       "unit": "GB/s", "peak_source": peak_kind, "dram_bytes_per_launch": traffic}
+    from brkga_fft2_b200.build import decoder_source_id
     rec["profile_build_id"] = prof.get("build_id")
-    rec["profile_matches_build"] = prof.get("build_id") == build_id
+    rec["profile_decoder_source_id"] = prof.get("decoder_source_id")
+    rec["profile_matches_build"] = prof.get("decoder_source_id") == decoder_source_id()
     return rec
 
 

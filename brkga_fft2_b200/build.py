@@ -51,6 +51,23 @@ def build_id() -> str:
     return h.hexdigest()[:16]
 
 
+def decoder_source_id() -> str:
+    """Hash (16 hex digits) of what the decode kernel is compiled from: its
+    source, the headers it includes and the nvcc flags.  A profile of the
+    decode kernel (instruction counts, DRAM bytes) stays valid while this id
+    does, whatever else in the library changes."""
+    h = hashlib.sha256()
+    names = ["brkga_decoder.cu", "corr_i8.cuh", "umma_gemm.cuh"]
+    for path in [os.path.join(PKG, "csrc", n) for n in names] + sorted(glob.glob(os.path.join(REPO, "include", "*.h"))):
+        h.update(os.path.relpath(path, REPO).encode())
+        h.update(b"\0")
+        with open(path, "rb") as f:
+            h.update(f.read())
+        h.update(b"\0")
+    h.update(" ".join(ARCH + FLAGS).encode())
+    return h.hexdigest()[:16]
+
+
 def stamped_id() -> str:
     try:
         with open(STAMP) as f:
