@@ -86,6 +86,21 @@ struct RotDev {
   int imax, dmax;    // row with the longest run of ones and that length
 };
 
+// The rotations of one part type that fit one machine's plate
+// (numba_utils.py:82-84), fixed per (type, machine) and so built once at
+// problem creation: in rotation order and by height (stable; the order of
+// CTAs with fewer than four warps), the smallest height, and the words one
+// read of the plate and of each rotated mask takes (the scan-bytes counter).
+struct RotList {
+  unsigned char nr;
+  unsigned char r[4];   // rotation order
+  unsigned char rs[4];  // by height, ties in rotation order
+  unsigned char pad[3];
+  int hmin;
+  unsigned int scan_words;
+};
+static_assert(sizeof(RotList) == 20, "RotList layout");
+
 struct MachDev {
   int L, W, NW, RS;  // plate rows, columns, words per row, row stride (NW + 2 zero pad words)
   double area;       // MachineData.bin_area
@@ -124,6 +139,7 @@ struct Tables {
   const uint32_t* maskbits;
   const uint8_t* newbin_ok;
   const uint8_t* fits;
+  const RotList* rl;        // [(type, machine)], indexed like fits
 };
 
 // One instance's slice of a launch.
@@ -501,7 +517,8 @@ struct SearchShared {
   unsigned long long best;
   int chunk, total, nr;
   int rlist[4];
-  int rh[4];  // heights of the rotations in rlist
+  int rh[4];      // heights of the rotations in rlist
+  RotDev rd[4];   // their descriptors, read by every chunk
   unsigned char surv[kMaxItemWarps][32];  // per warp: lanes whose candidate passed the vacancy filter
 };
 
@@ -513,42 +530,34 @@ struct SearchShared {
 // all threads of the CTA; contains __syncthreads.
 __device__ __forceinline__ unsigned long long search_plate(const Tables& tb, const MachDev& md,
                                                            const uint32_t* grid, const uint16_t* vac, int enc,
-                                                           int t, int task_max, int32_t* status, SearchShared& sh,
+                                                           int t, const RotList* rlp, int task_max, int32_t* status,
+                                                           SearchShared& sh,
                                                            unsigned long long& c_tests,
                                                            unsigned long long& c_chunks,
                                                            unsigned long long& c_bytes) {
   const int tid = threadIdx.x, lane = tid & 31;
-  if (tid == 0) {
-    int nr = 0, hmin = kMaxSide + 1;
-    const int nrot = tb.nrot[t];
-    for (int r = 0; r < nrot; ++r) {
-      const RotDev rd = tb.rot[t * 4 + r];
-      if (rd.h <= md.L && rd.w <= md.W) {  // numba_utils.py:82-84
-        sh.rh[nr] = rd.h;
-        sh.rlist[nr++] = r;
-        hmin = min(hmin, rd.h);
-        c_bytes += 4ull * ((unsigned long long)md.L * md.NW + (unsigned long long)rd.h * rd.mw);
-      }
-    }
+  if (tid < 4) {  // one thread per rotation: the list was built at problem creation
+    const int nr0 = rlp->nr;
     // With fewer than four warps a level's chunks are taken one after another:
     // the shortest rotation first has the smallest best-case key and prunes
     // the others sooner (measured 4.5 % off the 2-warp P200M6 launch; with
     // four warps every rotation of a level starts at once and the order only
     // cost time).
-    if (blockDim.x < 128)
-      for (int i = 1; i < nr; ++i)
-        for (int j = i; j > 0 && sh.rh[j] < sh.rh[j - 1]; --j) {
-          const int th = sh.rh[j], tr = sh.rlist[j];
-          sh.rh[j] = sh.rh[j - 1];
-          sh.rlist[j] = sh.rlist[j - 1];
-          sh.rh[j - 1] = th;
-          sh.rlist[j - 1] = tr;
-        }
-    sh.nr = nr;
-    sh.total = nr ? nr * ((md.L - hmin + 1 + 31) >> 5) : 0;
-    sh.best = kKeyNone;
-    sh.chunk = 0;
-    c_tests += nr;
+    if (tid < nr0) {
+      const int r = blockDim.x < 128 ? rlp->rs[tid] : rlp->r[tid];
+      const RotDev rd = tb.rot[t * 4 + r];
+      sh.rlist[tid] = r;
+      sh.rh[tid] = rd.h;
+      sh.rd[tid] = rd;
+    }
+    if (tid == 0) {
+      sh.nr = nr0;
+      sh.total = nr0 ? nr0 * ((md.L - rlp->hmin + 1 + 31) >> 5) : 0;
+      sh.best = kKeyNone;
+      sh.chunk = 0;
+      c_tests += nr0;
+      c_bytes += 4ull * rlp->scan_words;
+    }
   }
   __syncthreads();
   const int nr = sh.nr, total = sh.total;
@@ -557,9 +566,10 @@ __device__ __forceinline__ unsigned long long search_plate(const Tables& tb, con
     if (lane == 0) ci = atomicAdd(&sh.chunk, 1);
     ci = __shfl_sync(kFull, ci, 0);
     if (ci >= total) break;
-    const int r = sh.rlist[ci % nr];
-    const int level = ci / nr;
-    const RotDev rd = tb.rot[t * 4 + r];
+    const int level = nr == 4 ? ci >> 2 : nr == 2 ? ci >> 1 : nr == 1 ? ci : ci / 3;
+    const int slot = ci - level * nr;
+    const int r = sh.rlist[slot];
+    const RotDev rd = sh.rd[slot];
     const int ty_hi = md.L - rd.h - 32 * level;
     if (ty_hi < 0) continue;
     unsigned long long cur = 0;
@@ -872,7 +882,9 @@ __global__ void __launch_bounds__(kThreads, kResidentWarps * 32 / kThreads)
         const uint32_t* grid = b < run.S ? smem + (size_t)b * run.slot_words
                                          : run.pool + (size_t)bs[b].pool * run.slot_words;
         const uint16_t* vac = reinterpret_cast<const uint16_t*>(grid + run.slot_vac_off);
-        key = search_plate(tb, md, grid, vac, bs[b].enc, t, run.task_max, run.status, sh2[sh_par], c_tests,
+        key = search_plate(tb, md, grid, vac, bs[b].enc, t,
+                           tb.rl + ctx.tmbase + (size_t)(t - ctx.tbase) * ctx.M + ctx.m, run.task_max, run.status,
+                           sh2[sh_par], c_tests,
                            c_chunks, c_bytes);
         sh_par ^= 1;
         if (key != kKeyNone) {
@@ -1023,7 +1035,8 @@ __global__ void __launch_bounds__(kGreedyThreads) greedy_kernel(const __grid_con
         const uint32_t* grid = g.pool + (size_t)bs[b].pool * g.slot_words;
         const unsigned long long key =
             search_plate(tb, md, grid, reinterpret_cast<const uint16_t*>(grid + g.slot_vac_off), bs[b].enc, t,
-                         kDefaultTaskMax, g.status, sh2[sh_par], c_tests, c_chunks, c_bytes);
+                         tb.rl + (size_t)t * g.M + m, kDefaultTaskMax, g.status, sh2[sh_par], c_tests, c_chunks,
+                         c_bytes);
         sh_par ^= 1;
         if (key == kKeyNone) continue;
         const double bpth = bs[b].pth;
@@ -1222,6 +1235,7 @@ struct BrkgaProblem {
   uint32_t* d_maskbits = nullptr;
   uint8_t* d_fits = nullptr;
   uint8_t* d_newbin_ok = nullptr;
+  RotList* d_rl = nullptr;
   double* d_bin_area = nullptr;
   // brkga_evaluate_host state
   std::mutex mu;
@@ -1496,6 +1510,7 @@ struct Merged {
   std::vector<uint2> truns;
   std::vector<uint32_t> maskbits;
   std::vector<uint8_t> fits, newbin_ok;
+  std::vector<RotList> rl;
   std::vector<MachDev> mach;
 };
 
@@ -1601,6 +1616,29 @@ void merge_instance(const BrkgaProblemDesc* d, Merged& g) {
   }
   g.fits.insert(g.fits.end(), fits.begin(), fits.end());
   g.newbin_ok.insert(g.newbin_ok.end(), newbin_ok.begin(), newbin_ok.end());
+  for (int t = 0; t < T; ++t)
+    for (int m = 0; m < M; ++m) {
+      const MachDev& md = g.mach[id.mbase + m];
+      RotList l{};
+      int rh[4];
+      l.hmin = kMaxSide + 1;
+      for (int r = 0; r < d->part_nrot[t]; ++r) {
+        const int h = d->rot_h[t * 4 + r], w = d->rot_w[t * 4 + r];
+        if (h <= md.L && w <= md.W) {  // numba_utils.py:82-84
+          rh[l.nr] = h;
+          l.r[l.nr] = l.rs[l.nr] = (unsigned char)r;
+          ++l.nr;
+          l.hmin = std::min(l.hmin, h);
+          l.scan_words += (unsigned)(md.L * md.NW + h * ((w + 31) / 32));
+        }
+      }
+      for (int i = 1; i < l.nr; ++i)  // stable insertion sort by height
+        for (int j = i; j > 0 && rh[j] < rh[j - 1]; --j) {
+          std::swap(rh[j], rh[j - 1]);
+          std::swap(l.rs[j], l.rs[j - 1]);
+        }
+      g.rl.push_back(l);
+    }
   for (int m = 0; m + 1 < M; ++m)
     g.thr.push_back(d->threshold_mode == BRKGA_THRESH_F32 ? (double)(float)d->thresholds[m] : d->thresholds[m]);
   for (int j = 0; j < N; ++j) g.gene_type.push_back(id.tbase + d->gene_type[j]);
@@ -1780,6 +1818,7 @@ int brkga_problem_create_multi(const BrkgaProblemDesc* descs, int32_t K, BrkgaPr
       (st = upload(pb, &pb->d_vtest, g.vtest)) || (st = upload(pb, &pb->d_truns, g.truns)) ||
       (st = upload(pb, &pb->d_maskbits, g.maskbits)) ||
       (st = upload(pb, &pb->d_fits, g.fits)) || (st = upload(pb, &pb->d_newbin_ok, g.newbin_ok)) ||
+      (st = upload(pb, &pb->d_rl, g.rl)) ||
       (st = upload(pb, &pb->d_bin_area, g.bin_area)) || (st = configure(pb, 0, 0, -1))) {
     brkga_problem_destroy(pb);
     return st;
@@ -1800,6 +1839,7 @@ int brkga_problem_create_multi(const BrkgaProblemDesc* descs, int32_t K, BrkgaPr
   tb.maskbits = pb->d_maskbits;
   tb.newbin_ok = pb->d_newbin_ok;
   tb.fits = pb->d_fits;
+  tb.rl = pb->d_rl;
   if (cudaGetSymbolAddress(&pb->noalloc_scratch, g_noalloc_scratch) != cudaSuccess) {
     brkga_problem_destroy(pb);
     return BRKGA_ERR_CUDA;
