@@ -8,9 +8,9 @@
 // threads copy the A and B tiles with cp.async (six buffers in dynamic shared
 // memory: four steps of copies in flight, two of MMAs) in the canonical K-major
 // "interleaved" layout (8 x 16-byte core matrices; core (row block, k chunk)
-// at (row_block * 8 + k_chunk) * 128 bytes, so the descriptor's leading byte
-// offset — next k chunk — is 128 B and its stride byte offset — next 8-row
-// block — is 1024 B), one elected thread issues four K=16
+// at (row_block * kChunks + k_chunk) * 128 bytes, so the descriptor's leading
+// byte offset — next k chunk — is 128 B and its stride byte offset — next
+// 8-row block — is 128 x kChunks B, 1024 B for the 64-wide K tile), one elected thread issues four K=16
 // tcgen05.mma.cta_group::1.kind::f16 with the fp32 accumulator in tensor
 // memory (BN columns), and tcgen05.commit signals an mbarrier the CTA waits on.
 // The epilogue reads the accumulator with tcgen05.ld.32x32b (warp w owns
@@ -37,6 +37,7 @@ namespace umma {
 
 constexpr int kTileM = 128;
 constexpr int kTileK = 64;
+constexpr int kChunks = kTileK / 8;  // 16-byte chunks of K per row in one stage
 constexpr long long kSpinLimit = 20000000;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -174,18 +175,20 @@ __global__ void __launch_bounds__(128) gemm_bf16_kernel(const __nv_bfloat16* __r
   const uint32_t tmem = tmem_base;
   constexpr uint32_t idesc = instr_desc_bf16(kTileM, BN);
 
-  // copy a 128 x 64 A tile and a BN x 64 B tile of step kt into stage buf:
-  // chunk (r, c) of 8 bf16 -> core ((r/8)*8 + c), row r%8
+  // copy a 128 x kTileK A tile and a BN x kTileK B tile of step kt into stage
+  // buf: chunk (r, c) of 8 bf16 -> core ((r/8)*kChunks + c), row r%8
   auto stage = [&](int buf, int kt) {
 #pragma unroll
-    for (int j = 0; j < kTileM * 8 / 128; ++j) {
-      const int i = tid + 128 * j, r = i >> 3, c = i & 7;
-      cp_async16(tileA(buf) + ((r >> 3) * 8 + c) * 8 + (r & 7), A + (size_t)(m0 + r) * lda + kt * kTileK + c * 8);
+    for (int j = 0; j < kTileM * kChunks / 128; ++j) {
+      const int i = tid + 128 * j, r = i / kChunks, c = i % kChunks;
+      cp_async16(tileA(buf) + ((r >> 3) * kChunks + c) * 8 + (r & 7),
+                 A + (size_t)(m0 + r) * lda + kt * kTileK + c * 8);
     }
 #pragma unroll
-    for (int j = 0; j < BN * 8 / 128; ++j) {
-      const int i = tid + 128 * j, r = i >> 3, c = i & 7;
-      cp_async16(tileB(buf) + ((r >> 3) * 8 + c) * 8 + (r & 7), B + (size_t)(n0 + r) * ldb + kt * kTileK + c * 8);
+    for (int j = 0; j < BN * kChunks / 128; ++j) {
+      const int i = tid + 128 * j, r = i / kChunks, c = i % kChunks;
+      cp_async16(tileB(buf) + ((r >> 3) * kChunks + c) * 8 + (r & 7),
+                 B + (size_t)(n0 + r) * ldb + kt * kTileK + c * 8);
     }
   };
 
@@ -207,8 +210,8 @@ __global__ void __launch_bounds__(128) gemm_bf16_kernel(const __nv_bfloat16* __r
 #pragma unroll
       for (int s = 0; s < kTileK / 16; ++s) {
         // K = 16 is two 8-wide chunks: chunk 2s at +256*s bytes, the next one +128 B (LBO)
-        const uint64_t ad = smem_desc(a0 + 256u * s, 128u, 1024u);
-        const uint64_t bd = smem_desc(b0 + 256u * s, 128u, 1024u);
+        const uint64_t ad = smem_desc(a0 + 256u * s, 128u, 128u * kChunks);
+        const uint64_t bd = smem_desc(b0 + 256u * s, 128u, 128u * kChunks);
         mma_bf16(tmem, ad, bd, idesc, (kt > 0 || s > 0) ? 1u : 0u);
       }
       commit_to(&bar[buf]);
