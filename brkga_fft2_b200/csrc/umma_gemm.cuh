@@ -176,19 +176,20 @@ __global__ void __launch_bounds__(128) gemm_bf16_kernel(const __nv_bfloat16* __r
   constexpr uint32_t idesc = instr_desc_bf16(kTileM, BN);
 
   // copy a 128 x kTileK A tile and a BN x kTileK B tile of step kt into stage
-  // buf: chunk (r, c) of 8 bf16 -> core ((r/8)*kChunks + c), row r%8
+  // buf: chunk (r, c) of 8 bf16 -> core ((r/8)*kChunks + c), row r%8.  Eight
+  // consecutive lanes fill the 8 rows of one core matrix (128 contiguous
+  // bytes: no bank conflict), the next eight the next chunk of the same rows,
+  // so a warp reads 64 contiguous bytes of each of 8 rows (whole sectors).
   auto stage = [&](int buf, int kt) {
 #pragma unroll
     for (int j = 0; j < kTileM * kChunks / 128; ++j) {
-      const int i = tid + 128 * j, r = i / kChunks, c = i % kChunks;
-      cp_async16(tileA(buf) + ((r >> 3) * kChunks + c) * 8 + (r & 7),
-                 A + (size_t)(m0 + r) * lda + kt * kTileK + c * 8);
+      const int i = tid + 128 * j, ri = i & 7, c = (i >> 3) % kChunks, r = ((i >> 3) / kChunks) * 8 + ri;
+      cp_async16(tileA(buf) + ((r >> 3) * kChunks + c) * 8 + ri, A + (size_t)(m0 + r) * lda + kt * kTileK + c * 8);
     }
 #pragma unroll
     for (int j = 0; j < BN * kChunks / 128; ++j) {
-      const int i = tid + 128 * j, r = i / kChunks, c = i % kChunks;
-      cp_async16(tileB(buf) + ((r >> 3) * kChunks + c) * 8 + (r & 7),
-                 B + (size_t)(n0 + r) * ldb + kt * kTileK + c * 8);
+      const int i = tid + 128 * j, ri = i & 7, c = (i >> 3) % kChunks, r = ((i >> 3) / kChunks) * 8 + ri;
+      cp_async16(tileB(buf) + ((r >> 3) * kChunks + c) * 8 + ri, B + (size_t)(n0 + r) * ldb + kt * kTileK + c * 8);
     }
   };
 
