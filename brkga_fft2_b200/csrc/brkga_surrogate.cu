@@ -28,6 +28,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "../../include/brkga_b200.h"
@@ -450,22 +451,45 @@ __global__ void set_norm_kernel(const double* ms, int P, double* norm) {
   }
 }
 
-// Ring-buffer slots of the feasible rows, in row order (one CTA; deterministic).
-__global__ void observe_slots_kernel(const double* ms, int P, const double* norm, long long* count, int cap,
-                                     int* slot) {
-  if (threadIdx.x != 0) return;
-  long long c = *count;
+// Ring-buffer slots of the feasible rows, in row order: one CTA of 1024
+// threads takes 1024 rows per pass and numbers the feasible ones by a prefix
+// count (ballots within a warp, then a scan of the 32 warp totals), so the
+// slots are those of a walk over the rows in order.
+constexpr int kObsThreads = 1024;
+__global__ void __launch_bounds__(kObsThreads) observe_slots_kernel(const double* ms, int P, const double* norm,
+                                                                    long long* count, int cap, int* slot) {
+  __shared__ int warp_sum[kObsThreads / 32];
+  __shared__ long long base;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  if (tid == 0) base = *count;
   const bool ready = norm[2] != 0.0;
-  for (int r = 0; r < P; ++r) {
-    const double v = ms[r];
-    if (ready && v < 1e15 && v == v) {
-      slot[r] = (int)(c % cap);
-      ++c;
-    } else {
-      slot[r] = -1;
+  __syncthreads();
+  for (int r0 = 0; r0 < P; r0 += kObsThreads) {
+    const int r = r0 + tid;
+    bool ok = false;
+    if (r < P) {
+      const double v = ms[r];
+      ok = ready && v < 1e15 && v == v;
     }
+    const unsigned bal = __ballot_sync(0xFFFFFFFFu, ok);
+    if (lane == 0) warp_sum[wid] = __popc(bal);
+    __syncthreads();
+    if (wid == 0) {  // inclusive scan of the warp totals
+      int v = warp_sum[lane];
+      for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xFFFFFFFFu, v, o);
+        if (lane >= o) v += u;
+      }
+      warp_sum[lane] = v;
+    }
+    __syncthreads();
+    const long long idx = base + (wid ? warp_sum[wid - 1] : 0) + __popc(bal & ((1u << lane) - 1u));
+    if (r < P) slot[r] = ok ? (int)(idx % cap) : -1;
+    __syncthreads();
+    if (tid == 0) base += warp_sum[kObsThreads / 32 - 1];
+    __syncthreads();
   }
-  *count = c;
+  if (tid == 0) *count = base;
 }
 
 // Append feasible rows (features + standardised target) to their slots.
@@ -591,15 +615,53 @@ int prepare_gemm() {
 // (these GEMMs are small: more CTAs matter more than tile reuse).
 int tile_n(int M, int N) { return (N % 128 == 0 && (long long)(M / 128) * (N / 128) >= 2 * 148) ? 128 : 64; }
 
+// cuTensorMapEncodeTiled from the driver, looked up once per process through
+// the runtime (no link against libcuda).
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  });
+  return fn;
+}
+
+// Tensor map of a bf16 [rows, K] K-major operand with row stride ld
+// elements: boxes of 64 K elements (128 bytes) x box_rows rows, 128-byte
+// swizzle.  The base must be 16-byte aligned and ld a multiple of 8.
+int tile_map(CUtensorMap* map, const __nv_bfloat16* ptr, int rows, int K, int ld, int box_rows) {
+  EncodeTiledFn enc = encode_tiled();
+  if (!enc) return BRKGA_ERR_CUDA;
+  if (reinterpret_cast<uintptr_t>(ptr) % 16 || ld % 8) return BRKGA_ERR_INVALID_ARGUMENT;
+  const cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+  const cuuint32_t box[2] = {(cuuint32_t)umma::kTileK, (cuuint32_t)box_rows};
+  const cuuint32_t elem[2] = {1, 1};
+  const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16*>(ptr), dims, strides,
+                         box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? BRKGA_OK : BRKGA_ERR_INVALID_ARGUMENT;
+}
+
 int gemm(const __nv_bfloat16* A, int lda, const __nv_bfloat16* B, int ldb, const umma::Epilogue& ep, int M, int N,
          int K, int* err, cudaStream_t st) {
   if (M % 128 || K % 64 || N % 64) return BRKGA_ERR_INVALID_ARGUMENT;
-  if (tile_n(M, N) == 128) {
-    umma::gemm_bf16_kernel<128><<<dim3(M / 128, N / 128), 128, umma::gemm_smem_bytes<128>(), st>>>(A, lda, B, ldb,
-                                                                                                  ep, K, err);
+  const int bn = tile_n(M, N);
+  CUtensorMap ta, tb;
+  int r;
+  if ((r = tile_map(&ta, A, M, K, lda, umma::kTileM)) || (r = tile_map(&tb, B, N, K, ldb, bn))) return r;
+  if (bn == 128) {
+    umma::gemm_bf16_kernel<128><<<dim3(M / 128, N / 128), 128, umma::gemm_smem_bytes<128>(), st>>>(ta, tb, ep, K,
+                                                                                                  err);
   } else {
-    umma::gemm_bf16_kernel<64><<<dim3(M / 128, N / 64), 128, umma::gemm_smem_bytes<64>(), st>>>(A, lda, B, ldb, ep,
-                                                                                               K, err);
+    umma::gemm_bf16_kernel<64><<<dim3(M / 128, N / 64), 128, umma::gemm_smem_bytes<64>(), st>>>(ta, tb, ep, K, err);
   }
   return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
 }
@@ -922,7 +984,7 @@ int brkga_surrogate_observe(BrkgaSurrogate* s, const float* d_chrom, const doubl
     op.bufY = s->bufY;
     op.cap = s->cap;
     op.norm = s->norm;
-    observe_slots_kernel<<<1, 32, 0, st>>>(op.makespan, n, s->norm, s->count, s->cap, s->slot);
+    observe_slots_kernel<<<1, kObsThreads, 0, st>>>(op.makespan, n, s->norm, s->count, s->cap, s->slot);
     observe_kernel<<<n, 128, 0, st>>>(op, s->slot);
   }
   return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
@@ -986,7 +1048,9 @@ int brkga_surrogate_features(BrkgaSurrogate* s, const float* d_chrom, int32_t P,
 // checkpoints): 0 = parameters (fp32, flat), 1 = gradients, 2 = activations X
 // (bf16 [max_batch, in_pad]), 3 = predictions y (fp32 [max_batch]), 4 = loss
 // (fp32 [1]), 5 = target standardisation (float64 mean, std, set flag),
-// 6 = Adam moments m and v (fp32, 2 x parameters), 7 = Adam step (int64).
+// 6 = Adam moments m and v (fp32, 2 x parameters), 7 = Adam step (int64),
+// 8 = the example ring's standardised targets (fp32 [capacity]), 9 = examples
+// observed so far (int64).
 int brkga_surrogate_io(BrkgaSurrogate* s, int32_t what, void* host, int64_t bytes, int32_t to_device) {
   if (!s || !host || bytes < 0) return BRKGA_ERR_INVALID_ARGUMENT;
   void* dev = nullptr;
@@ -1000,6 +1064,8 @@ int brkga_surrogate_io(BrkgaSurrogate* s, int32_t what, void* host, int64_t byte
     case 5: dev = s->norm; size = 24; break;
     case 6: dev = s->mom; size = s->n_params * 8; break;  // mom and vel are separate allocations
     case 7: dev = s->adam_t; size = 8; break;
+    case 8: dev = s->bufY; size = (int64_t)s->cap * 4; break;
+    case 9: dev = s->count; size = 8; break;
     default: return BRKGA_ERR_INVALID_ARGUMENT;
   }
   if (bytes > size) return BRKGA_ERR_INVALID_ARGUMENT;

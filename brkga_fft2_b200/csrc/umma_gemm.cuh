@@ -4,17 +4,17 @@
 //   A: bf16 [M, K] K-major (row-major, lda), B: bf16 [N, K] K-major (ldb).
 //   M % 128 == 0, N % BN == 0 (BN = 64 or 128), K % 64 == 0 (callers pad with zeros).
 //
-// One CTA of 128 threads per 128 x BN output tile.  Per 64-wide K step the
-// threads copy the A and B tiles with cp.async (six buffers in dynamic shared
-// memory: four steps of copies in flight, two of MMAs) in the canonical K-major
-// "interleaved" layout (8 x 16-byte core matrices; core (row block, k chunk)
-// at (row_block * kChunks + k_chunk) * 128 bytes, so the descriptor's leading
-// byte offset — next k chunk — is 128 B and its stride byte offset — next
-// 8-row block — is 128 x kChunks B, 1024 B for the 64-wide K tile), one elected thread issues four K=16
-// tcgen05.mma.cta_group::1.kind::f16 with the fp32 accumulator in tensor
-// memory (BN columns), and tcgen05.commit signals an mbarrier the CTA waits on.
-// The epilogue reads the accumulator with tcgen05.ld.32x32b (warp w owns
-// lanes 32w..32w+31 = output rows) and stores fp32.
+// One CTA of 128 threads per 128 x BN output tile.  Per 64-wide K step one
+// thread loads the A and B tiles with TMA (cp.async.bulk.tensor, tensor maps
+// built on the host, 128-byte swizzle: rows of 64 bf16, the layout the MMA's
+// K-major SWIZZLE_128B descriptor reads) into a ring of stages in dynamic
+// shared memory, counted on one mbarrier per stage; a second thread issues
+// four K = 16 tcgen05.mma.cta_group::1.kind::f16 per step with the fp32
+// accumulator in tensor memory (BN columns) and frees the stage with
+// tcgen05.commit.  All copies of a small GEMM are in flight at once; the
+// tensor core never waits for a CTA-wide barrier.  The epilogue reads the
+// accumulator with tcgen05.ld.32x32b (warp w owns lanes 32w..32w+31 = output
+// rows).
 //
 // The epilogue (Epilogue below) either stores the fp32 tile, or applies the
 // surrogate's elementwise step in registers before anything leaves the SM:
@@ -26,9 +26,10 @@
 //
 // Every wait is bounded: after kSpinLimit polls the kernel records
 // BRKGA_ERR_CUDA in *err, skips its epilogue, frees its tensor memory and
-// returns.  No TMA and no multicast are used.
+// returns, after waiting (bounded) for the copies it issued.  No multicast.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -37,14 +38,14 @@ namespace umma {
 
 constexpr int kTileM = 128;
 constexpr int kTileK = 64;
-constexpr int kChunks = kTileK / 8;  // 16-byte chunks of K per row in one stage
 constexpr long long kSpinLimit = 20000000;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
-// Shared-memory matrix descriptor, SWIZZLE_NONE, K-major.
+// Shared-memory matrix descriptor, SWIZZLE_NONE, K-major (core matrices of
+// 8 rows x 16 bytes; used by the INT8 correlation kernel).
 __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo_bytes, uint32_t sbo_bytes) {
   uint64_t d = 0;
   d |= (uint64_t)((addr >> 4) & 0x3FFFu);
@@ -52,6 +53,20 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo_bytes,
   d |= (uint64_t)((sbo_bytes >> 4) & 0x3FFFu) << 32;
   d |= (uint64_t)1 << 46;  // descriptor version for sm_100
   return d;                // base offset 0, legacy LBO mode, layout type 0 (no swizzle)
+}
+
+// Shared-memory matrix descriptor, K-major with the 128-byte swizzle that
+// the TMA copies write: rows of 128 bytes (64 bf16), 8-row groups 1024 bytes
+// apart (stride byte offset); the leading byte offset is unused for this
+// layout.  A K = 16 slice of the row starts 32 bytes further.
+__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr >> 4) & 0x3FFFu);
+  d |= (uint64_t)1 << 16;              // leading byte offset (16 B, ignored)
+  d |= (uint64_t)(1024u >> 4) << 32;   // stride byte offset
+  d |= (uint64_t)1 << 46;              // descriptor version for sm_100
+  d |= (uint64_t)2 << 61;              // layout: 128-byte swizzle
+  return d;
 }
 
 // Instruction descriptor: D fp32, A and B bf16, both K-major, M x N.
@@ -92,22 +107,39 @@ __device__ __forceinline__ bool wait_parity(uint64_t* bar, uint32_t parity) {
   return false;
 }
 
-constexpr int kStages = 6;  // shared-memory buffers
-constexpr int kAhead = 4;   // K steps of copies in flight; the MMAs of kStages - kAhead steps may still run
-
-// Dynamic shared memory of gemm_bf16_kernel<BN>: kStages stages of A and B tiles.
+// Stages of A and B tiles in shared memory (24 KB per stage at BN = 64,
+// 32 KB at BN = 128): enough that the copies of every K step of the
+// surrogate's GEMMs (K <= 640) are in flight at once.
 template <int BN>
-constexpr int gemm_smem_bytes() {
-  return kStages * (kTileM * kTileK + BN * kTileK) * 2;
+__host__ __device__ constexpr int gemm_stages() {
+  return BN == 128 ? 5 : 6;
 }
 
-__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem_dst)), "l"(gmem_src) : "memory");
+// Dynamic shared memory of gemm_bf16_kernel<BN>: the stages plus 1 KB to
+// align them on the swizzle's 1024-byte period.
+template <int BN>
+__host__ __device__ constexpr int gemm_smem_bytes() {
+  return gemm_stages<BN>() * (kTileM * kTileK + BN * kTileK) * 2 + 1024;
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+// One arrival that also announces `bytes` of asynchronous copies to come.
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+// TMA tile load (no multicast): box at (x = K element, y = row) of the
+// tensor map into shared memory, completion counted on `bar`.  x is a
+// multiple of 64 elements (128 bytes), so every copy starts 16-byte aligned.
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
 }
 
 // What the epilogue does with an output tile (see the file comment).
@@ -133,29 +165,36 @@ struct Epilogue {
   int ld_part = 0;
 };
 
-// Pipeline: the threads keep kAhead K steps of tiles in flight as
-// asynchronous copies (cp.async, straight into shared memory) while one
-// thread issues the MMAs of the oldest complete step; a buffer is refilled
-// only after the MMAs that read it (kStages - kAhead steps earlier) have
-// signalled their mbarrier, so the MMAs of the last steps keep running.
+// Pipeline (warp-specialised, one CTA of 128 threads per 128 x BN tile):
+//   thread 0   (producer) loads the A and B tiles of each 64-wide K step with
+//              two TMA copies (cp.async.bulk.tensor.2d, 128-byte swizzle)
+//              into stage kt % kSt; the stage's "full" mbarrier counts the
+//              bytes (expect_tx), and a stage is refilled only after its
+//              "empty" mbarrier reports that the MMAs reading it are done;
+//   thread 32  (MMA issuer) waits for "full", issues the step's four K = 16
+//              tcgen05.mma and commits them to the stage's "empty" barrier;
+//              after the last step one more commit signals "acc";
+//   all warps  wait for "acc" and run the epilogue from tensor memory.
+// No multicast; every wait is bounded (the error path is in the kernel).
 template <int BN>
-__global__ void __launch_bounds__(128) gemm_bf16_kernel(const __nv_bfloat16* __restrict__ A, int lda,
-                                                        const __nv_bfloat16* __restrict__ B, int ldb,
+__global__ void __launch_bounds__(128) gemm_bf16_kernel(const __grid_constant__ CUtensorMap tmA,
+                                                        const __grid_constant__ CUtensorMap tmB,
                                                         const __grid_constant__ Epilogue ep, int K, int* err) {
   static_assert(BN == 64 || BN == 128, "BN must be 64 or 128");
-  constexpr int kCols = BN;                    // tensor-memory columns (power of two >= 32)
-  constexpr int kAWords = kTileM * kTileK / 8;  // uint4 per A stage
-  constexpr int kBWords = BN * kTileK / 8;
-  extern __shared__ __align__(1024) uint4 smem_tiles[];
-  __shared__ __align__(8) uint64_t bar[kStages];
+  constexpr int kSt = gemm_stages<BN>();
+  constexpr int kCols = BN;  // tensor-memory columns (power of two >= 32)
+  constexpr uint32_t kABytes = kTileM * kTileK * 2, kBBytes = BN * kTileK * 2, kStageBytes = kABytes + kBBytes;
+  extern __shared__ uint8_t smem_raw[];
+  __shared__ __align__(8) uint64_t full[kSt];
+  __shared__ __align__(8) uint64_t empty[kSt];
+  __shared__ __align__(8) uint64_t accb;
   __shared__ uint32_t tmem_base;
-  __shared__ int s_fail;
+  __shared__ int s_fail, s_issued, s_consumed;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int m0 = blockIdx.x * kTileM, n0 = blockIdx.y * BN;
-  // stage b: A tile at b * (kAWords + kBWords), B tile right after it
-  auto tileA = [&](int b) { return smem_tiles + b * (kAWords + kBWords); };
-  auto tileB = [&](int b) { return smem_tiles + b * (kAWords + kBWords) + kAWords; };
+  // the 128-byte swizzle repeats every 1024 bytes: stages start on that boundary
+  const uint32_t base = (smem_u32(smem_raw) + 1023u) & ~1023u;
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
@@ -163,85 +202,67 @@ __global__ void __launch_bounds__(128) gemm_bf16_kernel(const __nv_bfloat16* __r
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
-  if (tid == 0) {
+  if (tid == 32) {
     s_fail = 0;
-    for (int b = 0; b < kStages; ++b)
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar[b])) : "memory");
+    s_issued = 0;
+    s_consumed = 0;
+    for (int b = 0; b < kSt; ++b) {
+      mbar_init(&full[b], 1);
+      mbar_init(&empty[b], 1);
+    }
+    mbar_init(&accb, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (tid == 64) {
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmA)) : "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmB)) : "memory");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_base;
   constexpr uint32_t idesc = instr_desc_bf16(kTileM, BN);
-
-  // copy a 128 x kTileK A tile and a BN x kTileK B tile of step kt into stage
-  // buf: chunk (r, c) of 8 bf16 -> core ((r/8)*kChunks + c), row r%8.  Eight
-  // consecutive lanes fill the 8 rows of one core matrix (128 contiguous
-  // bytes: no bank conflict), the next eight the next chunk of the same rows,
-  // so a warp reads 64 contiguous bytes of each of 8 rows (whole sectors).
-  auto stage = [&](int buf, int kt) {
-#pragma unroll
-    for (int j = 0; j < kTileM * kChunks / 128; ++j) {
-      const int i = tid + 128 * j, ri = i & 7, c = (i >> 3) % kChunks, r = ((i >> 3) / kChunks) * 8 + ri;
-      cp_async16(tileA(buf) + ((r >> 3) * kChunks + c) * 8 + ri, A + (size_t)(m0 + r) * lda + kt * kTileK + c * 8);
-    }
-#pragma unroll
-    for (int j = 0; j < BN * kChunks / 128; ++j) {
-      const int i = tid + 128 * j, ri = i & 7, c = (i >> 3) % kChunks, r = ((i >> 3) / kChunks) * 8 + ri;
-      cp_async16(tileB(buf) + ((r >> 3) * kChunks + c) * 8 + ri, B + (size_t)(n0 + r) * ldb + kt * kTileK + c * 8);
-    }
-  };
-
   const int ksteps = K / kTileK;
-#pragma unroll
-  for (int p = 0; p < kAhead; ++p) {
-    if (p < ksteps) stage(p, p);
-    cp_async_commit();  // one group per step, empty ones included, so the group count stays uniform
-  }
-  int last = -1;  // last k step whose MMAs were committed
-  for (int kt = 0; kt < ksteps; ++kt) {
-    const int buf = kt % kStages;
-    cp_async_wait<kAhead - 1>();  // this thread's copies of step kt have landed
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncthreads();
-    if (tid == 0) {
+
+  if (tid == 0) {  // producer
+    int kt = 0;
+    for (; kt < ksteps; ++kt) {
+      const int b = kt % kSt;
+      if (kt >= kSt && !wait_parity(&empty[b], (uint32_t)((kt / kSt - 1) & 1))) {
+        atomicExch(&s_fail, 1);
+        break;
+      }
+      if (*(volatile int*)&s_fail) break;
+      const uint32_t a_dst = base + (uint32_t)b * kStageBytes;
+      mbar_expect_tx(&full[b], kStageBytes);
+      tma_load_2d(a_dst, &tmA, kt * kTileK, m0, &full[b]);
+      tma_load_2d(a_dst + kABytes, &tmB, kt * kTileK, n0, &full[b]);
+    }
+    s_issued = kt;
+  } else if (tid == 32) {  // MMA issuer
+    int kt = 0;
+    for (; kt < ksteps; ++kt) {
+      const int b = kt % kSt;
+      if (!wait_parity(&full[b], (uint32_t)((kt / kSt) & 1))) {
+        atomicExch(&s_fail, 1);
+        break;
+      }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint32_t a0 = smem_u32(tileA(buf)), b0 = smem_u32(tileB(buf));
+      const uint32_t a0 = base + (uint32_t)b * kStageBytes, b0 = a0 + kABytes;
 #pragma unroll
-      for (int s = 0; s < kTileK / 16; ++s) {
-        // K = 16 is two 8-wide chunks: chunk 2s at +256*s bytes, the next one +128 B (LBO)
-        const uint64_t ad = smem_desc(a0 + 256u * s, 128u, 128u * kChunks);
-        const uint64_t bd = smem_desc(b0 + 256u * s, 128u, 128u * kChunks);
-        mma_bf16(tmem, ad, bd, idesc, (kt > 0 || s > 0) ? 1u : 0u);
-      }
-      commit_to(&bar[buf]);
+      for (int s = 0; s < kTileK / 16; ++s)  // K = 16 is 32 bytes along the swizzled 128-byte row
+        mma_bf16(tmem, smem_desc_sw128(a0 + 32u * s), smem_desc_sw128(b0 + 32u * s), idesc,
+                 (kt > 0 || s > 0) ? 1u : 0u);
+      commit_to(&empty[b]);
     }
-    last = kt;
-    const int nk = kt + kAhead;  // the step to prefetch, into the buffer of step kt - (kStages - kAhead)
-    constexpr int kLag = kStages - kAhead;
-    if (nk < ksteps) {
-      if (kt >= kLag) {
-        const int pb = (kt - kLag) % kStages;
-        if (!wait_parity(&bar[pb], (uint32_t)(((kt - kLag) / kStages) & 1))) {
-          if (lane == 0) atomicExch(&s_fail, 1);
-        }
-        __syncthreads();
-        if (s_fail) break;
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      }
-      stage(nk % kStages, nk);
-    }
-    cp_async_commit();
+    s_consumed = kt;
+    commit_to(&accb);  // tracks every MMA this thread issued, whether the loop finished or not
   }
-  // the MMAs of one thread complete in order: the last commit covers them all
-  if (!s_fail && last >= 0) {
-    if (!wait_parity(&bar[last % kStages], (uint32_t)((last / kStages) & 1))) {
-      if (lane == 0) atomicExch(&s_fail, 1);
-    }
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    __syncthreads();
-  }
+  __syncwarp();
+  const bool acc_ok = wait_parity(&accb, 0u);
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (!acc_ok && lane == 0) atomicExch(&s_fail, 1);
+  __syncthreads();
 
   if (!s_fail) {
     const int row = m0 + warp * 32 + lane;
@@ -308,10 +329,10 @@ __global__ void __launch_bounds__(128) gemm_bf16_kernel(const __nv_bfloat16* __r
     if (ep.dotw) ep.part[(size_t)blockIdx.y * ep.ld_part + row] = dot;
   } else if (tid == 0) {
     atomicExch(err, 3 /* BRKGA_ERR_CUDA */);
-    // let the MMAs still in flight finish before the tensor memory is released
-    if (last >= 0) wait_parity(&bar[last % kStages], (uint32_t)((last / kStages) & 1));
+    // no copy may land after the CTA is gone: wait (bounded) for every stage
+    // the producer issued and the MMA thread did not consume
+    for (int kt = s_consumed; kt < s_issued; ++kt) wait_parity(&full[kt % kSt], (uint32_t)((kt / kSt) & 1));
   }
-  asm volatile("cp.async.wait_all;" ::: "memory");  // no copy may land after the CTA is gone
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0) {

@@ -357,8 +357,9 @@ int brkga_ga_track(const double* d_fitness, const float* d_pop, int32_t P, int32
 /* ---- bf16 GEMM on the tensor cores (tcgen05) ----
  * C[M,N] fp32 (row-major, ldc) = sum_k A[m,k] B[n,k]; A [M,K] and B [N,K]
  * bf16 row-major (K contiguous).  M % 128 == 0, N % 64 == 0, K % 64 == 0;
- * *d_err is set to BRKGA_ERR_CUDA if a tensor-core wait times out.  Used by
- * the surrogate; no reference counterpart. */
+ * d_A and d_B 16-byte aligned, lda and ldb multiples of 8 (the operands are
+ * loaded by TMA); *d_err is set to BRKGA_ERR_CUDA if a tensor-core or copy
+ * wait times out.  Used by the surrogate; no reference counterpart. */
 int brkga_gemm_bf16(const void* d_A, int32_t lda, const void* d_B, int32_t ldb, float* d_C, int32_t ldc,
                     int32_t M, int32_t N, int32_t K, int32_t* d_err, void* stream);
 

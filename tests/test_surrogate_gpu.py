@@ -112,3 +112,34 @@ def test_online_training_learns_to_rank(torch, p100):
     sur.train(300, batch=512, lr=1e-3)
     after = spearman(sur.predict(test).cpu().numpy(), exact)
     assert after > 0.7 and after > before + 0.2, (before, after)
+
+
+def test_observe_fills_ring_in_row_order(torch, p100):
+    """Feasible rows (finite, below 1e15) take ring slots in row order, across
+    the 1024-row passes of one call and across calls, wrapping at capacity;
+    infeasible and NaN rows take none."""
+    from brkga_fft2_b200.surrogate import Surrogate
+    inst, pk, dd, _ = p100
+    cap = 3000
+    sur = Surrogate(dd.native, max_batch=1024, buffer_capacity=cap, seed=1)
+    rng = np.random.default_rng(5)
+    ms = rng.uniform(5e5, 9e5, 5000)
+    ms[::7] = 1e16
+    ms[3::11] = np.nan
+    ch = torch.from_numpy(instances.chromosomes(5000, inst.nb_parts, 4)).cuda()
+    msd = torch.from_numpy(ms).cuda()
+    sur.observe(ch[:2500], msd[:2500])
+    sur.observe(ch[2500:], msd[2500:])
+    torch.cuda.synchronize()
+    norm = sur._io(5, np.zeros(3, np.float64), False)
+    count = sur._io(9, np.zeros(1, np.int64), False)
+    ring = sur._io(8, np.zeros(cap, np.float32), False)
+    feas = np.isfinite(ms) & (ms < 1e15)
+    first = ms[:2500][feas[:2500]]
+    assert norm[2] == 1.0
+    assert norm[0] == pytest.approx(first.mean(), rel=1e-12)
+    assert int(count[0]) == int(feas.sum())
+    want = np.full(cap, np.nan, np.float32)
+    for k, v in enumerate(ms[feas]):
+        want[k % cap] = np.float32((v - norm[0]) / norm[1])
+    np.testing.assert_array_equal(ring, want)
