@@ -720,24 +720,48 @@ __device__ __forceinline__ unsigned long long search_plate(const Tables& tb, con
 // column x (binClassNew.py:155-174): OR the mask rows into the plate words,
 // recompute the vacancy of the touched rows (numba_utils.py:160-188); thread 0
 // updates the plate scalars with the part's area and times on this machine.
-// All threads of the CTA; contains __syncthreads.
+// One thread per mask row does both the OR of its row and that plate row's
+// vacancy (a plate row is touched by one mask row only), so no barrier
+// separates them.  All threads of the CTA; ends with __syncthreads.
 __device__ __forceinline__ void place_part(const Tables& tb, const MachDev& md, uint32_t* grid, uint16_t* vac,
                                            BinScal* scal, int t, int r, int x, int ty, double a, double ptv,
                                            double pthv) {
   const int tid = threadIdx.x;
   const RotDev rd = tb.rot[t * 4 + r];
-  const int sx = x & 31, wx = x >> 5, span = rd.mw + 1;
+  const int sx = x & 31, wx = x >> 5, mw = rd.mw;
   const uint32_t* mb = tb.maskbits + rd.mask_base;
-  for (int idx = tid; idx < rd.h * span; idx += blockDim.x) {
-    const int i = idx / span, j = idx - i * span;
-    const uint32_t lo = j > 0 ? __ldg(mb + i * rd.mw + j - 1) : 0u;
-    const uint32_t hi = j < rd.mw ? __ldg(mb + i * rd.mw + j) : 0u;
-    const uint32_t v = __funnelshift_l(lo, hi, sx);
-    if (v) grid[(size_t)(ty + i) * md.RS + wx + j] |= v;
+  for (int i = tid; i < rd.h; i += blockDim.x) {
+    uint32_t* row = grid + (size_t)(ty + i) * md.RS;
+    const uint32_t* m = mb + (size_t)i * mw;
+    uint32_t* dst = row + wx;
+    if (mw <= 8) {  // all loads first, so their latencies overlap
+      uint32_t w[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) w[j] = j < mw ? __ldg(m + j) : 0u;
+      uint32_t prev = 0u;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        if (j < mw) {
+          const uint32_t v = __funnelshift_l(prev, w[j], sx);
+          if (v) dst[j] |= v;
+          prev = w[j];
+        }
+      }
+      const uint32_t v = __funnelshift_l(prev, 0u, sx);
+      if (v) dst[mw] |= v;
+    } else {
+      uint32_t prev = 0u;
+      for (int j = 0; j < mw; ++j) {
+        const uint32_t cur = __ldg(m + j);
+        const uint32_t v = __funnelshift_l(prev, cur, sx);
+        if (v) dst[j] |= v;
+        prev = cur;
+      }
+      const uint32_t v = __funnelshift_l(prev, 0u, sx);
+      if (v) dst[mw] |= v;
+    }
+    vac[ty + i] = (uint16_t)max_zero_run(row, md.W, md.NW);
   }
-  __syncthreads();
-  for (int i = tid; i < rd.h; i += blockDim.x)
-    vac[ty + i] = (uint16_t)max_zero_run(grid + (size_t)(ty + i) * md.RS, md.W, md.NW);
   if (tid == 0) {
     BinScal s = *scal;
     s.area += a;
