@@ -143,3 +143,23 @@ def test_observe_fills_ring_in_row_order(torch, p100):
     for k, v in enumerate(ms[feas]):
         want[k % cap] = np.float32((v - norm[0]) / norm[1])
     np.testing.assert_array_equal(ring, want)
+
+
+def test_gemm_bf16_refuses_misaligned_operands(torch):
+    """The operands are loaded by TMA: a base address that is not 16-byte
+    aligned is refused before anything is launched."""
+    lib = abi.load_library()
+    A = torch.zeros(128 * 64 + 8, dtype=torch.bfloat16, device="cuda")
+    B = torch.zeros(64, 64, dtype=torch.bfloat16, device="cuda")
+    C = torch.zeros(128, 64, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    bad = ctypes.c_void_p(A.data_ptr() + 2)  # one bf16 element off a 16-byte boundary
+    st = lib.brkga_gemm_bf16(bad, 64, ctypes.c_void_p(B.data_ptr()), 64, ctypes.c_void_p(C.data_ptr()), 64,
+                             128, 64, 64, ctypes.c_void_p(err.data_ptr()), s)
+    assert st == abi.ERR_INVALID_ARGUMENT
+    st = lib.brkga_gemm_bf16(ctypes.c_void_p(A.data_ptr()), 64, ctypes.c_void_p(B.data_ptr()), 64,
+                             ctypes.c_void_p(C.data_ptr()), 64, 128, 64, 64, ctypes.c_void_p(err.data_ptr()), s)
+    assert st == 0
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
