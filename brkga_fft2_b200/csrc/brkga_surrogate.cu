@@ -29,6 +29,7 @@
 #include <cstdint>
 #include <cstring>
 #include <mutex>
+#include <utility>
 #include <vector>
 
 #include "../../include/brkga_b200.h"
@@ -109,6 +110,8 @@ struct FeatParams {
 // sequencing key alone, machine keys ignored, and per part its key, its area
 // over the largest part area and its height time on machine 0 over the largest.
 __global__ void features_kernel(FeatParams p) {
+  umma::pdl_wait();
+  umma::pdl_trigger();
   extern __shared__ unsigned long long keys[];
   __shared__ float s_area[256], s_pt[256];
   __shared__ int s_cnt[257], s_start[257];
@@ -194,6 +197,26 @@ __global__ void features_kernel(FeatParams p) {
   }
 }
 
+// Launch with programmatic stream serialisation: the kernel may begin while
+// the one before it in the stream finishes; it waits for that kernel's
+// results in pdl_wait() (see umma_gemm.cuh).  In a captured graph the
+// dependency becomes a programmatic edge.  A failed launch is reported by
+// the next cudaGetLastError().
+template <typename... KArgs, typename... Args>
+void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
 // out[h] = sum_b A[b, h] * (scale ? scale[b] : 1) * (mask ? (mask[b, h] > 0) : 1) * (colscale ? colscale[h] : 1)
 // 32 columns per CTA (threadIdx.x, coalesced rows), the rows split over
 // kColRows thread rows and summed in shared memory in a fixed order, so the
@@ -202,6 +225,8 @@ constexpr int kColRows = 16;
 __global__ void __launch_bounds__(32 * kColRows) col_reduce_kernel(const float* A, const float* scale,
                                                                    const float* mask, const float* colscale, int B,
                                                                    int H, float* out) {
+  umma::pdl_wait();
+  umma::pdl_trigger();
   __shared__ float part[kColRows][33];
   const int h = blockIdx.x * 32 + threadIdx.x;
   float s = 0.f;
@@ -226,7 +251,7 @@ __global__ void __launch_bounds__(32 * kColRows) col_reduce_kernel(const float* 
 
 void col_reduce(const float* A, const float* scale, const float* mask, const float* colscale, int B, int H,
                 float* out, cudaStream_t st) {
-  col_reduce_kernel<<<(H + 31) / 32, dim3(32, kColRows), 0, st>>>(A, scale, mask, colscale, B, H, out);
+  launch_pdl(col_reduce_kernel, (H + 31) / 32, dim3(32, kColRows), 0, st, A, scale, mask, colscale, B, H, out);
 }
 
 // The output layer's backward pass and the loss, from the partial dot
@@ -243,6 +268,8 @@ __global__ void __launch_bounds__(256) out_backward_kernel(
     const float* part, int n_tiles, int ld_part, const float* b3, const float* t, const int* n_valid, const float* Z2,
     const float* w3, int B, float* y, __nv_bfloat16* dZ, __nv_bfloat16* dZT, float* pw3, float* pb2, float* pb3,
     float* ploss, long long* step, long long* adam_t, int bump) {
+  umma::pdl_wait();
+  umma::pdl_trigger();
   __shared__ float s_dy[32], s_e[32];
   __shared__ __nv_bfloat16 s_t[32][34];  // [column][row], padded
   __shared__ float s_w[8][33], s_b[8][33];
@@ -337,6 +364,8 @@ __device__ __forceinline__ float out_grad(int i, float g, int off_b2, const OutP
 // The output layer's gradients and the loss into the flat gradient vector
 // (the gradients entry point, which runs no Adam).
 __global__ void out_grads_kernel(float* grads, int off_b2, OutPartials op) {
+  umma::pdl_wait();
+  umma::pdl_trigger();
   for (int j = threadIdx.x; j < 2 * kH2 + 1; j += blockDim.x) grads[off_b2 + j] = out_grad(off_b2 + j, 0.f, off_b2, op);
 }
 
@@ -344,6 +373,8 @@ __global__ void out_grads_kernel(float* grads, int off_b2, OutPartials op) {
 // once the target scaling is set.
 __global__ void predict_out_kernel(const float* part, int n_tiles, int ld_part, const float* b3, int P,
                                    const double* norm, float* y, double* out) {
+  umma::pdl_wait();
+  umma::pdl_trigger();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= P) return;
   float v = b3[0];
@@ -360,6 +391,8 @@ __global__ void predict_out_kernel(const float* part, int n_tiles, int ld_part, 
 __global__ void adam_cast_kernel(float* w, float* g, float* m, float* v, int n, float lr, float b1, float b2,
                                  float eps, const long long* t_ptr, int nW1, int offW2, int nW2, __nv_bfloat16* W1b,
                                  __nv_bfloat16* W2b, __nv_bfloat16* W2Tb, int off_b2, OutPartials op) {
+  umma::pdl_wait();
+  umma::pdl_trigger();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const float t = (float)(*t_ptr);
@@ -418,6 +451,8 @@ struct ObsParams {
 
 // Standardisation from the first observed batch (feasible rows only).
 __global__ void set_norm_kernel(const double* ms, int P, double* norm) {
+  umma::pdl_wait();
+  umma::pdl_trigger();
   if (norm[2] != 0.0) return;
   __shared__ double s1[256], s2[256], sn[256];
   const int tid = threadIdx.x;
@@ -458,6 +493,8 @@ __global__ void set_norm_kernel(const double* ms, int P, double* norm) {
 constexpr int kObsThreads = 1024;
 __global__ void __launch_bounds__(kObsThreads) observe_slots_kernel(const double* ms, int P, const double* norm,
                                                                     long long* count, int cap, int* slot) {
+  umma::pdl_wait();
+  umma::pdl_trigger();
   __shared__ int warp_sum[kObsThreads / 32];
   __shared__ long long base;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
@@ -494,6 +531,8 @@ __global__ void __launch_bounds__(kObsThreads) observe_slots_kernel(const double
 
 // Append feasible rows (features + standardised target) to their slots.
 __global__ void observe_kernel(ObsParams p, const int* slot) {
+  umma::pdl_wait();
+  umma::pdl_trigger();
   const int r = blockIdx.x;
   if (r >= p.P) return;
   const int sl = slot[r];
@@ -507,6 +546,8 @@ __global__ void observe_kernel(ObsParams p, const int* slot) {
 __global__ void gather_kernel(const __nv_bfloat16* bufX, const float* bufY, const long long* count, int cap, int B,
                               int n_valid_max, int in_pad, uint32_t k0, uint32_t k1, const long long* step,
                               __nv_bfloat16* X, __nv_bfloat16* XT, float* y, int* n_valid) {
+  umma::pdl_wait();
+  umma::pdl_trigger();
   const int b = blockIdx.x;
   const long long filled = min((long long)cap, *count);
   const int nv = (int)min((long long)n_valid_max, filled);
@@ -658,10 +699,11 @@ int gemm(const __nv_bfloat16* A, int lda, const __nv_bfloat16* B, int ldb, const
   int r;
   if ((r = tile_map(&ta, A, M, K, lda, umma::kTileM)) || (r = tile_map(&tb, B, N, K, ldb, bn))) return r;
   if (bn == 128) {
-    umma::gemm_bf16_kernel<128><<<dim3(M / 128, N / 128), 128, umma::gemm_smem_bytes<128>(), st>>>(ta, tb, ep, K,
-                                                                                                  err);
+    launch_pdl(umma::gemm_bf16_kernel<128>, dim3(M / 128, N / 128), 128, umma::gemm_smem_bytes<128>(), st, ta, tb,
+               ep, K, err);
   } else {
-    umma::gemm_bf16_kernel<64><<<dim3(M / 128, N / 64), 128, umma::gemm_smem_bytes<64>(), st>>>(ta, tb, ep, K, err);
+    launch_pdl(umma::gemm_bf16_kernel<64>, dim3(M / 128, N / 64), 128, umma::gemm_smem_bytes<64>(), st, ta, tb, ep,
+               K, err);
   }
   return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
 }
@@ -697,7 +739,7 @@ int features(BrkgaSurrogate* s, const float* d_chrom, int P, __nv_bfloat16* X, c
   fp.row_offset = 0;
   int S2 = 1;
   while (S2 < s->N) S2 <<= 1;
-  features_kernel<<<P, std::min(1024, std::max(64, S2 / 2)), (size_t)S2 * 8, st>>>(fp);
+  launch_pdl(features_kernel, P, std::min(1024, std::max(64, S2 / 2)), (size_t)S2 * 8, st, fp);
   return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
 }
 
@@ -769,11 +811,11 @@ int gradients(BrkgaSurrogate* s, int B, int bump, cudaStream_t st) {
   float* pw3 = s->outp;
   float* pb2 = pw3 + (size_t)nrb * kH2;
   float* pb3 = pb2 + (size_t)nrb * kH2;
-  out_backward_kernel<<<dim3(kH2 / 32, nrb), dim3(32, 8), 0, st>>>(
+  launch_pdl(out_backward_kernel, dim3(kH2 / 32, nrb), dim3(32, 8), 0, st,
       s->part, n_tiles, s->max_batch, s->b3, s->t, s->n_valid, s->Z2, s->w3, B, s->y, s->dZ2b, s->dZ2Tb, pw3, pb2,
       pb3, pb3 + nrb, s->step, s->adam_t, bump);
   s->last_nrb = nrb;
-  if (!bump) out_grads_kernel<<<1, 256, 0, st>>>(s->grads, off_b2(s), out_partials(s, nrb));
+  if (!bump) launch_pdl(out_grads_kernel, 1, 256, 0, st, s->grads, off_b2(s), out_partials(s, nrb));
   if ((r = gemm(s->dZ2Tb, B, s->H1Tb, B, store_to(s->gW2, kH1), kH2, kH1, B, s->err, st))) return r;
   umma::Epilogue eh;
   eh.kind = umma::kReluMask;
@@ -794,10 +836,9 @@ int gradients(BrkgaSurrogate* s, int B, int bump, cudaStream_t st) {
 int adam_cast(BrkgaSurrogate* s, float lr, bool fused_out, cudaStream_t st) {
   const long long nW1 = (long long)kH1 * s->in_pad;
   OutPartials op = out_partials(s, fused_out ? s->last_nrb : 0);
-  adam_cast_kernel<<<grid_for(s->n_params), 256, 0, st>>>(s->params, s->grads, s->mom, s->vel, (int)s->n_params, lr,
-                                                          0.9f, 0.999f, 1e-8f, s->adam_t, (int)nW1,
-                                                          (int)(nW1 + kH1), kH2 * kH1, s->W1b, s->W2b, s->W2Tb,
-                                                          off_b2(s), op);
+  launch_pdl(adam_cast_kernel, grid_for(s->n_params), 256, 0, st, s->params, s->grads, s->mom, s->vel,
+             (int)s->n_params, lr, 0.9f, 0.999f, 1e-8f, s->adam_t, (int)nW1, (int)(nW1 + kH1), kH2 * kH1, s->W1b,
+             s->W2b, s->W2Tb, off_b2(s), op);
   return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
 }
 
@@ -960,8 +1001,8 @@ int brkga_surrogate_predict(BrkgaSurrogate* s, const float* d_chrom, int32_t P, 
     if ((r = features(s, d_chrom + (size_t)off * 2 * s->N, n, s->X, st))) return r;
     int n_tiles = 0;
     if ((r = forward(s, B, false, &n_tiles, st))) return r;
-    predict_out_kernel<<<(n + 255) / 256, 256, 0, st>>>(s->part, n_tiles, s->max_batch, s->b3, n, s->norm, s->y,
-                                                        d_pred + off);
+    launch_pdl(predict_out_kernel, (n + 255) / 256, 256, 0, st, s->part, n_tiles, s->max_batch, s->b3, n, s->norm,
+               s->y, d_pred + off);
   }
   return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
 }
@@ -971,7 +1012,7 @@ int brkga_surrogate_observe(BrkgaSurrogate* s, const float* d_chrom, const doubl
   if (!s || P < 0 || (P > 0 && (!d_chrom || !d_makespan))) return BRKGA_ERR_INVALID_ARGUMENT;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   int r;
-  set_norm_kernel<<<1, 256, 0, st>>>(d_makespan, P, s->norm);
+  launch_pdl(set_norm_kernel, 1, 256, 0, st, d_makespan, P, s->norm);
   for (int off = 0; off < P; off += s->max_batch) {
     const int n = std::min(s->max_batch, P - off);
     if ((r = features(s, d_chrom + (size_t)off * 2 * s->N, n, s->X, st))) return r;
@@ -984,8 +1025,8 @@ int brkga_surrogate_observe(BrkgaSurrogate* s, const float* d_chrom, const doubl
     op.bufY = s->bufY;
     op.cap = s->cap;
     op.norm = s->norm;
-    observe_slots_kernel<<<1, kObsThreads, 0, st>>>(op.makespan, n, s->norm, s->count, s->cap, s->slot);
-    observe_kernel<<<n, 128, 0, st>>>(op, s->slot);
+    launch_pdl(observe_slots_kernel, 1, kObsThreads, 0, st, op.makespan, n, s->norm, s->count, s->cap, s->slot);
+    launch_pdl(observe_kernel, n, 128, 0, st, op, s->slot);
   }
   return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
 }
@@ -1013,9 +1054,8 @@ int brkga_surrogate_train(BrkgaSurrogate* s, int32_t steps, int32_t batch, float
   // layer's backward pass (which also advances the step counters), three
   // backward GEMMs, one column reduction, Adam with the bf16 casts
   for (int i = 0; i < steps; ++i) {
-    gather_kernel<<<batch, 128, 0, st>>>(s->bufX, s->bufY, s->count, s->cap, batch, batch, s->in_pad,
-                                         (uint32_t)s->seed, (uint32_t)(s->seed >> 32), s->step, s->X, s->XT, s->t,
-                                         s->n_valid);
+    launch_pdl(gather_kernel, batch, 128, 0, st, s->bufX, s->bufY, s->count, s->cap, batch, batch, s->in_pad,
+               (uint32_t)s->seed, (uint32_t)(s->seed >> 32), s->step, s->X, s->XT, s->t, s->n_valid);
     if ((r = gradients(s, batch, 1, st))) return r;
     if ((r = adam_cast(s, lr, true, st))) return r;
   }

@@ -122,6 +122,16 @@ __host__ __device__ constexpr int gemm_smem_bytes() {
   return gemm_stages<BN>() * (kTileM * kTileK + BN * kTileK) * 2 + 1024;
 }
 
+// Programmatic dependent launch: a kernel launched with programmatic stream
+// serialisation may start while the kernel before it in the stream is still
+// running; pdl_wait() blocks until that kernel has completed and its memory
+// is visible, so it comes before the first global access of any kernel
+// launched that way.  pdl_trigger() lets the next such kernel start
+// launching (its CTAs then wait in their own pdl_wait).  Both are no-ops for
+// a kernel launched without the attribute.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
 }
@@ -223,6 +233,10 @@ __global__ void __launch_bounds__(128) gemm_bf16_kernel(const __grid_constant__ 
   const uint32_t tmem = tmem_base;
   constexpr uint32_t idesc = instr_desc_bf16(kTileM, BN);
   const int ksteps = K / kTileK;
+  // the set-up above touched no global memory: from here on the operands of
+  // the kernel before this one must be complete
+  pdl_wait();
+  pdl_trigger();
 
   if (tid == 0) {  // producer
     int kt = 0;
