@@ -102,6 +102,15 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def measured_peaks_bf16():
+    """Dense bf16 tensor-core peak in TFLOP/s: the burst figure of MEASURED_PEAKS.json, else the fallback."""
+    path = os.path.join(HERE, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return float(json.load(f)["bf16_tflops"])
+    return 1590.0
+
+
 class ClockSampler:
     """nvidia-smi clock and throttle-reason samples (every 20 ms, timestamped)
     around the timed region; only the samples taken inside it are reported."""
@@ -244,6 +253,15 @@ def roofline_record(prof, kern_s, scan, tests, sm_count, sm_mhz, smem, hbm_peak,
                    "note": "algorithmic bytes = per placement test one read of the bit-packed plate and rotated "
                            "mask, 4*(L*ceil(W/32)+h*ceil(w/32)); the kernel stops early, so this is a scan "
                            "rate, not traffic"}
+    if prof.get("smem_bytes_per_launch"):  # bytes the shared-memory instructions moved (ncu), not the scan model
+        rec["smem"]["actual_bytes_per_launch"] = prof["smem_bytes_per_launch"]
+        rec["smem"]["actual_gbs"] = prof["smem_bytes_per_launch"] / kern_s / 1e9
+        rec["smem"]["actual_frac"] = rec["smem"]["actual_gbs"] / smem["gbs"]
+    if prof.get("l2_bytes_per_launch"):
+        rec["l2"] = {"achieved": prof["l2_bytes_per_launch"] / kern_s / 1e9, "unit": "GB/s",
+                     "bytes_per_launch": prof["l2_bytes_per_launch"],
+                     "l1_global_bytes_per_launch": prof.get("l1_global_bytes_per_launch"),
+                     "note": "L2 requests (lts__t_bytes); no measured L2 peak on this pool"}
     traffic = prof.get("dram_bytes_per_launch")
     rec["traffic"] = traffic
     if traffic:
@@ -253,6 +271,55 @@ def roofline_record(prof, kern_s, scan, tests, sm_count, sm_mhz, smem, hbm_peak,
     rec["profile_build_id"] = prof.get("build_id")
     rec["profile_decoder_source_id"] = prof.get("decoder_source_id")
     rec["profile_matches_build"] = prof.get("decoder_source_id") == decoder_source_id()
+    return rec
+
+
+def surrogate_record(torch, dd, inst, bf16_peak, steps=6, batch=512, n_pred=3600):
+    """The surrogate's tensor-core work on this workload, timed alone as CUDA
+    graph replays: `steps` training steps of `batch` rows (five tcgen05 GEMMs
+    each) and one prediction of `n_pred` rows (two), as FLOP/s of their GEMMs
+    against the dense bf16 peak."""
+    from brkga_fft2_b200 import instances
+    from brkga_fft2_b200.surrogate import Surrogate
+    sur = Surrogate(dd.native, max_batch=4096, buffer_capacity=20000, seed=11)
+    rows = torch.from_numpy(instances.chromosomes(4096, inst.nb_parts, 777)).cuda()
+    ms = torch.empty(4096, dtype=torch.float64, device="cuda")
+    for off in range(0, 4096, dd.max_pop):
+        dd.decode(rows[off:off + dd.max_pop], ms[off:off + dd.max_pop])
+    sur.observe(rows, ms)
+    side = torch.cuda.Stream()
+    pred = torch.empty(n_pred, dtype=torch.float64, device="cuda")
+    I = sur.in_pad
+    jobs = {"train": (lambda: sur.train(steps, batch, 1e-3, stream=side),
+                      steps * 2.0 * batch * (2 * 512 * I + 3 * 256 * 512)),
+            "predict": (lambda: sur.predict(rows[:n_pred], out=pred, stream=side), 2.0 * n_pred * (512 * I + 256 * 512))}
+    rec = {"workload": f"P100M4 features ({I} inputs), MLP {I}-512-256-1 bf16, fp32 accumulation",
+           "peak_tflops": bf16_peak, "peak_source": "measured bf16 burst (MEASURED_PEAKS.json)"}
+    torch.cuda.synchronize()
+    for name, (fn, flops) in jobs.items():
+        with torch.cuda.stream(side):
+            fn()
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=side):
+            fn()
+        for _ in range(3):
+            g.replay()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(side)
+        with torch.cuda.stream(side):
+            for _ in range(20):
+                g.replay()
+        e1.record(side)
+        torch.cuda.synchronize()
+        sec = e0.elapsed_time(e1) / 1000.0 / 20
+        tf = flops / sec / 1e12
+        rec[name] = {"us": sec * 1e6, "gemm_flops": flops, "tflops": tf,
+                     "frac": tf / bf16_peak if bf16_peak else None}
+    rec["train"]["steps"], rec["train"]["batch"] = steps, batch
+    rec["predict"]["rows"] = n_pred
+    sur.close()
     return rec
 
 
@@ -454,6 +521,7 @@ def run_ours(args):
                 line["cpu_baseline"] = cpu
             failed = parity["exact"] != parity["rows"] or not parity["placements_exact"]
         if world == 1 and not args.no_ttt:
+            line["surrogate"] = surrogate_record(torch, dd, inst, measured_peaks_bf16())
             import bench_ga
             # family screening: 8 children per parent pair, the surrogate keeps the best-predicted one;
             # 6 training steps of 512 rows per generation beside the decode

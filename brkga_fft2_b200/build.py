@@ -57,7 +57,7 @@ def decoder_source_id() -> str:
     decode kernel (instruction counts, DRAM bytes) stays valid while this id
     does, whatever else in the library changes."""
     h = hashlib.sha256()
-    names = ["brkga_decoder.cu", "corr_i8.cuh", "umma_gemm.cuh"]
+    names = ["brkga_decoder.cu", "corr_i8.cuh", "umma_core.cuh"]
     for path in [os.path.join(PKG, "csrc", n) for n in names] + sorted(glob.glob(os.path.join(REPO, "include", "*.h"))):
         h.update(os.path.relpath(path, REPO).encode())
         h.update(b"\0")

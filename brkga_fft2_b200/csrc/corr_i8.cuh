@@ -46,7 +46,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#include "umma_gemm.cuh"
+#include "umma_core.cuh"
 
 namespace corr {
 
