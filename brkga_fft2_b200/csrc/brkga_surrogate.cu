@@ -152,13 +152,31 @@ __global__ void features_kernel(FeatParams p) {
       acc += s_cnt[m];
     }
   }
+  // Each part's share of its machine's loads, all parts at once (the table
+  // reads overlap); the per-machine sums below then add them in decode order
+  // from shared memory.
+  float* c_area = reinterpret_cast<float*>(keys + S2);  // [N]
+  float* c_load = c_area + p.N;                         // [N]
+  if (p.kind != BRKGA_SURROGATE_FEATURES_ORDER) {
+    for (int q = tid; q < p.N; q += nt) {
+      const unsigned long long key = keys[q];
+      const int m = (int)(key >> 48);
+      float av = 0.f, lv = 0.f;
+      if (m < p.M) {
+        const int t = p.gene_type[(int)(key & 0xFFFFu)];
+        av = (float)(p.part_area[t] / p.bin_area[m]);
+        lv = (float)p.pt[(size_t)m * p.T + t] * p.inv_pt;
+      }
+      c_area[q] = av;
+      c_load[q] = lv;
+    }
+  }
   __syncthreads();
-  for (int m = tid; m < p.M; m += nt) {
+  for (int m = tid; m < p.M && p.kind != BRKGA_SURROGATE_FEATURES_ORDER; m += nt) {
     float area = 0.f, load = 0.f;
     for (int q = s_start[m]; q < s_start[m] + s_cnt[m]; ++q) {
-      const int t = p.gene_type[(int)(keys[q] & 0xFFFFu)];
-      area += (float)(p.part_area[t] / p.bin_area[m]);
-      load += (float)p.pt[(size_t)m * p.T + t] * p.inv_pt;
+      area += c_area[q];
+      load += c_load[q];
     }
     s_area[m] = area;
     s_pt[m] = load;
@@ -192,6 +210,149 @@ __global__ void features_kernel(FeatParams p) {
     } else if (i < 3 * p.N + 2 * p.M) {
       const int q = i - 3 * p.N;
       v = (q & 1) ? s_pt[q >> 1] : s_area[q >> 1];
+    }
+    row[i] = __float2bfloat16(v);
+  }
+}
+
+// The same features with one warp per chromosome, for N <= 32 E parts and at
+// most 32 machines: the warp sorts the (machine, key, gene) keys in
+// registers (E per lane, bitonic network, partners in other lanes exchanged
+// by shuffles; no CTA barrier), then works from its own slice of shared
+// memory.  Same keys, same order of the per-machine sums, same values as
+// features_kernel: the rows are identical.
+constexpr int kFeatWarps = 8;  // warps (chromosomes) per CTA
+__host__ __device__ constexpr size_t feat_warp_bytes(int E) {
+  return (size_t)32 * E * 8 + (size_t)32 * E * 12 + 4 * 33 * 4;  // keys, shares + types, per-machine arrays
+}
+template <int E>
+__global__ void __launch_bounds__(32 * kFeatWarps) features_warp_kernel(FeatParams p) {
+  umma::pdl_wait();
+  umma::pdl_trigger();
+  extern __shared__ __align__(16) unsigned char fsm[];
+  constexpr int S2 = 32 * E;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int c = blockIdx.x * kFeatWarps + warp;
+  if (c >= p.P) return;
+  unsigned char* base = fsm + (size_t)warp * feat_warp_bytes(E);
+  unsigned long long* keys = reinterpret_cast<unsigned long long*>(base);
+  float* c_area = reinterpret_cast<float*>(keys + S2);
+  float* c_load = c_area + S2;
+  int* c_type = reinterpret_cast<int*>(c_load + S2);
+  int* m_start = c_type + S2;  // [33]
+  float* m_area = reinterpret_cast<float*>(m_start + 33);
+  float* m_load = m_area + 33;
+  const float* ch = p.chrom + (size_t)c * 2 * p.N;
+  const bool order = p.kind == BRKGA_SURROGATE_FEATURES_ORDER;
+  unsigned long long k[E];
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const int i = lane * E + e;
+    k[e] = ~0ull;
+    if (i < p.N) {
+      const int m = order ? 0 : machine_of(ch[p.N + i], p.thr, p.M, p.mode);
+      k[e] = ((unsigned long long)m << 48) | ((unsigned long long)ordered_bits(ch[i]) << 16) | (unsigned long long)i;
+    }
+  }
+  // bitonic sort of S2 keys, element i = lane * E + e
+#pragma unroll 1
+  for (int kk = 2; kk <= S2; kk <<= 1) {
+#pragma unroll 1
+    for (int j = kk >> 1; j > 0; j >>= 1) {
+      if (j >= E) {  // partner in lane ^ (j / E), same register
+        const int dl = j / E;
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          const int i = lane * E + e;
+          const unsigned long long o = __shfl_xor_sync(0xFFFFFFFFu, k[e], dl);
+          const bool asc = (i & kk) == 0, lower = (i & j) == 0;
+          k[e] = (asc == lower) ? (k[e] < o ? k[e] : o) : (k[e] > o ? k[e] : o);
+        }
+      } else {  // partner in the same lane
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+#pragma unroll
+          for (int jj = 1; jj < E; jj <<= 1) {
+            if (jj == j && (e & jj) == 0) {
+              const int i = lane * E + e;
+              const bool asc = (i & kk) == 0;
+              const unsigned long long a = k[e], b = k[e | jj];
+              if ((a > b) == asc) {
+                k[e] = b;
+                k[e | jj] = a;
+              }
+            }
+          }
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int e = 0; e < E; ++e) keys[lane * E + e] = k[e];
+  __syncwarp();
+  // first sorted position of each machine 0..M (the keys are ordered by machine)
+  for (int m = lane; m <= p.M && m <= 32; m += 32) {
+    int lo = 0, hi = S2;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if ((int)(keys[mid] >> 48) < m) lo = mid + 1;
+      else hi = mid;
+    }
+    m_start[m] = lo;
+  }
+  for (int q = lane; q < p.N; q += 32) {
+    const unsigned long long key = keys[q];
+    const int m = (int)(key >> 48);
+    float av = 0.f, lv = 0.f;
+    int t = -1;
+    if (m < p.M) {
+      t = p.gene_type[(int)(key & 0xFFFFu)];
+      if (!order) {
+        av = (float)(p.part_area[t] / p.bin_area[m]);
+        lv = (float)p.pt[(size_t)m * p.T + t] * p.inv_pt;
+      }
+    }
+    c_area[q] = av;
+    c_load[q] = lv;
+    c_type[q] = t;
+  }
+  __syncwarp();
+  if (!order && lane < p.M) {  // per machine, in decode order
+    float area = 0.f, load = 0.f;
+    for (int q = m_start[lane]; q < m_start[lane + 1]; ++q) {
+      area += c_area[q];
+      load += c_load[q];
+    }
+    m_area[lane] = area;
+    m_load[lane] = load;
+  }
+  __syncwarp();
+  __nv_bfloat16* row = p.X + (size_t)(p.row_offset + c) * p.in_pad;
+  if (order) {
+    for (int i = lane; i < p.in_pad; i += 32) {
+      float v = 0.f;
+      if (i < 3 * p.N) {
+        const int q = i / 3, f = i - 3 * q, g = (int)(keys[q] & 0xFFFFu), t = c_type[q];
+        v = f == 0 ? ch[g] : f == 1 ? (float)p.part_area[t] * p.inv_area : (float)p.pth[t] * p.inv_pth;
+      }
+      row[i] = __float2bfloat16(v);
+    }
+    return;
+  }
+  const float mscale = p.M > 1 ? 1.f / (float)(p.M - 1) : 0.f;
+  for (int i = lane; i < p.in_pad; i += 32) {
+    float v = 0.f;
+    if (i < 3 * p.N) {
+      const int q = i / 3, f = i - 3 * q;
+      const int m = (int)(keys[q] >> 48);
+      if (m < p.M) {
+        const int t = c_type[q];
+        v = f == 0 ? (float)m * mscale
+                   : f == 1 ? (float)p.pt[(size_t)m * p.T + t] * p.inv_pt : (float)p.pth[(size_t)m * p.T + t] * p.inv_pth;
+      }
+    } else if (i < 3 * p.N + 2 * p.M) {
+      const int q = i - 3 * p.N;
+      v = (q & 1) ? m_load[q >> 1] : m_area[q >> 1];
     }
     row[i] = __float2bfloat16(v);
   }
@@ -716,6 +877,10 @@ umma::Epilogue store_to(float* C, int ldc) {
   return e;
 }
 
+// Dynamic shared memory of features_kernel: the sort keys, then each part's
+// area and time shares of its machine.
+size_t features_smem(int S2, int N) { return (size_t)S2 * 8 + (size_t)N * 8; }
+
 int features(BrkgaSurrogate* s, const float* d_chrom, int P, __nv_bfloat16* X, cudaStream_t st) {
   FeatParams fp;
   fp.chrom = d_chrom;
@@ -739,7 +904,15 @@ int features(BrkgaSurrogate* s, const float* d_chrom, int P, __nv_bfloat16* X, c
   fp.row_offset = 0;
   int S2 = 1;
   while (S2 < s->N) S2 <<= 1;
-  launch_pdl(features_kernel, P, std::min(1024, std::max(64, S2 / 2)), (size_t)S2 * 8, st, fp);
+  if (s->M <= 32 && S2 <= 256) {  // one warp per chromosome
+    const dim3 grid((P + kFeatWarps - 1) / kFeatWarps), block(32 * kFeatWarps);
+    if (S2 <= 32) launch_pdl(features_warp_kernel<1>, grid, block, kFeatWarps * feat_warp_bytes(1), st, fp);
+    else if (S2 <= 64) launch_pdl(features_warp_kernel<2>, grid, block, kFeatWarps * feat_warp_bytes(2), st, fp);
+    else if (S2 <= 128) launch_pdl(features_warp_kernel<4>, grid, block, kFeatWarps * feat_warp_bytes(4), st, fp);
+    else launch_pdl(features_warp_kernel<8>, grid, block, kFeatWarps * feat_warp_bytes(8), st, fp);
+  } else {
+    launch_pdl(features_kernel, P, std::min(1024, std::max(64, S2 / 2)), features_smem(S2, s->N), st, fp);
+  }
   return cudaGetLastError() == cudaSuccess ? BRKGA_OK : BRKGA_ERR_CUDA;
 }
 
@@ -929,7 +1102,10 @@ int brkga_surrogate_create_ex(const BrkgaProblem* problem, int32_t max_batch, in
     s->inv_pth = mh > 0 ? (float)(1.0 / mh) : 1.f;
     s->inv_area = ma > 0 ? (float)(1.0 / ma) : 1.f;
   }
-  if (cudaFuncSetAttribute(features_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxGenes * 8) !=
+  if (cudaFuncSetAttribute(features_warp_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)(kFeatWarps * feat_warp_bytes(8))) != cudaSuccess ||
+      cudaFuncSetAttribute(features_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)features_smem(kMaxGenes, kMaxGenes)) !=
           cudaSuccess ||
       prepare_gemm() != BRKGA_OK) {
     delete s;

@@ -60,6 +60,29 @@ def test_features_match_oracle(torch, p100):
     np.testing.assert_array_equal(got, ref)
 
 
+@pytest.mark.parametrize("workload", ["p50m2", "p200m6", "p400m8"])
+def test_features_match_oracle_across_sizes(torch, workload):
+    """Both feature kernels (one warp per chromosome up to 256 parts, one CTA
+    per chromosome beyond) against the oracle, with tied sequencing keys, a
+    NaN machine key (the part matches no machine) and keys on the float32
+    thresholds."""
+    from brkga_fft2_b200.evaluator import DeviceDecoder
+    from brkga_fft2_b200.surrogate import Surrogate
+    inst = getattr(instances, workload)(0)
+    pk = pack_problem(inst.problem_data, inst.nb_parts, inst.nb_machines, inst.thresholds, inst.instance_parts)
+    dd = DeviceDecoder(pk, max_pop=64)
+    N = inst.nb_parts
+    ch = instances.chromosomes(37, N, 21)
+    ch[0, :7] = ch[0, 7]
+    ch[1, N + 3] = np.float32(np.nan)
+    ch[2, N:N + 4] = np.float32(1.0 / inst.nb_machines)
+    for kind, ref in (("decode", mo.features), ("order", mo.order_features)):
+        sur = Surrogate(dd.native, max_batch=128, buffer_capacity=1000, seed=3, features=kind)
+        got = sur.features(torch.from_numpy(ch).cuda())
+        np.testing.assert_array_equal(got, ref(pk, ch, sur.in_pad))
+        sur.close()
+
+
 def test_order_features_match_oracle(torch, p100):
     """The screened configuration's input (per part its sequencing key, area
     and height, parts sorted by key); here P100M4: 300 values."""
