@@ -174,6 +174,9 @@ class DeviceBRKGA:
             # observed up to the previous generation), joined before the next prediction.
             self.overlap_training = bool(overlap_training)
             self._train_stream = torch.cuda.Stream(dev) if self.overlap_training else None
+            # the surrogate's quality statistics (two ranks, Spearman, MAE) run on a third
+            # stream beside the example-ring update; they only read the predictions and makespans
+            self._stats_stream = torch.cuda.Stream(dev)
             # exploration: that share of the decoded rows is spread evenly over the
             # pool's lower-ranked candidates instead of taken from its top
             cand = self.pool_rows - self.n_fixed
@@ -249,16 +252,20 @@ class DeviceBRKGA:
         exact = self.fitness_buf[nxt][first:]
         if not screened:
             self.surrogate.predict(decoded, out=self.pred_sel[:rows])
-        self._rank(self.pred_sel, rows, self.o_pred)
-        self._rank(exact, rows, self.o_exact)
-        abi.check(self.lib.brkga_ga_screen_stats(self._ptr(self.pred_sel), self._ptr(exact), self._ptr(self.o_pred),
-                                                 self._ptr(self.o_exact), rows, self._ptr(self.generation),
-                                                 self._ptr(self.stats_dev), self.num_generations + 1,
-                                                 self._ptr(self.stat_scratch), self._stream()),
-                  "brkga_ga_screen_stats")
+        main = self.torch.cuda.current_stream(self.device)
+        self._stats_stream.wait_stream(main)
+        with self.torch.cuda.stream(self._stats_stream):
+            self._rank(self.pred_sel, rows, self.o_pred)
+            self._rank(exact, rows, self.o_exact)
+            abi.check(self.lib.brkga_ga_screen_stats(self._ptr(self.pred_sel), self._ptr(exact),
+                                                     self._ptr(self.o_pred), self._ptr(self.o_exact), rows,
+                                                     self._ptr(self.generation), self._ptr(self.stats_dev),
+                                                     self.num_generations + 1, self._ptr(self.stat_scratch),
+                                                     self._stream()), "brkga_ga_screen_stats")
         self.surrogate.observe(decoded, self.fitness_buf[nxt][ne:])
         if not self.overlap_training:
             self.surrogate.train(self.train_steps, self.train_batch, self.lr)
+        main.wait_stream(self._stats_stream)
 
     def _step_learn(self, cur):
         """Plain generation that also measures and trains the surrogate."""
