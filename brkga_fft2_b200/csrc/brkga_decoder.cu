@@ -1268,6 +1268,10 @@ struct BrkgaProblem {
   double* e_out = nullptr;
   int32_t* e_status = nullptr;
   BrkgaPlacement* e_log = nullptr;
+  // page-locked staging of a call's results: status at 0, counters at 8,
+  // makespans from 64, so the three copies back are queued without a
+  // staging round trip each and waited for once
+  unsigned char* e_host = nullptr;
   void* e_ws = nullptr;
   size_t e_ws_bytes = 0;
   int e_cap_P = 0;
@@ -1795,6 +1799,7 @@ void brkga_problem_destroy(BrkgaProblem* pb) {
     if (pb->e_status) cudaFree(pb->e_status);
     if (pb->e_log) cudaFree(pb->e_log);
     if (pb->e_ws) cudaFree(pb->e_ws);
+    if (pb->e_host) cudaFreeHost(pb->e_host);
     if (pb->stream) cudaStreamDestroy(pb->stream);
   }
   delete pb;
@@ -2016,6 +2021,8 @@ int brkga_evaluate_host(BrkgaProblem* pb, const float* h_chrom, int32_t P, doubl
     cudaFree(pb->e_out);
     cudaFree(pb->e_status);
     cudaFree(pb->e_log);
+    if (pb->e_host) cudaFreeHost(pb->e_host);
+    pb->e_host = nullptr;
     pb->e_chrom = nullptr;
     pb->e_out = nullptr;
     pb->e_status = nullptr;
@@ -2023,7 +2030,8 @@ int brkga_evaluate_host(BrkgaProblem* pb, const float* h_chrom, int32_t P, doubl
     pb->e_cap_P = 0;
     if (cudaMalloc(&pb->e_chrom, (size_t)cap * 2 * pb->N * sizeof(float)) != cudaSuccess ||
         cudaMalloc(&pb->e_out, (size_t)cap * sizeof(double)) != cudaSuccess ||
-        cudaMalloc(&pb->e_status, sizeof(int32_t)) != cudaSuccess)
+        cudaMalloc(&pb->e_status, sizeof(int32_t)) != cudaSuccess ||
+        cudaHostAlloc(&pb->e_host, 64 + (size_t)cap * sizeof(double), cudaHostAllocDefault) != cudaSuccess)
       return BRKGA_ERR_CUDA;
     if ((want_log || pb->e_cap_log) &&
         cudaMalloc(&pb->e_log, (size_t)cap * pb->M * pb->N * sizeof(BrkgaPlacement)) != cudaSuccess)
@@ -2050,17 +2058,19 @@ int brkga_evaluate_host(BrkgaProblem* pb, const float* h_chrom, int32_t P, doubl
     int st = brkga_decode(pb, pb->e_chrom, P, pb->e_out, want_log ? pb->e_log : nullptr, pb->e_status, pb->e_ws,
                           pb->e_ws_bytes, pb->e_pool_bins, pb->stream);
     if (st) return st;
-    int32_t status = 0;
-    if (cudaMemcpyAsync(&status, pb->e_status, sizeof(int32_t), cudaMemcpyDeviceToHost, pb->stream) !=
-            cudaSuccess ||
-        cudaMemcpyAsync(h_makespan, pb->e_out, (size_t)P * sizeof(double), cudaMemcpyDeviceToHost,
-                        pb->stream) != cudaSuccess)
-      return BRKGA_ERR_CUDA;
-    unsigned long long counters[4] = {0, 0, 0, 0};
-    if (cudaMemcpyAsync(counters, static_cast<char*>(pb->e_ws) + l.off_ctr + 8, sizeof(counters),
-                        cudaMemcpyDeviceToHost, pb->stream) != cudaSuccess)
+    unsigned char* hs = pb->e_host;
+    if (cudaMemcpyAsync(hs, pb->e_status, sizeof(int32_t), cudaMemcpyDeviceToHost, pb->stream) != cudaSuccess ||
+        cudaMemcpyAsync(hs + 8, static_cast<char*>(pb->e_ws) + l.off_ctr + 8, 4 * sizeof(unsigned long long),
+                        cudaMemcpyDeviceToHost, pb->stream) != cudaSuccess ||
+        cudaMemcpyAsync(hs + 64, pb->e_out, (size_t)P * sizeof(double), cudaMemcpyDeviceToHost, pb->stream) !=
+            cudaSuccess)
       return BRKGA_ERR_CUDA;
     if (cudaStreamSynchronize(pb->stream) != cudaSuccess) return BRKGA_ERR_CUDA;
+    int32_t status = 0;
+    unsigned long long counters[4];
+    std::memcpy(&status, hs, sizeof(status));
+    std::memcpy(counters, hs + 8, sizeof(counters));
+    std::memcpy(h_makespan, hs + 64, (size_t)P * sizeof(double));
     for (int i = 0; i < 4; ++i) pb->last_counters[i] = (int64_t)counters[i];
     if (status == BRKGA_ERR_CAPACITY) {
       pb->e_pool_bins *= 2;
