@@ -333,12 +333,12 @@ def run_reference(args):
     from brkga_fft2_b200 import instances
     inst, packed = load_workload()
     threads = os.cpu_count() or 1
-    # size each step for ~2 s of CPU work
-    probe = instances.chromosomes(threads, inst.nb_parts, 99)
+    # size each step for ~3 s of CPU work, from a probe of four rows per thread
+    probe = instances.chromosomes(4 * threads, inst.nb_parts, 99)
     t0 = time.perf_counter()
     oracle_decode(packed, probe, n_threads=threads)
-    rate = threads / (time.perf_counter() - t0)
-    n = int(min(args.pop, max(threads, threads * round(2.0 * rate / threads))))
+    rate = 4 * threads / (time.perf_counter() - t0)
+    n = int(min(args.pop, max(threads, threads * round(3.0 * rate / threads))))
     for s in range(args.warmup):
         oracle_decode(packed, instances.chromosomes(n, inst.nb_parts, chrom_seed(0, s)), n_threads=threads)
     total = 0.0

@@ -406,7 +406,8 @@ static double decode_one(const Model* m, const float* chrom, BrkgaPlacement* log
 typedef struct {
   const Model* m;
   const float* chrom;
-  int P, tid, nthreads;
+  int P;
+  int* next;  /* the next row to decode, shared by the threads */
   double* out;
   BrkgaPlacement* log;
   int err;
@@ -418,7 +419,10 @@ static void* worker(void* arg) {
   const int N = d->n_genes, M = d->n_machines;
   KeyGene* buf = (KeyGene*)malloc(sizeof(KeyGene) * (size_t)(N > 0 ? N : 1));
   Plate* plates = (Plate*)malloc(sizeof(Plate) * (size_t)(N > 0 ? N : 1));
-  for (int c = jb->tid; c < jb->P; c += jb->nthreads) {
+  /* rows are taken one at a time from a shared counter, so a thread that
+     drew short rows takes more of them (rows differ in cost several-fold) */
+  for (int c = __atomic_fetch_add(jb->next, 1, __ATOMIC_RELAXED); c < jb->P;
+       c = __atomic_fetch_add(jb->next, 1, __ATOMIC_RELAXED)) {
     BrkgaPlacement* lg = jb->log ? jb->log + (size_t)c * M * N : NULL;
     if (lg)
       for (size_t i = 0; i < (size_t)M * N; ++i) {
@@ -445,12 +449,12 @@ int oracle_decode(const BrkgaProblemDesc* d, const float* chrom, int P, double* 
   model_init(&m, d);
   Job* jobs = (Job*)calloc((size_t)n_threads, sizeof(Job));
   pthread_t* th = (pthread_t*)calloc((size_t)n_threads, sizeof(pthread_t));
+  int next = 0;
   for (int i = 0; i < n_threads; ++i) {
     jobs[i].m = &m;
     jobs[i].chrom = chrom;
     jobs[i].P = P;
-    jobs[i].tid = i;
-    jobs[i].nthreads = n_threads;
+    jobs[i].next = &next;
     jobs[i].out = makespan;
     jobs[i].log = log;
     jobs[i].err = 0;
