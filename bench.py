@@ -114,8 +114,10 @@ def measured_peaks_bf16():
 
 
 class ClockSampler:
-    """nvidia-smi clock and throttle-reason samples (every 20 ms, timestamped)
-    around the timed region; only the samples taken inside it are reported."""
+    """nvidia-smi clock and throttle-reason samples (every 5 ms asked, as fast
+    as nvidia-smi answers; timestamped) around the timed region; only the
+    samples taken inside it are reported."""
+    INTERVAL_MS = 5
     FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -127,7 +129,7 @@ class ClockSampler:
         self.t0 = self.t1 = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                                          "-lms", "20", "-i", str(gpu_index)],
+                                          "-lms", str(self.INTERVAL_MS), "-i", str(gpu_index)],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -170,7 +172,7 @@ class ClockSampler:
         reasons = sorted({names[i] for _, _, _, r in use for i, v in enumerate(r) if v.lower() == "active"})
         return {"sm_mhz": statistics.median(r[1] for r in use), "sm_max_mhz": max(r[2] for r in use),
                 "reasons": reasons, "samples": len(use), "in_timed_region": bool(inside),
-                "interval_ms": 20}
+                "interval_ms": self.INTERVAL_MS}
 
 
 def decode_profile():
