@@ -110,3 +110,18 @@ def test_six_machine_golden_exercises_the_float32_thresholds():
     m64 = oracle_decode(p64, ch, n_threads=4)
     np.testing.assert_array_equal(m32, z["makespans"])
     assert (m32 != m64).any()
+
+
+def test_oracle_results_do_not_depend_on_threads():
+    """The oracle's threads take rows from a shared counter: any thread count
+    gives the same makespans and placement logs, row for row."""
+    from brkga_fft2_b200 import instances, pack_problem
+    from oracle import oracle_decode
+    inst = instances.p50m2(0)
+    pk = pack_problem(inst.problem_data, inst.nb_parts, inst.nb_machines, inst.thresholds, inst.instance_parts)
+    ch = instances.chromosomes(37, inst.nb_parts, 5)
+    ms1, log1 = oracle_decode(pk, ch, n_threads=1, with_log=True)
+    for nt in (3, 8, 64):
+        ms, log = oracle_decode(pk, ch, n_threads=nt, with_log=True)
+        np.testing.assert_array_equal(ms, ms1)
+        assert (log == log1).all()
