@@ -64,6 +64,10 @@ def main():
                          "runs one screened GA per value")
     ap.add_argument("--train-batch", type=int, default=512, help="rows per surrogate training step (multiple of 128)")
     ap.add_argument("--lr", type=float, default=1e-3, help="the surrogate's Adam learning rate")
+    ap.add_argument("--spearman-threshold", type=float, default=0.3,
+                    help="screening runs while the surrogate's recent Spearman is at least this")
+    ap.add_argument("--check-every", type=int, default=5, help="generations between screening decisions")
+    ap.add_argument("--warmup-generations", type=int, default=5, help="generations before screening may start")
     ap.add_argument("--screen-mode", default="family",
                     help="family: the surrogate picks one child per parent pair; pool: the best rows of the pool")
     ap.add_argument("--screen-mutants", type=int, default=0,
@@ -80,11 +84,13 @@ def main():
                 for f in str(args.features).split(",")]
     print(json.dumps(time_to_target(args.workload, args.pop, args.generations, args.seeds, args.oversample,
                                     variants, args.screened_limit, bool(args.screen_mutants), args.screen_mode,
-                                    args.train_batch, args.lr)))
+                                    args.train_batch, args.lr,
+                                    gate=(args.spearman_threshold, args.check_every, args.warmup_generations))))
 
 
 def time_to_target(workload, P, generations, seeds, oversample=5, variants=((8, 0.0, 1, "decode"),),
-                   screened_limit=2.0, screen_mutants=False, screen_mode="family", train_batch=512, lr=1e-3):
+                   screened_limit=2.0, screen_mutants=False, screen_mode="family", train_batch=512, lr=1e-3,
+                   gate=(0.3, 5, 5)):
     """Plain GPU GA for `generations` generations, then each screened variant
     (train_steps, explore, overlap, surrogate features) against its best
     makespan, per seed; the record printed by this script (medians per
@@ -111,7 +117,7 @@ def time_to_target(workload, P, generations, seeds, oversample=5, variants=((8, 
         for ts, ex, ov, ft in variants:
             runs.append(screened_run(generations, screened_limit, oversample, inst, pk, P, ne, nm, seed, ts, ex, ov,
                                      ft, target, t_plain, p_hit, t_plain_hit, screen_mutants, screen_mode,
-                                     train_batch, lr))
+                                     train_batch, lr, gate))
             torch.cuda.empty_cache()
     by_variant = {}
     for ts, ex, ov, ft in variants:
@@ -128,6 +134,7 @@ def time_to_target(workload, P, generations, seeds, oversample=5, variants=((8, 
             "pop": P, "generations": generations, "oversample": oversample,
             "screened_limit": screened_limit, "screen_mode": screen_mode, "screen_mutants": screen_mutants,
             "train_batch": train_batch, "lr": lr,
+            "gate": {"spearman_threshold": gate[0], "check_every": gate[1], "warmup_generations": gate[2]},
             "train_steps": variants[0][0],
             "explore": variants[0][1], "overlap": variants[0][2], "features": variants[0][3], "seeds": seeds,
             "reached": first["reached"],
@@ -138,7 +145,7 @@ def time_to_target(workload, P, generations, seeds, oversample=5, variants=((8, 
 
 def screened_run(generations, screened_limit, oversample, inst, pk, P, ne, nm, seed, train_steps, explore, overlap,
                  features, target, t_plain, p_hit, t_plain_hit, screen_mutants=False, screen_mode="family",
-                 train_batch=512, lr=1e-3):
+                 train_batch=512, lr=1e-3, gate=(0.3, 5, 5)):
     """One screened GA against the plain run's target; a dict for the JSON line."""
     from brkga_fft2_b200.ga import DeviceBRKGA
     scr = DeviceBRKGA(None, inst.nb_parts, inst.nb_machines, inst.thresholds, inst.instance_parts,
@@ -147,7 +154,8 @@ def screened_run(generations, screened_limit, oversample, inst, pk, P, ne, nm, s
                       eliteCProb=0.7, seed=seed, packed=pk, screening=True, oversample=oversample,
                       train_steps=train_steps, explore=explore, overlap_training=bool(overlap), target=target,
                       surrogate_features=features, screen_mutants=screen_mutants, screen_mode=screen_mode,
-                      train_batch=train_batch, lr=lr)
+                      train_batch=train_batch, lr=lr, spearman_threshold=gate[0], check_every=gate[1],
+                      warmup_generations=gate[2])
     scr.fit()
     mins = np.array(scr.history["min"])
     hit = np.flatnonzero(mins <= target)
