@@ -91,8 +91,10 @@ def workload_config(pop: int, world: int) -> dict:
 CPU_CODE = "oracle/brkga_oracle.c"
 CPU_NOTE = ("the C restatement (port) of the reference's sequential decoder, placement.py:94-165 with "
             "binClassNew.py:45-174; not the reference's own Python placementProcedure + numba + torch_cpu path, "
-            "which cannot be installed or shipped to this box; that path's single-core rate measured on the "
-            "reference's real P100M4-0 instance is 1.33 decodes/s (the port: about 7 per thread)")
+            "which cannot be installed or shipped to this box; on one core of the build host and this "
+            "benchmark's own first rows that path decodes 1.45 rows/s and the port 5.53, with equal makespans "
+            "and placements (tests/golden/time_reference.py), so the port is about 3.8x faster per core; "
+            "on the reference's real P100M4-0 instance the path's single-core rate is 1.33 decodes/s")
 
 
 def measured_peaks():

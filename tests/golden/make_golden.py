@@ -369,6 +369,12 @@ def main():
     syn_case("syn_P50M2_s0", i50, syn.chromosomes(32, 50, 1))
     i100 = syn.p100m4(0)
     syn_case("syn_P100M4_s0", i100, syn.chromosomes(8, 100, 1))
+    # the benchmark's own rows: the first 16 chromosomes of the population of
+    # bench.py's first timed step (P100M4 population 500, default warm-up of 5)
+    if want("syn_bench_P100M4_rows"):
+        import bench as bench_py
+        ch = syn.chromosomes(bench_py.POP, 100, bench_py.chrom_seed(0, 5))[:16]
+        syn_case("syn_bench_P100M4_rows", syn.p100m4(bench_py.INSTANCE_SEED), ch)
     # six machines: the thresholds 1/6, 2/6, 4/6, 5/6 are not float32-exact
     # (placement.py:122-127 compares in float32); some machine keys sit on
     # f32(k/6) and on the next float above it
