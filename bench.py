@@ -93,7 +93,8 @@ CPU_NOTE = ("the C restatement (port) of the reference's sequential decoder, pla
             "binClassNew.py:45-174; not the reference's own Python placementProcedure + numba + torch_cpu path, "
             "which cannot be installed or shipped to this box; on one core of the build host and this "
             "benchmark's own first rows that path decodes 1.45 rows/s and the port 5.53, with equal makespans "
-            "and placements (tests/golden/time_reference.py), so the port is about 3.8x faster per core; "
+            "and placements, and on its 8 cores 11.1 rows/s through the reference's process pool against "
+            "41.7 for the port on 8 threads (tests/golden/time_reference.py): the port is about 3.8x faster; "
             "on the reference's real P100M4-0 instance the path's single-core rate is 1.33 decodes/s")
 
 

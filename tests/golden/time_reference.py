@@ -12,6 +12,14 @@ instance).  The first row is decoded once untimed (numba compiles on first
 use).  The oracle (``oracle/brkga_oracle.c``) decodes the same rows on one
 thread.  Prints one JSON line: both rates in decodes/s per core, their ratio,
 and whether every makespan (==) and every placement agree.
+
+With ``--workers W`` it also times the reference the way its GA spreads a
+population over the host cores (``eval_mode="process"``, BRKGA_alg3.py:149-154):
+a process pool of W workers, each holding its own copy of the problem (built,
+and numba compiled, before the clock starts, so the pool's start-up and the
+per-generation pickling the reference pays are left out), mapping the first
+``--pool-rows`` rows of the same population; and the oracle on W threads on
+those rows.
 """
 from __future__ import annotations
 
@@ -32,10 +40,51 @@ from make_golden import Reference, log_to_array  # noqa: E402
 from tests.goldens import part_ids_of_log  # noqa: E402
 
 
+_WORKER = {}
+
+
+def _worker_init(reference):
+    """One process of the pool: the reference and its problem, compiled on one row."""
+    import bench
+    from brkga_fft2_b200 import instances
+    inst, _ = bench.load_workload()
+    ref = Reference(reference)
+    rpd = ref.problem(inst.problem_data, inst.nb_machines)
+    _WORKER.update(ref=ref, rpd=rpd, inst=inst)
+    ref.decode(rpd, inst.nb_parts, inst.nb_machines, inst.thresholds,
+               instances.chromosomes(1, inst.nb_parts, 7)[0], inst.instance_parts)
+
+
+def _worker_decode(row):
+    w = _WORKER
+    inst = w["inst"]
+    return w["ref"].decode(w["rpd"], inst.nb_parts, inst.nb_machines, inst.thresholds, row, inst.instance_parts)[0]
+
+
+def pool_rates(reference, rows, workers, packed):
+    """(reference rows/s over a process pool of `workers`, oracle rows/s on as many threads, equal?)."""
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+    from oracle import oracle_decode
+    ctx = mp.get_context("spawn")
+    with ProcessPoolExecutor(max_workers=workers, mp_context=ctx, initializer=_worker_init,
+                             initargs=(reference,)) as ex:
+        list(ex.map(_worker_decode, rows[:workers]))  # every worker started and compiled
+        t0 = time.perf_counter()
+        ref_ms = np.array(list(ex.map(_worker_decode, rows)), np.float64)
+        ref_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    ora_ms = oracle_decode(packed, rows, n_threads=workers)
+    ora_s = time.perf_counter() - t0
+    return len(rows) / ref_s, len(rows) / ora_s, bool(np.array_equal(ref_ms, ora_ms))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
     ap.add_argument("--rows", type=int, default=12)
+    ap.add_argument("--workers", type=int, default=0)
+    ap.add_argument("--pool-rows", type=int, default=96)
     args = ap.parse_args()
     import bench
     from brkga_fft2_b200 import instances
@@ -74,6 +123,13 @@ def main():
     ours = part_ids_of_log(packed, ora_log)
     feasible = ref_ms < 1e15
     n = len(rows) - 1
+    pool = {}
+    if args.workers > 0:
+        prow = instances.chromosomes(bench.POP, N, bench.chrom_seed(0, 5))[: args.pool_rows]
+        r_rate, o_rate, same = pool_rates(args.reference, prow, args.workers, packed)
+        pool = {"pool": {"workers": args.workers, "rows": len(prow),
+                         "reference_decodes_per_s": r_rate, "oracle_decodes_per_s": o_rate,
+                         "port_over_reference": o_rate / r_rate, "makespans_equal": same}}
     print(json.dumps({
         "workload": "P100M4 pop 500, rows 0..%d of the first timed step" % n,
         "reference": {"code": "placement.py placementProcedure, torch_cpu backend, parallel=False",
@@ -84,7 +140,7 @@ def main():
         "port_over_reference": (n / ora_s) / (n / ref_s),
         "makespans_equal": bool(np.array_equal(ref_ms, ora_ms)),
         "placements_equal": bool((ref_logs[feasible] == ours[feasible]).all()),
-        "feasible_rows": int(feasible.sum()), "rows": len(rows),
+        "feasible_rows": int(feasible.sum()), "rows": len(rows), **pool,
     }))
 
 
