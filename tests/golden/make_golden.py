@@ -23,6 +23,9 @@ column x, bottom row y, rotation).  Outputs:
       feasible / infeasible counts of the whole population.
 * ``syn_<name>.npz`` — seeded synthetic instances (brkga_fft2_b200.instances)
   with reference makespans and placement logs for a batch of chromosomes.
+* ``refms_bench_P100M4_step0.npz`` — the reference's makespans of all 500 rows
+  of the population bench.py times first (decoded over a process pool of
+  all host cores; the rows are regenerated from their seed).
 
 Nothing under tests/ reads the reference at run time; only this script does.
 """
@@ -233,6 +236,38 @@ def log_to_array(log, nb_machines, nb_parts):
     return out
 
 
+_POOL = {}
+
+
+def _pool_init(root):
+    """A process of the reference pool: the reference decoder and the problem of
+    the benchmark's workload (P100M4, bench.py), numba compiled on one row."""
+    import bench as bench_py
+    inst, _ = bench_py.load_workload()
+    ref = Reference(root)
+    rpd = ref.problem(inst.problem_data, inst.nb_machines)
+    _POOL.update(ref=ref, rpd=rpd, inst=inst)
+    ref.decode(rpd, inst.nb_parts, inst.nb_machines, inst.thresholds,
+               syn.chromosomes(1, inst.nb_parts, 7)[0], inst.instance_parts)
+
+
+def _pool_decode(row):
+    """The reference's makespan of one benchmark chromosome (in a pool process)."""
+    p = _POOL
+    inst = p["inst"]
+    return p["ref"].decode(p["rpd"], inst.nb_parts, inst.nb_machines, inst.thresholds, row, inst.instance_parts)[0]
+
+
+def bench_pool(root, workers):
+    """A process pool decoding benchmark rows with the reference, the way its GA
+    spreads a population over the host cores (eval_mode="process",
+    BRKGA_alg3.py:149-154), every worker started with its own problem."""
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+    return ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn"), initializer=_pool_init,
+                               initargs=(root,))
+
+
 def real_heights(root):
     spec = read_xlsx(os.path.join(root, "data/PartsMachines/part-machine-information.xlsx"))
     return {int(r["A"]): r["D"] for r in spec["part"][1:]}
@@ -429,6 +464,19 @@ def main():
             "greedy_placements": np.stack(recs), "height_ids": np.array(ids),
             "heights": np.array([heights[i] for i in ids], np.float64)})
         print(f"{tag}: {len(seeds)} greedy runs  [{time.time() - t0:.1f}s]")
+
+    # the reference's makespans of the whole population of bench.py's first
+    # timed step (500 P100M4 rows, regenerated from their seed by the test)
+    if want("refms_bench_P100M4_step0"):
+        import bench as bench_py
+        seed = bench_py.chrom_seed(0, 5)
+        rows = syn.chromosomes(bench_py.POP, 100, seed)
+        with bench_pool(root, os.cpu_count() or 1) as ex:
+            mss = np.array(list(ex.map(_pool_decode, rows, chunksize=4)), np.float64)
+        np.savez(os.path.join(args.out, "refms_bench_P100M4_step0.npz"), makespans=mss,
+                 pop=np.int64(bench_py.POP), seed=np.int64(seed), instance_seed=np.int64(bench_py.INSTANCE_SEED),
+                 rows_sum=np.float64(rows.astype(np.float64).sum()), first_row=rows[0])
+        print(f"refms_bench_P100M4_step0: {len(rows)} makespans  [{time.time() - t0:.1f}s]")
 
     hts = real_heights(root)
     for (n, mm, k) in ((50, 2, 0), (75, 2, 0), (100, 4, 0)):

@@ -36,42 +36,17 @@ REPO = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, REPO)
 sys.path.insert(0, HERE)
 
-from make_golden import Reference, log_to_array  # noqa: E402
+from make_golden import Reference, _pool_decode, bench_pool, log_to_array  # noqa: E402
 from tests.goldens import part_ids_of_log  # noqa: E402
-
-
-_WORKER = {}
-
-
-def _worker_init(reference):
-    """One process of the pool: the reference and its problem, compiled on one row."""
-    import bench
-    from brkga_fft2_b200 import instances
-    inst, _ = bench.load_workload()
-    ref = Reference(reference)
-    rpd = ref.problem(inst.problem_data, inst.nb_machines)
-    _WORKER.update(ref=ref, rpd=rpd, inst=inst)
-    ref.decode(rpd, inst.nb_parts, inst.nb_machines, inst.thresholds,
-               instances.chromosomes(1, inst.nb_parts, 7)[0], inst.instance_parts)
-
-
-def _worker_decode(row):
-    w = _WORKER
-    inst = w["inst"]
-    return w["ref"].decode(w["rpd"], inst.nb_parts, inst.nb_machines, inst.thresholds, row, inst.instance_parts)[0]
 
 
 def pool_rates(reference, rows, workers, packed):
     """(reference rows/s over a process pool of `workers`, oracle rows/s on as many threads, equal?)."""
-    import multiprocessing as mp
-    from concurrent.futures import ProcessPoolExecutor
     from oracle import oracle_decode
-    ctx = mp.get_context("spawn")
-    with ProcessPoolExecutor(max_workers=workers, mp_context=ctx, initializer=_worker_init,
-                             initargs=(reference,)) as ex:
-        list(ex.map(_worker_decode, rows[:workers]))  # every worker started and compiled
+    with bench_pool(reference, workers) as ex:
+        list(ex.map(_pool_decode, rows[:workers]))  # every worker started and compiled
         t0 = time.perf_counter()
-        ref_ms = np.array(list(ex.map(_worker_decode, rows)), np.float64)
+        ref_ms = np.array(list(ex.map(_pool_decode, rows)), np.float64)
         ref_s = time.perf_counter() - t0
     t0 = time.perf_counter()
     ora_ms = oracle_decode(packed, rows, n_threads=workers)

@@ -125,3 +125,23 @@ def test_oracle_results_do_not_depend_on_threads():
         ms, log = oracle_decode(pk, ch, n_threads=nt, with_log=True)
         np.testing.assert_array_equal(ms, ms1)
         assert (log == log1).all()
+
+
+def test_benchmark_population_against_reference():
+    """All 500 rows of the population bench.py times first: the oracle's
+    makespans equal the reference's own (its sequential decoder run over a
+    process pool by tests/golden/make_golden.py).  bench.py compares the GPU
+    with the oracle on the same rows every run, so the benchmarked rows are
+    tied to the reference row for row."""
+    import os
+    import bench
+    from brkga_fft2_b200 import instances
+    z = np.load(f"{goldens.GOLDEN}/refms_bench_P100M4_step0.npz")
+    assert int(z["pop"]) == bench.POP and int(z["seed"]) == bench.chrom_seed(0, 5)
+    assert int(z["instance_seed"]) == bench.INSTANCE_SEED
+    inst, packed = bench.load_workload()
+    rows = instances.chromosomes(int(z["pop"]), inst.nb_parts, int(z["seed"]))
+    np.testing.assert_array_equal(rows[0], z["first_row"])
+    assert rows.astype(np.float64).sum() == float(z["rows_sum"])
+    ms = oracle_decode(packed, rows, n_threads=os.cpu_count() or 1)
+    np.testing.assert_array_equal(ms, z["makespans"])
