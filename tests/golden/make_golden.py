@@ -25,7 +25,9 @@ column x, bottom row y, rotation).  Outputs:
   with reference makespans and placement logs for a batch of chromosomes.
 * ``refms_bench_P100M4_step0.npz`` — the reference's makespans of all 500 rows
   of the population bench.py times first (decoded over a process pool of
-  all host cores; the rows are regenerated from their seed).
+  all host cores; the rows are regenerated from their seed);
+  ``refms_P200M6_s13.npz`` / ``refms_P400M8_s14.npz`` — the same for the rows
+  the GPU tests compare with the oracle at the 200- and 400-part sizes.
 
 Nothing under tests/ reads the reference at run time; only this script does.
 """
@@ -239,11 +241,11 @@ def log_to_array(log, nb_machines, nb_parts):
 _POOL = {}
 
 
-def _pool_init(root):
+def _pool_init(root, maker="p100m4", inst_seed=0):
     """A process of the reference pool: the reference decoder and the problem of
-    the benchmark's workload (P100M4, bench.py), numba compiled on one row."""
-    import bench as bench_py
-    inst, _ = bench_py.load_workload()
+    a synthetic workload (default: the benchmark's, P100M4 instance seed 0),
+    numba compiled on one row."""
+    inst = getattr(syn, maker)(inst_seed)
     ref = Reference(root)
     rpd = ref.problem(inst.problem_data, inst.nb_machines)
     _POOL.update(ref=ref, rpd=rpd, inst=inst)
@@ -258,14 +260,14 @@ def _pool_decode(row):
     return p["ref"].decode(p["rpd"], inst.nb_parts, inst.nb_machines, inst.thresholds, row, inst.instance_parts)[0]
 
 
-def bench_pool(root, workers):
-    """A process pool decoding benchmark rows with the reference, the way its GA
-    spreads a population over the host cores (eval_mode="process",
+def bench_pool(root, workers, maker="p100m4", inst_seed=0):
+    """A process pool decoding rows of a synthetic workload with the reference,
+    the way its GA spreads a population over the host cores (eval_mode="process",
     BRKGA_alg3.py:149-154), every worker started with its own problem."""
     import multiprocessing as mp
     from concurrent.futures import ProcessPoolExecutor
     return ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn"), initializer=_pool_init,
-                               initargs=(root,))
+                               initargs=(root, maker, inst_seed))
 
 
 def real_heights(root):
@@ -477,6 +479,21 @@ def main():
                  pop=np.int64(bench_py.POP), seed=np.int64(seed), instance_seed=np.int64(bench_py.INSTANCE_SEED),
                  rows_sum=np.float64(rows.astype(np.float64).sum()), first_row=rows[0])
         print(f"refms_bench_P100M4_step0: {len(rows)} makespans  [{time.time() - t0:.1f}s]")
+    # the rows the GPU tests compare with the oracle at the larger configurations
+    # (tests/test_decoder_gpu.py, test_benchmark_workloads_vs_oracle): P200M6 24
+    # rows of seed 13, P400M8 8 rows of seed 14 (workers bounded by memory: the
+    # reference keeps every rotation's plate-sized FFT, ~3 GB and ~18 GB a process)
+    for maker, P, seed, workers in (("p200m6", 24, 13, 4), ("p400m8", 8, 14, 2)):
+        tag = f"refms_{maker.upper()}_s{seed}"
+        if not want(tag):
+            continue
+        inst = getattr(syn, maker)(0)
+        rows = syn.chromosomes(P, inst.nb_parts, seed)
+        with bench_pool(root, workers, maker, 0) as ex:
+            mss = np.array(list(ex.map(_pool_decode, rows)), np.float64)
+        np.savez(os.path.join(args.out, f"{tag}.npz"), makespans=mss, pop=np.int64(P), seed=np.int64(seed),
+                 instance_seed=np.int64(0), rows_sum=np.float64(rows.astype(np.float64).sum()), first_row=rows[0])
+        print(f"{tag}: {len(rows)} makespans  [{time.time() - t0:.1f}s]")
 
     hts = real_heights(root)
     for (n, mm, k) in ((50, 2, 0), (75, 2, 0), (100, 4, 0)):

@@ -145,3 +145,20 @@ def test_benchmark_population_against_reference():
     assert rows.astype(np.float64).sum() == float(z["rows_sum"])
     ms = oracle_decode(packed, rows, n_threads=os.cpu_count() or 1)
     np.testing.assert_array_equal(ms, z["makespans"])
+
+
+@pytest.mark.parametrize("tag,maker", [("refms_P200M6_s13", "p200m6"), ("refms_P400M8_s14", "p400m8")])
+def test_large_workload_rows_against_reference(tag, maker):
+    """The rows that the GPU tests compare with the oracle at the 200- and
+    400-part sizes (tests/test_decoder_gpu.py, test_benchmark_workloads_vs_oracle):
+    the oracle's makespans equal the reference's own."""
+    import os
+    from brkga_fft2_b200 import instances, pack_problem
+    z = np.load(f"{goldens.GOLDEN}/{tag}.npz")
+    inst = getattr(instances, maker)(int(z["instance_seed"]))
+    packed = pack_problem(inst.problem_data, inst.nb_parts, inst.nb_machines, inst.thresholds, inst.instance_parts)
+    rows = instances.chromosomes(int(z["pop"]), inst.nb_parts, int(z["seed"]))
+    np.testing.assert_array_equal(rows[0], z["first_row"])
+    assert rows.astype(np.float64).sum() == float(z["rows_sum"])
+    ms = oracle_decode(packed, rows, n_threads=os.cpu_count() or 1)
+    np.testing.assert_array_equal(ms, z["makespans"])
