@@ -27,7 +27,8 @@ column x, bottom row y, rotation).  Outputs:
   of the population bench.py times first (decoded over a process pool of
   all host cores; the rows are regenerated from their seed);
   ``refms_P200M6_s13.npz`` / ``refms_P400M8_s14.npz`` — the same for the rows
-  the GPU tests compare with the oracle at the 200- and 400-part sizes.
+  the GPU tests compare with the oracle at the 200- and 400-part sizes;
+  ``refms_uneven.npz`` — and for the rows of the uneven multi-instance test.
 
 Nothing under tests/ reads the reference at run time; only this script does.
 """
@@ -494,6 +495,23 @@ def main():
         np.savez(os.path.join(args.out, f"{tag}.npz"), makespans=mss, pop=np.int64(P), seed=np.int64(seed),
                  instance_seed=np.int64(0), rows_sum=np.float64(rows.astype(np.float64).sum()), first_row=rows[0])
         print(f"{tag}: {len(rows)} makespans  [{time.time() - t0:.1f}s]")
+    # the rows of the uneven multi-instance GPU test (tests/test_multi_gpu.py:
+    # instance k = instances.uneven(k), POPS[k] rows of seed 100 + k), except
+    # the one-machine instance, which the reference cannot decode (placement.py
+    # reads thresholds[0] of an empty list)
+    if want("refms_uneven"):
+        pops = [12, 0, 9, 16, 3, 7, 5]
+        out = {"pops": np.array(pops, np.int64)}
+        for k, P in enumerate(pops):
+            inst = syn.uneven(k)
+            if P == 0 or inst.nb_machines < 2:
+                continue
+            rows = syn.chromosomes(P, inst.nb_parts, 100 + k)
+            with bench_pool(root, min(4, P), "uneven", k) as ex:
+                out[f"makespans_{k}"] = np.array(list(ex.map(_pool_decode, rows)), np.float64)
+            out[f"rows_sum_{k}"] = np.float64(rows.astype(np.float64).sum())
+        np.savez(os.path.join(args.out, "refms_uneven.npz"), **out)
+        print(f"refms_uneven: {sorted(k for k in out if k.startswith('makespans'))}  [{time.time() - t0:.1f}s]")
 
     hts = real_heights(root)
     for (n, mm, k) in ((50, 2, 0), (75, 2, 0), (100, 4, 0)):

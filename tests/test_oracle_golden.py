@@ -162,3 +162,25 @@ def test_large_workload_rows_against_reference(tag, maker):
     assert rows.astype(np.float64).sum() == float(z["rows_sum"])
     ms = oracle_decode(packed, rows, n_threads=os.cpu_count() or 1)
     np.testing.assert_array_equal(ms, z["makespans"])
+
+
+def test_uneven_instance_rows_against_reference():
+    """The rows of the uneven multi-instance GPU test (tests/test_multi_gpu.py,
+    instance k = uneven(k) with rows of seed 100 + k): the oracle's makespans
+    equal the reference's own on every instance with at least two machines."""
+    import os
+    from brkga_fft2_b200 import instances, pack_problem
+    z = np.load(f"{goldens.GOLDEN}/refms_uneven.npz")
+    done = 0
+    for k, P in enumerate(z["pops"].tolist()):
+        if f"makespans_{k}" not in z:
+            continue
+        inst = instances.uneven(k)
+        packed = pack_problem(inst.problem_data, inst.nb_parts, inst.nb_machines, inst.thresholds,
+                              inst.instance_parts)
+        rows = instances.chromosomes(P, inst.nb_parts, 100 + k)
+        assert rows.astype(np.float64).sum() == float(z[f"rows_sum_{k}"])
+        ms = oracle_decode(packed, rows, n_threads=os.cpu_count() or 1)
+        np.testing.assert_array_equal(ms, z[f"makespans_{k}"], err_msg=f"instance {k}")
+        done += 1
+    assert done == 5
