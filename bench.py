@@ -368,19 +368,53 @@ def run_reference(args):
     }))
 
 
-def parity_and_cpu(dd, packed, host_rows, P, M, N, torch):
+# The reference's own makespans of the populations of the first and last timed
+# steps under the default warm-up and step counts (populations 5 and 24), made
+# by running the reference's decoder (tests/golden/make_golden.py).
+REFERENCE_FIXTURES = {5: "refms_bench_P100M4_step0", 24: "refms_bench_P100M4_step19"}
+
+
+def reference_anchor(step_makespans):
+    """Compare GPU makespans of whole timed populations, given as (population
+    index, makespans) pairs, with the reference's own where a fixture holds that
+    population (same seed and size); other populations are skipped."""
+    import numpy as np
+    rows = exact = 0
+    used = []
+    for step, ms in step_makespans:
+        tag = REFERENCE_FIXTURES.get(int(step))
+        path = os.path.join(HERE, "tests", "golden", f"{tag}.npz") if tag else ""
+        if not path or not os.path.exists(path):
+            continue
+        z = np.load(path)
+        ms = np.asarray(ms, np.float64)
+        if int(z["seed"]) != chrom_seed(0, int(step)) or int(z["pop"]) != ms.shape[0]:
+            continue
+        rows += ms.shape[0]
+        exact += int((ms == z["makespans"]).sum())
+        used.append(tag)
+    return {"rows": rows, "exact": exact, "fixtures": used,
+            "checked": "GPU makespans (==) against the reference's own sequential decoder (placement.py "
+                       "placementProcedure, torch_cpu backend) run on the same rows when the fixtures were made"}
+
+
+def parity_and_cpu(dd, packed, host_rows, P, M, N, torch, step_ids=()):
     """Decode the given host populations again on the GPU with placement logs
     and with the CPU oracle on all host threads; compare every makespan and
-    every placement.  Returns (parity record, cpu_baseline record)."""
+    every placement, and the makespans with the reference's own where a
+    fixture holds the population (``step_ids``: their population indices).
+    Returns (parity record, cpu_baseline record)."""
     import numpy as np
     from oracle import oracle_decode
     threads = os.cpu_count() or 1
     rows = exact = placements_bad = 0
     cpu_s = 0.0
+    gpu_ms = []
     for h in host_rows:
         dev = torch.from_numpy(h).cuda()
         log = torch.empty((P, M, N, 5), dtype=torch.int32, device="cuda")
         ms = dd.decode(dev, log=log).cpu().numpy()
+        gpu_ms.append(ms)
         glog = log.cpu().numpy()
         t0 = time.perf_counter()
         rms, rlog = oracle_decode(packed, h, n_threads=threads, with_log=True)
@@ -395,6 +429,10 @@ def parity_and_cpu(dd, packed, host_rows, P, M, N, torch):
               "rows_with_placement_differences": placements_bad,
               "checked": "every makespan (==) and every placement (gene, plate, x, bottom row y, rotation) of "
                          "the first and last timed steps' populations against the CPU oracle"}
+    try:
+        parity["reference"] = reference_anchor(list(zip(step_ids, gpu_ms)))
+    except Exception as exc:  # a report, never a reason to lose the bench line
+        parity["reference"] = {"error": f"{type(exc).__name__}: {exc}"}
     cpu = {"value": rows / cpu_s, "unit": UNIT, "cores": threads, "kind": "port", "code": CPU_CODE,
            "note": CPU_NOTE,
            "sample": f"the {rows} chromosomes of the parity check (the first and last timed steps), decoded "
@@ -521,8 +559,8 @@ def run_ours(args):
         if clocks:
             line["clocks"] = clocks
         if not args.no_cpu_baseline:
-            steps = [host[args.warmup]] + ([host[args.warmup + args.steps - 1]] if args.steps > 1 else [])
-            parity, cpu = parity_and_cpu(dd, packed, steps, P, M, N, torch)
+            ids = [args.warmup] + ([args.warmup + args.steps - 1] if args.steps > 1 else [])
+            parity, cpu = parity_and_cpu(dd, packed, [host[i] for i in ids], P, M, N, torch, step_ids=ids)
             line["parity"] = parity
             if world == 1:
                 line["cpu_baseline"] = cpu

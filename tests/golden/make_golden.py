@@ -23,9 +23,10 @@ column x, bottom row y, rotation).  Outputs:
       feasible / infeasible counts of the whole population.
 * ``syn_<name>.npz`` — seeded synthetic instances (brkga_fft2_b200.instances)
   with reference makespans and placement logs for a batch of chromosomes.
-* ``refms_bench_P100M4_step0.npz`` — the reference's makespans of all 500 rows
-  of the population bench.py times first (decoded over a process pool of
-  all host cores; the rows are regenerated from their seed);
+* ``refms_bench_P100M4_step0.npz`` / ``_step19.npz`` — the reference's
+  makespans of all 500 rows of the populations bench.py times first and last
+  (decoded over a process pool of all host cores; the rows are regenerated
+  from their seed);
   ``refms_P200M6_s13.npz`` / ``refms_P400M8_s14.npz`` — the same for the rows
   the GPU tests compare with the oracle at the 200- and 400-part sizes;
   ``refms_uneven.npz`` — and for the rows of the uneven multi-instance test.
@@ -468,18 +469,22 @@ def main():
             "heights": np.array([heights[i] for i in ids], np.float64)})
         print(f"{tag}: {len(seeds)} greedy runs  [{time.time() - t0:.1f}s]")
 
-    # the reference's makespans of the whole population of bench.py's first
-    # timed step (500 P100M4 rows, regenerated from their seed by the test)
-    if want("refms_bench_P100M4_step0"):
+    # the reference's makespans of the whole populations of bench.py's first and
+    # last timed steps with its defaults (warm-up 5, 20 steps: populations 5 and
+    # 24; 500 P100M4 rows each, regenerated from their seed by the test) — the
+    # two steps whose rows bench.py checks against the oracle
+    for tag, step in (("refms_bench_P100M4_step0", 5), ("refms_bench_P100M4_step19", 24)):
+        if not want(tag):
+            continue
         import bench as bench_py
-        seed = bench_py.chrom_seed(0, 5)
+        seed = bench_py.chrom_seed(0, step)
         rows = syn.chromosomes(bench_py.POP, 100, seed)
         with bench_pool(root, os.cpu_count() or 1) as ex:
             mss = np.array(list(ex.map(_pool_decode, rows, chunksize=4)), np.float64)
-        np.savez(os.path.join(args.out, "refms_bench_P100M4_step0.npz"), makespans=mss,
+        np.savez(os.path.join(args.out, f"{tag}.npz"), makespans=mss,
                  pop=np.int64(bench_py.POP), seed=np.int64(seed), instance_seed=np.int64(bench_py.INSTANCE_SEED),
                  rows_sum=np.float64(rows.astype(np.float64).sum()), first_row=rows[0])
-        print(f"refms_bench_P100M4_step0: {len(rows)} makespans  [{time.time() - t0:.1f}s]")
+        print(f"{tag}: {len(rows)} makespans  [{time.time() - t0:.1f}s]")
     # the rows the GPU tests compare with the oracle at the larger configurations
     # (tests/test_decoder_gpu.py, test_benchmark_workloads_vs_oracle): P200M6 24
     # rows of seed 13, P400M8 8 rows of seed 14 (workers bounded by memory: the

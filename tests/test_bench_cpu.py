@@ -64,3 +64,24 @@ def test_clock_sampler_keeps_the_timed_region(tmp_path):
     assert got["in_timed_region"] and got["samples"] == 3
     assert got["sm_mhz"] == 1965.0 and got["reasons"] == ["sw_power_cap"]
     assert not os.path.exists(cs.path)
+
+
+def test_reference_anchor_compares_with_the_reference_fixtures():
+    """bench.py's parity record compares the GPU makespans of the first and last
+    timed populations with the reference's own (tests/golden/refms_bench_*):
+    fed the reference's makespans it counts every row exact, one changed row
+    is counted, and populations without a fixture (other step counts or sizes)
+    are skipped."""
+    import numpy as np
+    bench = load_bench()
+    z0 = np.load(os.path.join(HERE, "golden", "refms_bench_P100M4_step0.npz"))
+    z19 = np.load(os.path.join(HERE, "golden", "refms_bench_P100M4_step19.npz"))
+    rec = bench.reference_anchor([(5, z0["makespans"]), (24, z19["makespans"])])
+    assert rec["rows"] == 1000 and rec["exact"] == 1000
+    assert rec["fixtures"] == ["refms_bench_P100M4_step0", "refms_bench_P100M4_step19"]
+    bad = z19["makespans"].copy()
+    bad[7] += 1.0
+    assert bench.reference_anchor([(5, z0["makespans"]), (24, bad)])["exact"] == 999
+    assert bench.reference_anchor([(6, z0["makespans"])])["rows"] == 0
+    assert bench.reference_anchor([(5, z0["makespans"][:100])])["rows"] == 0
+    json.dumps(rec)

@@ -127,17 +127,19 @@ def test_oracle_results_do_not_depend_on_threads():
         assert (log == log1).all()
 
 
-def test_benchmark_population_against_reference():
-    """All 500 rows of the population bench.py times first: the oracle's
-    makespans equal the reference's own (its sequential decoder run over a
-    process pool by tests/golden/make_golden.py).  bench.py compares the GPU
-    with the oracle on the same rows every run, so the benchmarked rows are
-    tied to the reference row for row."""
+@pytest.mark.parametrize("tag,step", [("refms_bench_P100M4_step0", 5), ("refms_bench_P100M4_step19", 24)])
+def test_benchmark_population_against_reference(tag, step):
+    """All 500 rows of the populations bench.py times first and last (with its
+    default 5 warm-up and 20 timed steps): the oracle's makespans equal the
+    reference's own (its sequential decoder run over a process pool by
+    tests/golden/make_golden.py).  bench.py compares the GPU with the oracle
+    on the same two populations every run, so the benchmarked rows are tied
+    to the reference row for row."""
     import os
     import bench
     from brkga_fft2_b200 import instances
-    z = np.load(f"{goldens.GOLDEN}/refms_bench_P100M4_step0.npz")
-    assert int(z["pop"]) == bench.POP and int(z["seed"]) == bench.chrom_seed(0, 5)
+    z = np.load(f"{goldens.GOLDEN}/{tag}.npz")
+    assert int(z["pop"]) == bench.POP and int(z["seed"]) == bench.chrom_seed(0, step)
     assert int(z["instance_seed"]) == bench.INSTANCE_SEED
     inst, packed = bench.load_workload()
     rows = instances.chromosomes(int(z["pop"]), inst.nb_parts, int(z["seed"]))
