@@ -30,6 +30,9 @@ column x, bottom row y, rotation).  Outputs:
   ``refms_P200M6_s13.npz`` / ``refms_P400M8_s14.npz`` — the same for the rows
   the GPU tests compare with the oracle at the 200- and 400-part sizes;
   ``refms_uneven.npz`` — and for the rows of the uneven multi-instance test.
+* ``ga_ops.npz`` — one generation of the reference's GA operators (partition,
+  mating, mutants) on seeded populations, its random draws replaced by the
+  device GA's Philox draws, so the GA oracle's breed can be compared with it.
 
 Nothing under tests/ reads the reference at run time; only this script does.
 """
@@ -270,6 +273,54 @@ def bench_pool(root, workers, maker="p100m4", inst_seed=0):
     from concurrent.futures import ProcessPoolExecutor
     return ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn"), initializer=_pool_init,
                                initargs=(root, maker, inst_seed))
+
+
+def reference_ga_step(root, pop, fit, ne, nm, rho, seed, gen):
+    """One generation of the reference's GA operators (BRKGA_alg3.py:178-208 and
+    the new population of :246-250: partition, mating, mutants) on (pop, fit),
+    numpy's random draws replaced by the device GA's Philox draws for (seed,
+    gen) — every offspring's elite and non-elite parent (mapped into the
+    reference's elite and non-elite arrays), its crossover uniforms, and the
+    mutants.  Returns the next population and the elites' carried fitness."""
+    from types import SimpleNamespace
+    sys.path.insert(0, root)
+    import BRKGA_alg3
+    sys.path.insert(0, REPO)
+    from oracle import ga_oracle as go
+    P, K = pop.shape
+    ns = SimpleNamespace(num_elites=ne, num_individuals=P, num_mutants=nm, num_gene=K, eliteCProb=rho)
+    order = go.rank(fit)
+    non_elite_rows = np.argpartition(np.asarray(fit), ne)[ne:]  # the reference's non-elite order
+    rows = np.arange(ne + nm, P)
+    pr = go.philox(0, rows, gen, go.TAG_PARENTS, seed)
+    e_idx = go.mulhi(pr[0], ne)
+    o_rows = order[ne + go.mulhi(pr[1], P - ne)]
+    pos = {int(r): j for j, r in enumerate(non_elite_rows)}
+    o_idx = np.array([pos[int(r)] for r in o_rows], np.int64)
+    ints = [e_idx, o_idx]
+    unis = [go.keys_block(rows, K, gen, go.TAG_MASK, seed), go.keys_block(np.arange(ne, ne + nm), K, gen,
+                                                                          go.TAG_MUTANT, seed)]
+
+    def randint(low, high=None, size=None):
+        v = ints.pop(0)
+        assert low == 0 and v.shape == (size,) and (v < high).all()
+        return v
+
+    def uniform(low=0.0, high=1.0, size=None):
+        v = unis.pop(0)
+        assert low == 0.0 and high == 1.0 and v.shape == tuple(size)
+        return v
+
+    saved = np.random.randint, np.random.uniform
+    np.random.randint, np.random.uniform = randint, uniform
+    try:
+        elites, non_elites, elite_fit = BRKGA_alg3.BRKGA.partition(ns, pop, fit)
+        offspring = BRKGA_alg3.BRKGA.mating(ns, elites, non_elites)
+        mutants = BRKGA_alg3.BRKGA.mutants(ns)
+    finally:
+        np.random.randint, np.random.uniform = saved
+    assert not ints and not unis
+    return np.concatenate((elites, mutants, offspring), axis=0), np.asarray(elite_fit, np.float64)
 
 
 def real_heights(root):
@@ -517,6 +568,23 @@ def main():
             out[f"rows_sum_{k}"] = np.float64(rows.astype(np.float64).sum())
         np.savez(os.path.join(args.out, "refms_uneven.npz"), **out)
         print(f"refms_uneven: {sorted(k for k in out if k.startswith('makespans'))}  [{time.time() - t0:.1f}s]")
+
+    # the reference's GA operators on seeded populations, fed the device GA's
+    # random draws: (P, N, elites, mutants, rho, seed, generation) per case —
+    # the reference's proportions, the 10/15 % of BRKGA_alg3.py:608-618, one
+    # elite and no mutants, and no offspring at all
+    if want("ga_ops"):
+        cases = [(40, 10, 6, 8, 0.7, 123, 3), (100, 25, 10, 15, 0.7, 7, 1), (57, 13, 1, 0, 0.5, 99, 200),
+                 (64, 8, 13, 51, 0.9, 5, 2)]
+        out = {"cases": np.array(cases, np.float64)}
+        rng = np.random.default_rng(2024)
+        for i, (P, N, ne, nm, rho, seed, gen) in enumerate(cases):
+            pop = rng.random((P, 2 * N)).astype(np.float32)
+            fit = rng.permutation(P).astype(np.float64) * 1000.0 + rng.random(P)  # no ties
+            nxt, efit = reference_ga_step(root, pop, fit, ne, nm, rho, seed, gen)
+            out.update({f"pop_{i}": pop, f"fit_{i}": fit, f"next_{i}": nxt, f"elite_fit_{i}": efit})
+        np.savez(os.path.join(args.out, "ga_ops.npz"), **out)
+        print(f"ga_ops: {len(cases)} cases  [{time.time() - t0:.1f}s]")
 
     hts = real_heights(root)
     for (n, mm, k) in ((50, 2, 0), (75, 2, 0), (100, 4, 0)):

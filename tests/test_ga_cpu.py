@@ -75,3 +75,22 @@ def test_multi_ga_refuses_bad_arguments_before_any_gpu_work(kwargs):
     pk = pack_problem(inst.problem_data, inst.nb_parts, inst.nb_machines, inst.thresholds, inst.instance_parts)
     with pytest.raises(ValueError):
         MultiBRKGA([pk], **dict(dict(num_generations=2, num_individuals=100), **kwargs))
+
+
+def test_breed_equals_the_reference_operators_on_the_same_draws():
+    """One generation of the reference's own partition, mating and mutants
+    (BRKGA_alg3.py:178-208, the new population of :246-250), run by
+    tests/golden/make_golden.py with numpy's random draws replaced by this
+    GA's Philox draws (the same parents, crossover uniforms and mutants):
+    the oracle's breed gives the same population, row for row and key for key,
+    and carries the same elite fitness.  Cases: 10/15 % elites/mutants, one
+    elite and no mutants, and no offspring at all."""
+    import os
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "ga_ops.npz"))
+    for i, (P, N, ne, nm, rho, seed, gen) in enumerate(z["cases"].tolist()):
+        P, ne, nm, seed, gen = int(P), int(ne), int(nm), int(seed), int(gen)
+        pop, fit = z[f"pop_{i}"], z[f"fit_{i}"]
+        nxt, nfit = go.breed(pop, fit, go.rank(fit), ne, nm, rho, seed, gen)
+        assert nxt.dtype == np.float32 and nxt.shape == z[f"next_{i}"].shape
+        np.testing.assert_array_equal(nxt, z[f"next_{i}"], err_msg=f"case {i}")
+        np.testing.assert_array_equal(nfit[:ne], z[f"elite_fit_{i}"], err_msg=f"case {i}")
