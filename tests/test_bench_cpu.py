@@ -85,3 +85,54 @@ def test_reference_anchor_compares_with_the_reference_fixtures():
     assert bench.reference_anchor([(6, z0["makespans"])])["rows"] == 0
     assert bench.reference_anchor([(5, z0["makespans"][:100])])["rows"] == 0
     json.dumps(rec)
+
+
+def test_parity_record_with_a_stand_in_decoder():
+    """bench.parity_and_cpu end to end on the CPU: a stand-in for the device
+    decoder (the oracle, behind numpy-backed stand-ins of the few torch calls
+    the function makes) gives every row exact, every placement exact, and no
+    reference rows for a population without a fixture."""
+    import numpy as np
+    bench = load_bench()
+    from brkga_fft2_b200 import instances
+    from oracle import oracle_decode
+    inst, packed = bench.load_workload()
+
+    class T:  # a host array standing in for a device tensor
+        def __init__(self, a):
+            self.a = a
+
+        def cuda(self):
+            return self
+
+        def cpu(self):
+            return self
+
+        def numpy(self):
+            return self.a
+
+    class FakeTorch:
+        int32 = np.int32
+
+        @staticmethod
+        def from_numpy(h):
+            return T(h)
+
+        @staticmethod
+        def empty(shape, dtype=None, device=None):
+            return T(np.zeros(shape, np.int32))
+
+    class Decoder:
+        def decode(self, dev, log=None):
+            ms, lg = oracle_decode(packed, dev.a, n_threads=2, with_log=True)
+            log.a[...] = np.stack([lg[f] for f in ("gene", "bin", "x", "y", "rot")], axis=-1)
+            return T(ms)
+
+    P, N, M = 8, inst.nb_parts, inst.nb_machines
+    rows = [instances.chromosomes(P, N, bench.chrom_seed(0, s)) for s in (3, 4)]
+    parity, cpu = bench.parity_and_cpu(Decoder(), packed, rows, P, M, N, FakeTorch, step_ids=[3, 4])
+    assert parity["rows"] == 16 and parity["exact"] == 16 and parity["placements_exact"]
+    assert parity["reference"]["rows"] == 0 and parity["reference"]["fixtures"] == []
+    assert cpu["kind"] == "port" and cpu["value"] > 0
+    json.dumps(parity)
+    json.dumps(cpu)
